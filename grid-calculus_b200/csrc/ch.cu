@@ -1,0 +1,295 @@
+// Cahn-Hilliard time stepping: fused RK4 / explicit-Euler stage kernels.
+//
+// RHS (examples/common/cahn_hilliard.hpp:38-59): M lap(mu), mu = -y + y^3 - kappa lap(y).
+// RK4 (solve/RK4.hpp:99-154): k1 = f(psi), k2 = f(psi + dt/2 k1),
+// k3 = f(psi + dt/2 k2), k4 = f(psi + dt k3),
+// psi' = psi + (dt/6 (k1 + k4) + dt/3 (k2 + k3)).
+//
+// One kernel per stage.  A CTA owns a TX x TY (x TZ) tile of output cells:
+//   phase 1  y = psi + a k_prev on the tile plus a 2r halo (wrapped loads),
+//            staged in shared memory;
+//   phase 2  mu on the tile plus an r halo from the staged y;
+//   phase 3  k_s = M lap(mu) on the tile; the last stage instead combines
+//            k1, k2, k3 (re-read at the own cell) with k4 and writes psi'.
+// Per step each field is read or written once in HBM: 13 field passes
+// (stage 1: 2, stages 2-3: 3 each, stage 4: 5); the halo re-reads are L2 hits.
+// psi' goes to a second buffer (other CTAs still read psi's halo), so steps
+// ping-pong between the caller's buffer and a context buffer; the step
+// sequence is captured once into a CUDA graph and replayed.
+// Double arithmetic keeps the reference's operation order without FMA, so
+// double results match the CPU reference bit for bit.
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+#include "stepper.cuh"
+
+namespace gcb {
+namespace {
+
+constexpr int kThreads = 256;
+
+enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+
+template <class T>
+struct StageParams {
+  const T* psi;    // state
+  const T* kin;    // previous stage (y = psi + a kin), nullptr for y = psi
+  T a;             // stage coefficient
+  T* out;          // k_s (MODE_RHS) or psi' (final modes)
+  const T* k1;     // MODE_RK4_FINAL only
+  const T* k2;
+  const T* k3;
+  T c6, c3;        // dt/6, dt/3 (RK4 final) ; c6 = dt (Euler final)
+  T mob, kappa;
+  T ihx2, ihy2, ihz2;
+  int nx, ny, nz;
+};
+
+template <class T, int ORDER, bool Z3>
+struct Tile;
+// 2-D tiles: 64 wide rows (512 B of doubles) for coalescing.
+template <class T, int ORDER>
+struct Tile<T, ORDER, false> { static constexpr int TX = 64, TY = 16, TZ = 1; };
+template <class T, int ORDER>
+struct Tile<T, ORDER, true> {
+  static constexpr int TX = 32, TY = ORDER == 2 ? 8 : 4, TZ = ORDER == 2 ? 8 : 4;
+};
+
+template <class T, int ORDER, bool Z3, int MODE>
+__global__ void __launch_bounds__(kThreads) ch_stage_kernel(const StageParams<T> p) {
+  constexpr int R = W<2, ORDER>::R;
+  constexpr int TX = Tile<T, ORDER, Z3>::TX, TY = Tile<T, ORDER, Z3>::TY, TZ = Tile<T, ORDER, Z3>::TZ;
+  constexpr int RZ = Z3 ? R : 0;
+  // y region: tile + 2R halo; mu region: tile + R halo.
+  constexpr int YX = TX + 4 * R, YY = TY + 4 * R, YZ = TZ + 4 * RZ;
+  constexpr int MX = TX + 2 * R, MY = TY + 2 * R, MZ = TZ + 2 * RZ;
+  constexpr int YN = YX * YY * YZ, MN = MX * MY * MZ, ON = TX * TY * TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ys = reinterpret_cast<T*>(smem_raw);
+  T* ms = ys + YN;
+
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  const size_t plane = static_cast<size_t>(nx) * ny;
+
+  // Phase 1: y on the tile + 2R halo.
+  for (int e = threadIdx.x; e < YN; e += kThreads) {
+    const int ex = e % YX;
+    const int rest = e / YX;
+    const int ey = rest % YY;
+    const int ez = rest / YY;
+    const int gx = wrap(x0 - 2 * R + ex, nx);
+    const int gy = wrap(y0 - 2 * R + ey, ny);
+    const int gz = Z3 ? wrap(z0 - 2 * RZ + ez, nz) : 0;
+    const size_t gi = static_cast<size_t>(gz) * plane + static_cast<size_t>(gy) * nx + gx;
+    T v = __ldg(p.psi + gi);
+    if (p.kin) v = Ar<T>::add(v, Ar<T>::mul(p.a, __ldg(p.kin + gi)));
+    ys[e] = v;
+  }
+  __syncthreads();
+
+  // Phase 2: mu = -y + y^3 - kappa lap(y) on the tile + R halo.
+  for (int e = threadIdx.x; e < MN; e += kThreads) {
+    const int ex = e % MX;
+    const int rest = e / MX;
+    const int ey = rest % MY;
+    const int ez = rest / MY;
+    const int c = ((ez + RZ) * YY + (ey + R)) * YX + (ex + R);  // same cell in y space
+    const T ax = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + o]; });
+    const T ay = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + o * YX]; });
+    const T az = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + (Z3 ? o : 0) * YX * YY]; });
+    const T lap = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+    const T y = ys[c];
+    ms[e] = Ar<T>::sub(Ar<T>::add(-y, Ar<T>::mul(Ar<T>::mul(y, y), y)), Ar<T>::mul(p.kappa, lap));
+  }
+  __syncthreads();
+
+  // Phase 3: k_s = M lap(mu) on the tile.
+  for (int e = threadIdx.x; e < ON; e += kThreads) {
+    const int ex = e % TX;
+    const int rest = e / TX;
+    const int ey = rest % TY;
+    const int ez = rest / TY;
+    const int gx = x0 + ex, gy = y0 + ey, gz = z0 + ez;
+    if (gx >= nx || gy >= ny || gz >= nz) continue;
+    const int c = ((ez + RZ) * MY + (ey + R)) * MX + (ex + R);
+    const T ax = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + o]; });
+    const T ay = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + o * MX]; });
+    const T az = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + (Z3 ? o : 0) * MX * MY]; });
+    const T lap = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+    const T rhs = Ar<T>::mul(lap, p.mob);
+    const size_t gi = static_cast<size_t>(gz) * plane + static_cast<size_t>(gy) * nx + gx;
+    if constexpr (MODE == MODE_RHS) {
+      p.out[gi] = rhs;
+    } else if constexpr (MODE == MODE_RK4_FINAL) {
+      const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
+      const T s23 = Ar<T>::add(__ldg(p.k2 + gi), __ldg(p.k3 + gi));
+      p.out[gi] = Ar<T>::add(__ldg(p.psi + gi), Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+    } else {
+      const int cy = ((ez + 2 * RZ) * YY + (ey + 2 * R)) * YX + (ex + 2 * R);
+      p.out[gi] = Ar<T>::add(ys[cy], Ar<T>::mul(p.c6, rhs));
+    }
+  }
+}
+
+template <class T, int ORDER, bool Z3, int MODE>
+gc_status launch_stage(gc_context* ctx, const StageParams<T>& p) {
+  constexpr int R = W<2, ORDER>::R;
+  using TL = Tile<T, ORDER, Z3>;
+  constexpr int RZ = Z3 ? R : 0;
+  constexpr size_t smem =
+      sizeof(T) * (static_cast<size_t>(TL::TX + 4 * R) * (TL::TY + 4 * R) * (TL::TZ + 4 * RZ) +
+                   static_cast<size_t>(TL::TX + 2 * R) * (TL::TY + 2 * R) * (TL::TZ + 2 * RZ));
+  auto kern = ch_stage_kernel<T, ORDER, Z3, MODE>;
+  if (smem > 48 * 1024) GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(div_up(p.nx, TL::TX), div_up(p.ny, TL::TY), Z3 ? div_up(p.nz, TL::TZ) : 1);
+  kern<<<grid, kThreads, smem, ctx->stream>>>(p);
+  GC_CHECK_LAUNCH("ch_stage_kernel");
+  return GC_OK;
+}
+
+template <class T, int MODE>
+gc_status launch_mode(gc_context* ctx, int order, const StageParams<T>& p) {
+  const bool z3 = p.nz > 1;
+  switch (order) {
+    case 2: return z3 ? launch_stage<T, 2, true, MODE>(ctx, p) : launch_stage<T, 2, false, MODE>(ctx, p);
+    case 4: return z3 ? launch_stage<T, 4, true, MODE>(ctx, p) : launch_stage<T, 4, false, MODE>(ctx, p);
+    case 6: return z3 ? launch_stage<T, 6, true, MODE>(ctx, p) : launch_stage<T, 6, false, MODE>(ctx, p);
+  }
+  return fail(GC_ERR_UNSUPPORTED, "gridcalc_b200: Cahn-Hilliard order must be 2, 4 or 6");
+}
+
+template <class T>
+StageParams<T> base_params(const gc_grid* g, const gc_ch_params* cp) {
+  StageParams<T> p{};
+  p.nx = g->nx; p.ny = g->ny; p.nz = g->nz;
+  p.ihx2 = static_cast<T>(1.0 / (g->hx * g->hx));
+  p.ihy2 = static_cast<T>(1.0 / (g->hy * g->hy));
+  p.ihz2 = static_cast<T>(1.0 / (g->hz * g->hz));
+  p.mob = static_cast<T>(cp->mobility);
+  p.kappa = static_cast<T>(cp->kappa);
+  return p;
+}
+
+// Enqueues one time step from `src` into `dst` (src != dst).
+template <class T>
+gc_status enqueue_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const T* src,
+                       T* dst, T* k1, T* k2, T* k3, double dt, gc_integrator integ) {
+  StageParams<T> p = base_params<T>(g, cp);
+  p.psi = src;
+  const int order = cp->order;
+  gc_status s;
+  if (integ == GC_EXPLICIT_EULER) {
+    p.kin = nullptr;
+    p.out = dst;
+    p.c6 = static_cast<T>(dt);
+    return launch_mode<T, MODE_EULER_FINAL>(ctx, order, p);
+  }
+  const double half_dt = 0.5 * dt, sixth_dt = dt / 6.0, third_dt = dt / 3.0;
+  p.kin = nullptr; p.out = k1;
+  if ((s = launch_mode<T, MODE_RHS>(ctx, order, p)) != GC_OK) return s;
+  p.kin = k1; p.a = static_cast<T>(half_dt); p.out = k2;
+  if ((s = launch_mode<T, MODE_RHS>(ctx, order, p)) != GC_OK) return s;
+  p.kin = k2; p.a = static_cast<T>(half_dt); p.out = k3;
+  if ((s = launch_mode<T, MODE_RHS>(ctx, order, p)) != GC_OK) return s;
+  p.kin = k3; p.a = static_cast<T>(dt); p.out = dst;
+  p.k1 = k1; p.k2 = k2; p.k3 = k3;
+  p.c6 = static_cast<T>(sixth_dt); p.c3 = static_cast<T>(third_dt);
+  return launch_mode<T, MODE_RK4_FINAL>(ctx, order, p);
+}
+
+template <class T>
+gc_status integrate_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, T* psi,
+                      double dt, int n_steps, gc_integrator integ) {
+  const size_t n = cells(g);
+  const size_t bytes = n * sizeof(T);
+  void *vb = nullptr, *v1 = nullptr, *v2 = nullptr, *v3 = nullptr;
+  gc_status s;
+  if ((s = scratch_get(ctx, kSlotPsiB, bytes, &vb)) != GC_OK) return s;
+  if (integ == GC_RK4) {
+    if ((s = scratch_get(ctx, kSlotK1, bytes, &v1)) != GC_OK) return s;
+    if ((s = scratch_get(ctx, kSlotK2, bytes, &v2)) != GC_OK) return s;
+    if ((s = scratch_get(ctx, kSlotK3, bytes, &v3)) != GC_OK) return s;
+  }
+  T* pb = static_cast<T*>(vb);
+  T *k1 = static_cast<T*>(v1), *k2 = static_cast<T*>(v2), *k3 = static_cast<T*>(v3);
+  const uint64_t key[8] = {reinterpret_cast<uint64_t>(psi) ^ 0x1ULL,
+                           reinterpret_cast<uint64_t>(pb),
+                           reinterpret_cast<uint64_t>(k1) ^ (reinterpret_cast<uint64_t>(k3) << 1),
+                           (static_cast<uint64_t>(g->nx) << 40) ^ (static_cast<uint64_t>(g->ny) << 20) ^
+                               static_cast<uint64_t>(g->nz) ^ (bits_of(g->hx) * 3) ^ (bits_of(g->hy) * 5) ^
+                               (bits_of(g->hz) * 7),
+                           bits_of(dt),
+                           bits_of(cp->mobility),
+                           bits_of(cp->kappa),
+                           (static_cast<uint64_t>(cp->order) << 8) | (static_cast<uint64_t>(integ) << 4) |
+                               (sizeof(T) == 8 ? 1u : 2u) | (0xC4ULL << 56)};
+  return run_steps<T>(ctx, psi, pb, bytes, n_steps, key, [&](const T* src, T* dst) {
+    return enqueue_step<T>(ctx, g, cp, src, dst, k1, k2, k3, dt, integ);
+  });
+}
+
+gc_status check_ch(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (!cp) return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: null Cahn-Hilliard parameters");
+  if (cp->order != 2 && cp->order != 4 && cp->order != 6)
+    return fail(GC_ERR_UNSUPPORTED, "gridcalc_b200: Cahn-Hilliard order must be 2, 4 or 6; got " +
+                                        std::to_string(cp->order));
+  if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: unknown dtype");
+  return GC_OK;
+}
+
+}  // namespace
+}  // namespace gcb
+
+using namespace gcb;
+
+extern "C" {
+
+GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp,
+                           const void* psi, void* out) {
+  Call call(ctx);
+  if (call.st != GC_OK) return call.st;
+  gc_status s = check_ch(ctx, g, dt, cp);
+  if (s != GC_OK) return s;
+  if ((s = require_axes(g, cp->order / 2)) != GC_OK) return s;
+  if (!psi || !out) return fail(GC_ERR_INVALID_ARG, "gc_ch_rhs: null field pointer");
+  if (dt == GC_F64) {
+    StageParams<double> p = base_params<double>(g, cp);
+    p.psi = static_cast<const double*>(psi);
+    p.out = static_cast<double*>(out);
+    return launch_mode<double, MODE_RHS>(ctx, cp->order, p);
+  }
+  StageParams<float> p = base_params<float>(g, cp);
+  p.psi = static_cast<const float*>(psi);
+  p.out = static_cast<float*>(out);
+  return launch_mode<float, MODE_RHS>(ctx, cp->order, p);
+}
+
+GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
+                                 const gc_ch_params* cp, void* psi, double dt_step, int n_steps,
+                                 gc_integrator integ) {
+  Call call(ctx);
+  if (call.st != GC_OK) return call.st;
+  gc_status s = check_ch(ctx, g, dt, cp);
+  if (s != GC_OK) return s;
+  const char* who = integ == GC_RK4 ? "solve::integrate(... RK4)" : "solve::integrate(... ExplicitEuler)";
+  if (integ != GC_RK4 && integ != GC_EXPLICIT_EULER)
+    return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: unknown integrator");
+  if (n_steps < 0)
+    return fail(GC_ERR_INVALID_ARG, std::string(who) + ": n_steps must be >= 0; got " + std::to_string(n_steps));
+  if (dt_step < 0.0)
+    return fail(GC_ERR_INVALID_ARG, std::string(who) + ": dt must be >= 0; got " + std::to_string(dt_step));
+  if (n_steps == 0) return GC_OK;
+  if ((s = require_axes(g, cp->order / 2)) != GC_OK) return s;
+  if (!psi) return fail(GC_ERR_INVALID_ARG, "gc_ch_integrate: null psi");
+  if (dt == GC_F64)
+    return integrate_t<double>(ctx, g, cp, static_cast<double*>(psi), dt_step, n_steps, integ);
+  return integrate_t<float>(ctx, g, cp, static_cast<float*>(psi), dt_step, n_steps, integ);
+}
+
+}  // extern "C"

@@ -1,0 +1,240 @@
+// Shared device/host helpers for the gridcalc_b200 kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "gridcalc_b200.h"
+
+namespace gcb {
+
+// ---------------------------------------------------------------------------
+// Error plumbing: thread-local message + status (never throws across the ABI).
+void set_error(const std::string& msg);
+gc_status fail(gc_status s, const std::string& msg);
+gc_status cuda_fail(cudaError_t e, const char* what);
+
+#define GC_CUDA(call)                                            \
+  do {                                                           \
+    cudaError_t gc_e_ = (call);                                  \
+    if (gc_e_ != cudaSuccess) return ::gcb::cuda_fail(gc_e_, #call); \
+  } while (0)
+
+#define GC_CHECK_LAUNCH(what)                                    \
+  do {                                                           \
+    cudaError_t gc_e_ = cudaGetLastError();                      \
+    if (gc_e_ != cudaSuccess) return ::gcb::cuda_fail(gc_e_, what); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Context: stream + cached scratch.
+struct Scratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace gcb
+
+struct gc_context {
+  int device = 0;
+  // All work runs on `stream`, owned by the context (capturable); each call
+  // first waits for the caller's stream and makes the caller's stream wait
+  // for it on return, so the call is ordered like a launch on that stream.
+  cudaStream_t stream = nullptr;
+  cudaStream_t user_stream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  int num_sms = 148;
+  // Named scratch slots, grown on demand and kept for the context's life.
+  gcb::Scratch scratch[16];
+  // Pinned host word(s) for small device->host results.
+  void* host_pinned = nullptr;
+  // Small cache of captured step graphs, keyed by everything the captured
+  // kernels bake in; least recently used entry is replaced.
+  static constexpr int kGraphSlots = 6;
+  cudaGraphExec_t graph_exec[kGraphSlots] = {};
+  uint64_t graph_key[kGraphSlots][8] = {};
+  uint64_t graph_used[kGraphSlots] = {};
+  uint64_t graph_clock = 0;
+};
+
+namespace gcb {
+
+enum ScratchSlot {
+  kSlotK1 = 0,
+  kSlotK2,
+  kSlotK3,
+  kSlotPsiB,
+  kSlotReduce,
+  kSlotIntegrand,
+  kSlotFlags,
+  kSlotMisc,
+};
+
+gc_status scratch_get(gc_context* ctx, int slot, size_t bytes, void** out);
+
+// Validation helpers mirroring the reference contracts.
+gc_status check_grid(const gc_grid* g);
+gc_status require_axes(const gc_grid* g, int radius);
+gc_status check_ctx(gc_context* ctx);
+
+// Scope of one API call: validates the context, orders the context stream
+// after the caller's stream on entry and the caller's stream after the
+// context stream on exit.
+struct Call {
+  gc_context* ctx;
+  gc_status st;
+  explicit Call(gc_context* c);
+  ~Call();
+};
+inline size_t cells(const gc_grid* g) {
+  return static_cast<size_t>(g->nx) * static_cast<size_t>(g->ny) * static_cast<size_t>(g->nz);
+}
+inline size_t dtype_size(gc_dtype d) { return d == GC_F64 ? 8 : 4; }
+
+// ---------------------------------------------------------------------------
+// Arithmetic policy.  Double follows the reference exactly: every product
+// and sum is rounded on its own (__dmul_rn/__dadd_rn are never fused into
+// an FMA), so tap-by-tap accumulation reproduces the CPU result bit for bit.
+// Float is the precision variant: the compiler may contract into FMAs.
+template <class T>
+struct Ar;
+
+template <>
+struct Ar<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  // acc + w * x, rounded twice (no FMA).
+  static __device__ __forceinline__ double mac(double acc, double w, double x) {
+    return __dadd_rn(acc, __dmul_rn(w, x));
+  }
+};
+
+template <>
+struct Ar<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+  static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+  static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+  static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+  static __device__ __forceinline__ float mac(float acc, float w, float x) { return fmaf(w, x, acc); }
+};
+
+// Periodic wrap, ((i % N) + N) % N (reference core/IndexPolicy.hpp:28), with
+// a branch for the common in-range case.
+__device__ __forceinline__ int wrap(int i, int n) {
+  if (i >= 0 && i < n) return i;
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// ---------------------------------------------------------------------------
+// Stencil weight tables (unscaled), as compile-time constants.
+// Kind 1: first derivative; kind 2: second derivative; kind 4: fourth.
+// Orders 2 and 4 are the reference tables (stencil/CentralDifference.hpp:41-74,
+// stencil/FirstDerivative.hpp:51-86, stencil/FourthDerivative.hpp:49-83);
+// order 6 is the standard central-difference set (radius 3, 3, 4).
+template <int Kind, int Order>
+struct W;
+
+template <> struct W<2, 2> {
+  static constexpr int R = 1;
+  static __host__ __device__ constexpr double w(int m) { return m == 1 ? -2.0 : 1.0; }
+};
+template <> struct W<2, 4> {
+  static constexpr int R = 2;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 || m == 4 ? -1.0 / 12.0 : (m == 1 || m == 3 ? 4.0 / 3.0 : -5.0 / 2.0);
+  }
+};
+template <> struct W<2, 6> {
+  static constexpr int R = 3;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 || m == 6 ? 1.0 / 90.0
+         : m == 1 || m == 5 ? -3.0 / 20.0
+         : m == 2 || m == 4 ? 3.0 / 2.0
+                            : -49.0 / 18.0;
+  }
+};
+template <> struct W<1, 2> {
+  static constexpr int R = 1;
+  static __host__ __device__ constexpr double w(int m) { return m == 0 ? -0.5 : (m == 2 ? 0.5 : 0.0); }
+};
+template <> struct W<1, 4> {
+  static constexpr int R = 2;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 ? 1.0 / 12.0 : m == 1 ? -2.0 / 3.0 : m == 2 ? 0.0 : m == 3 ? 2.0 / 3.0 : -1.0 / 12.0;
+  }
+};
+template <> struct W<1, 6> {
+  static constexpr int R = 3;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 ? -1.0 / 60.0 : m == 1 ? 3.0 / 20.0 : m == 2 ? -3.0 / 4.0 : m == 3 ? 0.0
+         : m == 4 ? 3.0 / 4.0 : m == 5 ? -3.0 / 20.0 : 1.0 / 60.0;
+  }
+};
+template <> struct W<4, 2> {
+  static constexpr int R = 2;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 || m == 4 ? 1.0 : (m == 1 || m == 3 ? -4.0 : 6.0);
+  }
+};
+template <> struct W<4, 4> {
+  static constexpr int R = 3;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 || m == 6 ? -1.0 / 6.0
+         : m == 1 || m == 5 ? 2.0
+         : m == 2 || m == 4 ? -13.0 / 2.0
+                            : 28.0 / 3.0;
+  }
+};
+template <> struct W<4, 6> {
+  static constexpr int R = 4;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 || m == 8 ? 7.0 / 240.0
+         : m == 1 || m == 7 ? -2.0 / 5.0
+         : m == 2 || m == 6 ? 169.0 / 60.0
+         : m == 3 || m == 5 ? -122.0 / 15.0
+                            : 91.0 / 8.0;
+  }
+};
+
+// Weight as the storage type T (float tables are the double ones rounded).
+template <class T, int Kind, int Order>
+__device__ __forceinline__ T wt(int m) {
+  return static_cast<T>(W<Kind, Order>::w(m));
+}
+
+// True when the weight is exactly 1 (the product w*x == x needs no multiply).
+template <int Kind, int Order>
+__host__ __device__ constexpr bool unit_weight(int m) {
+  return W<Kind, Order>::w(m) == 1.0;
+}
+template <int Kind, int Order>
+__host__ __device__ constexpr bool zero_weight(int m) {
+  return W<Kind, Order>::w(m) == 0.0;
+}
+
+// Tap-ordered 1-D stencil sum over values v[0..2R] (v[m] = f(x + m - R)):
+// acc = ((w0 v0 + w1 v1) + ...) accumulated left to right, as the reference
+// loops `acc += w[m] * field(...)`.  Zero-weight taps are skipped (that only
+// changes the sign of an exactly-zero sum) and unit weights skip the multiply.
+template <class T, int Kind, int Order, class Get>
+__device__ __forceinline__ T tap_sum(Get get) {
+  constexpr int R = W<Kind, Order>::R;
+  T acc = T(0);
+#pragma unroll
+  for (int m = 0; m <= 2 * R; ++m) {
+    if (zero_weight<Kind, Order>(m)) continue;
+    const T v = get(m - R);
+    if (unit_weight<Kind, Order>(m)) acc = Ar<T>::add(acc, v);
+    else acc = Ar<T>::mac(acc, wt<T, Kind, Order>(m), v);
+  }
+  return acc;
+}
+
+inline int div_up(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace gcb

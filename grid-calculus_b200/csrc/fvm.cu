@@ -1,0 +1,322 @@
+// Finite-volume heterogeneous diffusion and the constant-D heat equation.
+//
+// RHS kinds:
+//   KIND_FVM  fvm::cellLaplacian (fvm/CellLaplacian.hpp:91-143):
+//             sum over axes of [D+ (psi+ - psi) - D- (psi - psi-)] / h^2 with
+//             harmonic-mean faces D = 2ab/(a+b) (fvm/CellLaplacian.hpp:48-50);
+//   KIND_LAP  diff::laplacian<2> (diff/Laplacian.hpp:44-75), the RHS of
+//             solve::diffuse(psi, double D, ...) (solve/Diffusion.hpp:106-111).
+// A stage kernel stages y = psi + a k_prev (and D) with a one-cell periodic
+// halo in shared memory and writes k_s, or psi' on the last stage; RK4 costs
+// 13 field passes plus 4 reads of D per step.  Face coefficients are formed
+// on the fly from the staged D (no face arrays in HBM).
+#include <algorithm>
+
+#include "common.cuh"
+#include "stepper.cuh"
+
+namespace gcb {
+
+gc_status d_max_face_any(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D, double* result);
+gc_status first_nonpositive(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D, long long* first);
+
+namespace {
+
+constexpr int kThreads = 256;
+enum RhsKind { KIND_FVM = 0, KIND_LAP = 1 };
+enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+
+template <class T>
+struct FvmParams {
+  const T* psi;
+  const T* kin;
+  T a;
+  T* out;
+  const T* D;
+  const T* k1;
+  const T* k2;
+  const T* k3;
+  T c6, c3;
+  T ihx2, ihy2, ihz2;
+  int nx, ny, nz;
+};
+
+template <bool Z3>
+struct FvmTile;
+template <> struct FvmTile<false> { static constexpr int TX = 64, TY = 16, TZ = 1; };
+template <> struct FvmTile<true> { static constexpr int TX = 32, TY = 16, TZ = 8; };
+
+template <class T>
+__device__ __forceinline__ T hmean(T a, T b) {
+  return Ar<T>::div(Ar<T>::mul(Ar<T>::mul(T(2), a), b), Ar<T>::add(a, b));
+}
+
+template <class T, int KIND, bool Z3, int MODE>
+__global__ void __launch_bounds__(kThreads) fvm_stage_kernel(const FvmParams<T> p) {
+  constexpr int TX = FvmTile<Z3>::TX, TY = FvmTile<Z3>::TY, TZ = FvmTile<Z3>::TZ;
+  constexpr int RZ = Z3 ? 1 : 0;
+  constexpr int YX = TX + 2, YY = TY + 2, YZ = TZ + 2 * RZ;
+  constexpr int YN = YX * YY * YZ, ON = TX * TY * TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ys = reinterpret_cast<T*>(smem_raw);
+  T* ds = ys + YN;
+
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+  const size_t plane = static_cast<size_t>(nx) * ny;
+
+  for (int e = threadIdx.x; e < YN; e += kThreads) {
+    const int ex = e % YX;
+    const int rest = e / YX;
+    const int ey = rest % YY;
+    const int ez = rest / YY;
+    const int gx = wrap(x0 - 1 + ex, nx);
+    const int gy = wrap(y0 - 1 + ey, ny);
+    const int gz = Z3 ? wrap(z0 - 1 + ez, nz) : 0;
+    const size_t gi = static_cast<size_t>(gz) * plane + static_cast<size_t>(gy) * nx + gx;
+    T v = __ldg(p.psi + gi);
+    if (p.kin) v = Ar<T>::add(v, Ar<T>::mul(p.a, __ldg(p.kin + gi)));
+    ys[e] = v;
+    if constexpr (KIND == KIND_FVM) ds[e] = __ldg(p.D + gi);
+  }
+  __syncthreads();
+
+  for (int e = threadIdx.x; e < ON; e += kThreads) {
+    const int ex = e % TX;
+    const int rest = e / TX;
+    const int ey = rest % TY;
+    const int ez = rest / TY;
+    const int gx = x0 + ex, gy = y0 + ey, gz = z0 + ez;
+    if (gx >= nx || gy >= ny || gz >= nz) continue;
+    const int c = ((ez + RZ) * YY + (ey + 1)) * YX + (ex + 1);
+    constexpr int SX = 1, SY = YX, SZ = Z3 ? YX * YY : 0;
+    const T pc = ys[c];
+    T rhs;
+    if constexpr (KIND == KIND_FVM) {
+      const T dc = ds[c];
+      const T dxp = hmean(dc, ds[c + SX]), dxm = hmean(ds[c - SX], dc);
+      const T dyp = hmean(dc, ds[c + SY]), dym = hmean(ds[c - SY], dc);
+      const T dzp = hmean(dc, ds[c + SZ]), dzm = hmean(ds[c - SZ], dc);
+      const T rx = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dxp, Ar<T>::sub(ys[c + SX], pc)),
+                                         Ar<T>::mul(dxm, Ar<T>::sub(pc, ys[c - SX]))), p.ihx2);
+      const T ry = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dyp, Ar<T>::sub(ys[c + SY], pc)),
+                                         Ar<T>::mul(dym, Ar<T>::sub(pc, ys[c - SY]))), p.ihy2);
+      const T rz = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dzp, Ar<T>::sub(ys[c + SZ], pc)),
+                                         Ar<T>::mul(dzm, Ar<T>::sub(pc, ys[c - SZ]))), p.ihz2);
+      rhs = Ar<T>::add(Ar<T>::add(rx, ry), rz);
+    } else {
+      const T ax = tap_sum<T, 2, 2>([&](int o) { return ys[c + o * SX]; });
+      const T ay = tap_sum<T, 2, 2>([&](int o) { return ys[c + o * SY]; });
+      const T az = tap_sum<T, 2, 2>([&](int o) { return ys[c + o * SZ]; });
+      rhs = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+    }
+    const size_t gi = static_cast<size_t>(gz) * plane + static_cast<size_t>(gy) * nx + gx;
+    if constexpr (MODE == MODE_RHS) {
+      p.out[gi] = rhs;
+    } else if constexpr (MODE == MODE_RK4_FINAL) {
+      const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
+      const T s23 = Ar<T>::add(__ldg(p.k2 + gi), __ldg(p.k3 + gi));
+      p.out[gi] = Ar<T>::add(__ldg(p.psi + gi), Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+    } else {
+      p.out[gi] = Ar<T>::add(pc, Ar<T>::mul(p.c6, rhs));
+    }
+  }
+}
+
+template <class T, int KIND, bool Z3, int MODE>
+gc_status launch_fvm(gc_context* ctx, const FvmParams<T>& p) {
+  using TL = FvmTile<Z3>;
+  constexpr int RZ = Z3 ? 1 : 0;
+  constexpr size_t yn = static_cast<size_t>(TL::TX + 2) * (TL::TY + 2) * (TL::TZ + 2 * RZ);
+  constexpr size_t smem = sizeof(T) * yn * (KIND == KIND_FVM ? 2 : 1);
+  auto kern = fvm_stage_kernel<T, KIND, Z3, MODE>;
+  if (smem > 48 * 1024) GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(div_up(p.nx, TL::TX), div_up(p.ny, TL::TY), Z3 ? div_up(p.nz, TL::TZ) : 1);
+  kern<<<grid, kThreads, smem, ctx->stream>>>(p);
+  GC_CHECK_LAUNCH("fvm_stage_kernel");
+  return GC_OK;
+}
+
+template <class T, int KIND, int MODE>
+gc_status launch_kind(gc_context* ctx, const FvmParams<T>& p) {
+  return p.nz > 1 ? launch_fvm<T, KIND, true, MODE>(ctx, p) : launch_fvm<T, KIND, false, MODE>(ctx, p);
+}
+
+template <class T>
+FvmParams<T> fvm_params(const gc_grid* g) {
+  FvmParams<T> p{};
+  p.nx = g->nx; p.ny = g->ny; p.nz = g->nz;
+  p.ihx2 = static_cast<T>(1.0 / (g->hx * g->hx));
+  p.ihy2 = static_cast<T>(1.0 / (g->hy * g->hy));
+  p.ihz2 = static_cast<T>(1.0 / (g->hz * g->hz));
+  return p;
+}
+
+template <class T, int KIND>
+gc_status enqueue_step(gc_context* ctx, const gc_grid* g, const T* D, const T* src, T* dst, T* k1,
+                       T* k2, T* k3, double dt, gc_integrator integ) {
+  FvmParams<T> p = fvm_params<T>(g);
+  p.psi = src;
+  p.D = D;
+  gc_status s;
+  if (integ == GC_EXPLICIT_EULER) {
+    p.out = dst;
+    p.c6 = static_cast<T>(dt);
+    return launch_kind<T, KIND, MODE_EULER_FINAL>(ctx, p);
+  }
+  const double half_dt = 0.5 * dt, sixth_dt = dt / 6.0, third_dt = dt / 3.0;
+  p.out = k1;
+  if ((s = launch_kind<T, KIND, MODE_RHS>(ctx, p)) != GC_OK) return s;
+  p.kin = k1; p.a = static_cast<T>(half_dt); p.out = k2;
+  if ((s = launch_kind<T, KIND, MODE_RHS>(ctx, p)) != GC_OK) return s;
+  p.kin = k2; p.out = k3;
+  if ((s = launch_kind<T, KIND, MODE_RHS>(ctx, p)) != GC_OK) return s;
+  p.kin = k3; p.a = static_cast<T>(dt); p.out = dst;
+  p.k1 = k1; p.k2 = k2; p.k3 = k3;
+  p.c6 = static_cast<T>(sixth_dt); p.c3 = static_cast<T>(third_dt);
+  return launch_kind<T, KIND, MODE_RK4_FINAL>(ctx, p);
+}
+
+template <class T, int KIND>
+gc_status diffuse_t(gc_context* ctx, const gc_grid* g, const T* D, T* psi, double dt, int n_steps,
+                    gc_integrator integ) {
+  const size_t bytes = cells(g) * sizeof(T);
+  void *vb = nullptr, *v1 = nullptr, *v2 = nullptr, *v3 = nullptr;
+  gc_status s;
+  if ((s = scratch_get(ctx, kSlotPsiB, bytes, &vb)) != GC_OK) return s;
+  if (integ == GC_RK4) {
+    if ((s = scratch_get(ctx, kSlotK1, bytes, &v1)) != GC_OK) return s;
+    if ((s = scratch_get(ctx, kSlotK2, bytes, &v2)) != GC_OK) return s;
+    if ((s = scratch_get(ctx, kSlotK3, bytes, &v3)) != GC_OK) return s;
+  }
+  T* pb = static_cast<T*>(vb);
+  T *k1 = static_cast<T*>(v1), *k2 = static_cast<T*>(v2), *k3 = static_cast<T*>(v3);
+  const uint64_t key[8] = {reinterpret_cast<uint64_t>(psi) ^ 0x2ULL,
+                           reinterpret_cast<uint64_t>(pb),
+                           reinterpret_cast<uint64_t>(k1) ^ (reinterpret_cast<uint64_t>(k3) << 1),
+                           (static_cast<uint64_t>(g->nx) << 40) ^ (static_cast<uint64_t>(g->ny) << 20) ^
+                               static_cast<uint64_t>(g->nz) ^ (bits_of(g->hx) * 3) ^ (bits_of(g->hy) * 5) ^
+                               (bits_of(g->hz) * 7),
+                           bits_of(dt),
+                           reinterpret_cast<uint64_t>(D),
+                           0,
+                           (static_cast<uint64_t>(KIND) << 8) | (static_cast<uint64_t>(integ) << 4) |
+                               (sizeof(T) == 8 ? 1u : 2u) | (0xD1ULL << 56)};
+  return run_steps<T>(ctx, psi, pb, bytes, n_steps, key, [&](const T* src, T* dst) {
+    return enqueue_step<T, KIND>(ctx, g, D, src, dst, k1, k2, k3, dt, integ);
+  });
+}
+
+gc_status cfl_check(const gc_grid* g, double D, double dt, gc_integrator integ) {
+  const double limit = integ == GC_RK4 ? 0.6963 : 0.5;
+  const double inv_sum = 1.0 / (g->hx * g->hx) + 1.0 / (g->hy * g->hy) + 1.0 / (g->hz * g->hz);
+  const double cfl = D * dt * inv_sum;
+  if (cfl > limit) {
+    return fail(GC_ERR_CFL, std::string("solve::diffuse: explicit-diffusion CFL violated for ") +
+                                (integ == GC_RK4 ? "RK4" : "ExplicitEuler") + ": D=" + std::to_string(D) +
+                                ", dt=" + std::to_string(dt) + ", h=(" + std::to_string(g->hx) + ", " +
+                                std::to_string(g->hy) + ", " + std::to_string(g->hz) +
+                                "); D*dt*(1/hx^2 + 1/hy^2 + 1/hz^2) = " + std::to_string(cfl) + " > " +
+                                std::to_string(limit));
+  }
+  return GC_OK;
+}
+
+gc_status d_positive(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D, int64_t* bad,
+                     const char* who) {
+  long long first = -1;
+  gc_status s = first_nonpositive(ctx, g, dt, D, &first);
+  if (s != GC_OK) return s;
+  if (first >= 0) {
+    double v = 0.0;
+    if (dt == GC_F64) {
+      GC_CUDA(cudaMemcpy(&v, static_cast<const double*>(D) + first, sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+      float f = 0.f;
+      GC_CUDA(cudaMemcpy(&f, static_cast<const float*>(D) + first, sizeof(float), cudaMemcpyDeviceToHost));
+      v = f;
+    }
+    if (bad) *bad = first;
+    return fail(GC_ERR_NONPOSITIVE_D,
+                std::string(who) + ": D must be strictly positive at every cell (the harmonic-mean face-D "
+                                   "averaging is undefined otherwise); first violation at flat index " +
+                    std::to_string(first) + " with D=" + std::to_string(v));
+  }
+  return GC_OK;
+}
+
+}  // namespace
+}  // namespace gcb
+
+using namespace gcb;
+
+extern "C" {
+
+GC_API gc_status gc_cell_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
+                                   const void* D, void* out, int64_t* bad_index) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = require_axes(g, 1)) != GC_OK) return s;
+  if (!psi || !D || !out) return fail(GC_ERR_INVALID_ARG, "gc_cell_laplacian: null field pointer");
+  if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gc_cell_laplacian: unknown dtype");
+  if ((s = d_positive(ctx, g, dt, D, bad_index, "fvm::cellLaplacian")) != GC_OK) return s;
+  if (dt == GC_F64) {
+    FvmParams<double> p = fvm_params<double>(g);
+    p.psi = static_cast<const double*>(psi);
+    p.D = static_cast<const double*>(D);
+    p.out = static_cast<double*>(out);
+    return launch_kind<double, KIND_FVM, MODE_RHS>(ctx, p);
+  }
+  FvmParams<float> p = fvm_params<float>(g);
+  p.psi = static_cast<const float*>(psi);
+  p.D = static_cast<const float*>(D);
+  p.out = static_cast<float*>(out);
+  return launch_kind<float, KIND_FVM, MODE_RHS>(ctx, p);
+}
+
+GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi, double D,
+                            double dt_step, int n_steps, gc_integrator integ) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (integ != GC_RK4 && integ != GC_EXPLICIT_EULER) return fail(GC_ERR_INVALID_ARG, "gc_diffuse: unknown integrator");
+  if (D < 0.0) return fail(GC_ERR_INVALID_ARG, "solve::diffuse: D must be >= 0; got " + std::to_string(D));
+  if (dt_step < 0.0) return fail(GC_ERR_INVALID_ARG, "solve::diffuse: dt must be >= 0; got " + std::to_string(dt_step));
+  if (n_steps < 0) return fail(GC_ERR_INVALID_ARG, "solve::diffuse: n_steps must be >= 0; got " + std::to_string(n_steps));
+  if ((s = cfl_check(g, D, dt_step, integ)) != GC_OK) return s;
+  if (n_steps == 0) return GC_OK;
+  if ((s = require_axes(g, 1)) != GC_OK) return s;
+  if (!psi) return fail(GC_ERR_INVALID_ARG, "gc_diffuse: null psi");
+  // The reference integrates lap(psi) with step D*dt (solve/Diffusion.hpp:106-111).
+  if (dt == GC_F64) return diffuse_t<double, KIND_LAP>(ctx, g, nullptr, static_cast<double*>(psi), D * dt_step, n_steps, integ);
+  if (dt == GC_F32) return diffuse_t<float, KIND_LAP>(ctx, g, nullptr, static_cast<float*>(psi), D * dt_step, n_steps, integ);
+  return fail(GC_ERR_INVALID_ARG, "gc_diffuse: unknown dtype");
+}
+
+GC_API gc_status gc_diffuse_fvm(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi, const void* D,
+                                double dt_step, int n_steps, gc_integrator integ, int64_t* bad_index) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (integ != GC_RK4 && integ != GC_EXPLICIT_EULER) return fail(GC_ERR_INVALID_ARG, "gc_diffuse_fvm: unknown integrator");
+  if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gc_diffuse_fvm: unknown dtype");
+  if (dt_step < 0.0) return fail(GC_ERR_INVALID_ARG, "solve::diffuse: dt must be >= 0; got " + std::to_string(dt_step));
+  if (n_steps < 0) return fail(GC_ERR_INVALID_ARG, "solve::diffuse: n_steps must be >= 0; got " + std::to_string(n_steps));
+  if (!psi || !D) return fail(GC_ERR_INVALID_ARG, "gc_diffuse_fvm: null field pointer");
+  double dmax = 0.0;
+  if ((s = d_max_face_any(ctx, g, dt, D, &dmax)) != GC_OK) return s;
+  if ((s = cfl_check(g, dmax, dt_step, integ)) != GC_OK) return s;
+  if (n_steps == 0) return GC_OK;
+  // cellLaplacian's own preconditions, checked once instead of on every RHS
+  // call: D is constant over the call (fvm/CellLaplacian.hpp:95-109).
+  if ((s = require_axes(g, 1)) != GC_OK) return s;
+  if ((s = d_positive(ctx, g, dt, D, bad_index, "solve::diffuse: fvm::cellLaplacian")) != GC_OK) return s;
+  if (dt == GC_F64)
+    return diffuse_t<double, KIND_FVM>(ctx, g, static_cast<const double*>(D), static_cast<double*>(psi), dt_step, n_steps, integ);
+  return diffuse_t<float, KIND_FVM>(ctx, g, static_cast<const float*>(D), static_cast<float*>(psi), dt_step, n_steps, integ);
+}
+
+}  // extern "C"

@@ -1,0 +1,444 @@
+// Integrals: func::integrate (pairwise / Kahan), func::evaluate integrands,
+// the largest harmonic face D, and the D > 0 precondition.
+//
+// Pairwise sum, reproduced exactly.  The reference sums recursively
+// (func/Integrate.hpp:65-74): a range of n > 64 values splits at n/2, a range
+// of n <= 64 is summed left to right from 0.0.  Every node at depth d has
+// n/2^d rounded down or up values, so the tree is cut in two layers:
+//   1. the first D levels split the field into 2^D "chunks" of at most 8192
+//      values (every node above them is larger than 64, so it is a plain
+//      split); one CTA stages a chunk in shared memory and walks the next
+//      levels down to per-thread nodes of at most 128 values, which a thread
+//      sums exactly as the reference's base case (one extra split when the
+//      node holds 65..128 values); the node sums are combined up the perfect
+//      binary tree they form;
+//   2. the 2^D chunk sums form a perfect binary tree too, reduced in groups
+//      of 1024 (a perfect subtree each) until one value is left.
+// Because every addition happens between the same two operands as in the
+// reference, the double result is bit-identical.  Staging: a chunk is
+// loaded with coalesced loads and stored padded by one double every 64, so
+// that the 32 lanes walking 64-value nodes hit distinct banks.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gcb {
+namespace {
+
+constexpr int kChunkMax = 8192;   // values per chunk (layer 1)
+constexpr int kNodeMax = 128;     // values per thread node
+constexpr int kSumThreads = 256;
+
+__host__ __device__ constexpr int padpos(int e) { return e + (e >> 6); }
+
+// [lo, hi) of node `idx` at depth `depth` below the range [lo, hi).
+__device__ __forceinline__ void descend(long long& lo, long long& hi, long long idx, int depth) {
+  for (int b = depth - 1; b >= 0; --b) {
+    const long long mid = lo + (hi - lo) / 2;
+    if ((idx >> b) & 1) lo = mid;
+    else hi = mid;
+  }
+}
+
+__device__ __forceinline__ double seq_sum(const double* s, int a, int b) {
+  double acc = 0.0;
+  for (int e = a; e < b; ++e) acc = __dadd_rn(acc, s[padpos(e)]);
+  return acc;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSumThreads) pairwise_chunks(const T* __restrict__ x, long long n,
+                                                               int depth, long long nchunks,
+                                                               double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = reinterpret_cast<double*>(smem_raw);                 // padded chunk
+  double* ns = s + padpos(kChunkMax) + 8;                           // node sums
+  for (long long c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    long long lo = 0, hi = n;
+    descend(lo, hi, c, depth);
+    const int len = static_cast<int>(hi - lo);
+    const T* src = x + lo;
+#pragma unroll 8
+    for (int e = threadIdx.x; e < len; e += kSumThreads) s[padpos(e)] = static_cast<double>(src[e]);
+    // Depth below the chunk at which every node holds <= kNodeMax values.
+    int d2 = 0;
+    while (((len + (1 << d2) - 1) >> d2) > kNodeMax) ++d2;
+    const int nodes = 1 << d2;
+    __syncthreads();
+    if (threadIdx.x < nodes) {
+      long long a = 0, b = len;
+      descend(a, b, threadIdx.x, d2);
+      const int m = static_cast<int>(b - a);
+      double v;
+      if (m <= 64) {
+        v = seq_sum(s, static_cast<int>(a), static_cast<int>(b));
+      } else {
+        const int h = m / 2;
+        v = __dadd_rn(seq_sum(s, static_cast<int>(a), static_cast<int>(a) + h),
+                      seq_sum(s, static_cast<int>(a) + h, static_cast<int>(b)));
+      }
+      ns[threadIdx.x] = v;
+    }
+    __syncthreads();
+    // Adjacent pairs (2i, 2i+1) at every level, as the recursion pairs them;
+    // read and write are separated by a barrier (in place would race).
+    for (int w = nodes >> 1; w >= 1; w >>= 1) {
+      double v = 0.0;
+      if (threadIdx.x < w) v = __dadd_rn(ns[2 * threadIdx.x], ns[2 * threadIdx.x + 1]);
+      __syncthreads();
+      if (threadIdx.x < w) ns[threadIdx.x] = v;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[c] = ns[0];
+    __syncthreads();
+  }
+}
+
+// Reduces each group of `group` (a power of two) consecutive values to one,
+// as a perfect binary tree.
+__global__ void __launch_bounds__(1024) tree_groups(const double* __restrict__ in, long long count,
+                                                    int group, double* __restrict__ out) {
+  __shared__ double t[1024];
+  const long long base = static_cast<long long>(blockIdx.x) * group;
+  for (int i = threadIdx.x; i < group; i += blockDim.x) t[i] = (base + i < count) ? in[base + i] : 0.0;
+  __syncthreads();
+  for (int w = group >> 1; w >= 1; w >>= 1) {
+    double v = 0.0;
+    if (threadIdx.x < w) v = __dadd_rn(t[2 * threadIdx.x], t[2 * threadIdx.x + 1]);
+    __syncthreads();
+    if (threadIdx.x < w) t[threadIdx.x] = v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = t[0];
+}
+
+// ---- deterministic compensated sum (GC_SUM_KAHAN) -------------------------
+// Each thread runs Neumaier's update over a fixed strided subset, then the
+// (sum, compensation) pairs merge up a fixed tree with an error-free
+// two-sum.  Grid and block sizes are constants, so the result does not
+// depend on the device.
+constexpr int kKahanBlocks = 1024;
+constexpr int kKahanThreads = 256;
+
+struct SumC { double s, c; };
+
+__device__ __forceinline__ SumC neumaier_add(SumC a, double v) {
+  const double t = __dadd_rn(a.s, v);
+  if (fabs(a.s) >= fabs(v)) a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, t), v));
+  else a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(v, t), a.s));
+  a.s = t;
+  return a;
+}
+
+__device__ __forceinline__ SumC merge(SumC a, SumC b) {
+  const double t = __dadd_rn(a.s, b.s);
+  const double bp = __dsub_rn(t, a.s);
+  const double err = __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, bp)), __dsub_rn(b.s, bp));
+  return SumC{t, __dadd_rn(__dadd_rn(a.c, b.c), err)};
+}
+
+template <class T>
+__global__ void __launch_bounds__(kKahanThreads) kahan_blocks(const T* __restrict__ x, long long n,
+                                                              double* __restrict__ out) {
+  __shared__ SumC sh[kKahanThreads];
+  SumC acc{0.0, 0.0};
+  const long long stride = static_cast<long long>(kKahanBlocks) * kKahanThreads;
+  for (long long i = static_cast<long long>(blockIdx.x) * kKahanThreads + threadIdx.x; i < n; i += stride)
+    acc = neumaier_add(acc, static_cast<double>(x[i]));
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = kKahanThreads / 2; w >= 1; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = merge(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = sh[0].s;
+    out[2 * blockIdx.x + 1] = sh[0].c;
+  }
+}
+
+__global__ void __launch_bounds__(1024) kahan_final(const double* __restrict__ in, double* __restrict__ out) {
+  __shared__ SumC sh[kKahanBlocks];
+  sh[threadIdx.x] = SumC{in[2 * threadIdx.x], in[2 * threadIdx.x + 1]};
+  __syncthreads();
+  for (int w = kKahanBlocks / 2; w >= 1; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = merge(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = __dadd_rn(sh[0].s, sh[0].c);
+}
+
+// ---- integrands (func/Functional.hpp:88-148 over cahn_hilliard.hpp:64-77) --
+template <class T>
+__global__ void integrand_kernel(const T* __restrict__ psi, int nx, int ny, int nz, double ihx,
+                                 double ihy, double ihz, int kind, double kappa,
+                                 double* __restrict__ out) {
+  const size_t n = static_cast<size_t>(nx) * ny * nz;
+  for (size_t c = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+       c += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const double p = static_cast<double>(psi[c]);
+    double f;
+    if (kind == GC_INTEGRAND_PSI) {
+      f = p;
+    } else if (kind == GC_INTEGRAND_PSI_SQUARED) {
+      f = __dmul_rn(p, p);
+    } else {
+      const int i = static_cast<int>(c % nx);
+      const size_t rest = c / nx;
+      const int j = static_cast<int>(rest % ny);
+      const int k = static_cast<int>(rest / ny);
+      const size_t row = static_cast<size_t>(nx);
+      const size_t plane = static_cast<size_t>(nx) * ny;
+      auto val = [&](int ii, int jj, int kk) {
+        return static_cast<double>(psi[static_cast<size_t>(wrap(kk, nz)) * plane +
+                                       static_cast<size_t>(wrap(jj, ny)) * row + wrap(ii, nx)]);
+      };
+      // Order-2 gradient, the reference's default (diff/Gradient.hpp:59-69).
+      const double dx = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i - 1, j, k)), __dmul_rn(0.5, val(i + 1, j, k))), ihx);
+      const double dy = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i, j - 1, k)), __dmul_rn(0.5, val(i, j + 1, k))), ihy);
+      const double dz = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i, j, k - 1)), __dmul_rn(0.5, val(i, j, k + 1))), ihz);
+      const double sq = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      if (kind == GC_INTEGRAND_GRAD_SQUARED) {
+        f = sq;
+      } else {
+        const double t1 = __dmul_rn(__dmul_rn(-0.5, p), p);
+        const double t2 = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.25, p), p), p), p);
+        const double t3 = __dmul_rn(__dmul_rn(0.5, kappa), sq);
+        f = __dadd_rn(__dadd_rn(t1, t2), t3);
+      }
+    }
+    out[c] = f;
+  }
+}
+
+// ---- largest harmonic face D (solve/Diffusion.hpp:187-207) -----------------
+template <class T>
+__global__ void d_max_face_kernel(const T* __restrict__ D, int nx, int ny, int nz,
+                                  unsigned long long* __restrict__ best_bits) {
+  const size_t n = static_cast<size_t>(nx) * ny * nz;
+  double m = 0.0;
+  for (size_t c = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+       c += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int i = static_cast<int>(c % nx);
+    const size_t rest = c / nx;
+    const int j = static_cast<int>(rest % ny);
+    const int k = static_cast<int>(rest / ny);
+    const int ip = i + 1 == nx ? 0 : i + 1, jp = j + 1 == ny ? 0 : j + 1, kp = k + 1 == nz ? 0 : k + 1;
+    const double dc = static_cast<double>(D[c]);
+    const double nb[3] = {static_cast<double>(D[c - i + ip]),
+                          static_cast<double>(D[c + static_cast<size_t>(jp - j) * nx]),
+                          static_cast<double>(D[c + (static_cast<long long>(kp) - k) * static_cast<long long>(nx) * ny])};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double f = __ddiv_rn(__dmul_rn(__dmul_rn(2.0, dc), nb[a]), __dadd_rn(dc, nb[a]));
+      if (f > m) m = f;  // NaN and non-positive faces never win, as in the reference
+    }
+  }
+  // Non-negative doubles order like their bit patterns.
+  if (m > 0.0) atomicMax(best_bits, static_cast<unsigned long long>(__double_as_longlong(m)));
+}
+
+// First flat index with !(D > 0) (fvm/CellLaplacian.hpp:100-109).
+template <class T>
+__global__ void first_nonpositive_kernel(const T* __restrict__ D, long long n,
+                                         unsigned long long* __restrict__ first) {
+  for (long long c = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+    if (!(static_cast<double>(D[c]) > 0.0)) {
+      atomicMin(first, static_cast<unsigned long long>(c));
+      return;
+    }
+  }
+}
+
+}  // namespace
+
+// Exact pairwise sum of n values on the context's stream; result on the host.
+template <class T>
+gc_status pairwise_sum(gc_context* ctx, const T* x, long long n, double* result) {
+  if (n == 0) {
+    *result = 0.0;
+    return GC_OK;
+  }
+  int depth = 0;
+  while (((n + (1LL << depth) - 1) >> depth) > kChunkMax) ++depth;
+  const long long nchunks = 1LL << depth;
+  // Partials: level buffers for the chunk sums and the group reductions.
+  const size_t need = sizeof(double) * static_cast<size_t>(nchunks + nchunks / 1024 + 64);
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotReduce, need, &buf);
+  if (s != GC_OK) return s;
+  double* a = static_cast<double*>(buf);
+  double* b = a + nchunks;
+  const size_t smem = sizeof(double) * (padpos(kChunkMax) + 8 + kNodeMax);
+  static bool attr_set[2] = {false, false};
+  auto kern = pairwise_chunks<T>;
+  if (!attr_set[sizeof(T) == 8]) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr_set[sizeof(T) == 8] = true;
+  }
+  const long long grid = std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3);
+  kern<<<static_cast<unsigned>(grid), kSumThreads, smem, ctx->stream>>>(x, n, depth, nchunks, a);
+  GC_CHECK_LAUNCH("pairwise_chunks");
+  long long count = nchunks;
+  double* src = a;
+  double* dst = b;
+  while (count > 1) {
+    const int group = static_cast<int>(std::min<long long>(count, 1024));
+    const long long blocks = count / group;
+    tree_groups<<<static_cast<unsigned>(blocks), 1024, 0, ctx->stream>>>(src, count, group, dst);
+    GC_CHECK_LAUNCH("tree_groups");
+    count = blocks;
+    std::swap(src, dst);
+  }
+  double* host = static_cast<double*>(ctx->host_pinned);
+  GC_CUDA(cudaMemcpyAsync(host, src, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  *result = host[0];
+  return GC_OK;
+}
+
+template <class T>
+gc_status kahan_sum(gc_context* ctx, const T* x, long long n, double* result) {
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotReduce, sizeof(double) * (2 * kKahanBlocks + 8), &buf);
+  if (s != GC_OK) return s;
+  double* part = static_cast<double*>(buf);
+  kahan_blocks<T><<<kKahanBlocks, kKahanThreads, 0, ctx->stream>>>(x, n, part);
+  GC_CHECK_LAUNCH("kahan_blocks");
+  kahan_final<<<1, kKahanBlocks, 0, ctx->stream>>>(part, part + 2 * kKahanBlocks);
+  GC_CHECK_LAUNCH("kahan_final");
+  double* host = static_cast<double*>(ctx->host_pinned);
+  GC_CUDA(cudaMemcpyAsync(host, part + 2 * kKahanBlocks, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  *result = host[0];
+  return GC_OK;
+}
+
+template gc_status pairwise_sum<double>(gc_context*, const double*, long long, double*);
+template gc_status pairwise_sum<float>(gc_context*, const float*, long long, double*);
+
+gc_status sum_any(gc_context* ctx, gc_dtype dt, const void* x, long long n, gc_sum sum,
+                  double* result) {
+  if (dt == GC_F64) {
+    const double* p = static_cast<const double*>(x);
+    return sum == GC_SUM_KAHAN ? kahan_sum(ctx, p, n, result) : pairwise_sum(ctx, p, n, result);
+  }
+  const float* p = static_cast<const float*>(x);
+  return sum == GC_SUM_KAHAN ? kahan_sum(ctx, p, n, result) : pairwise_sum(ctx, p, n, result);
+}
+
+gc_status d_max_face_any(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D, double* result) {
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotFlags, 64, &buf);
+  if (s != GC_OK) return s;
+  unsigned long long* bits = static_cast<unsigned long long*>(buf);
+  GC_CUDA(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), ctx->stream));
+  const int blocks = ctx->num_sms * 8;
+  if (dt == GC_F64)
+    d_max_face_kernel<double><<<blocks, 256, 0, ctx->stream>>>(static_cast<const double*>(D), g->nx, g->ny, g->nz, bits);
+  else
+    d_max_face_kernel<float><<<blocks, 256, 0, ctx->stream>>>(static_cast<const float*>(D), g->nx, g->ny, g->nz, bits);
+  GC_CHECK_LAUNCH("d_max_face_kernel");
+  unsigned long long* host = static_cast<unsigned long long*>(ctx->host_pinned);
+  GC_CUDA(cudaMemcpyAsync(host, bits, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::memcpy(result, &host[0], sizeof(double));
+  return GC_OK;
+}
+
+gc_status first_nonpositive(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D, long long* first) {
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotFlags, 64, &buf);
+  if (s != GC_OK) return s;
+  unsigned long long* word = static_cast<unsigned long long*>(buf) + 1;
+  GC_CUDA(cudaMemsetAsync(word, 0xff, sizeof(unsigned long long), ctx->stream));
+  const long long n = static_cast<long long>(cells(g));
+  const int blocks = ctx->num_sms * 8;
+  if (dt == GC_F64)
+    first_nonpositive_kernel<double><<<blocks, 256, 0, ctx->stream>>>(static_cast<const double*>(D), n, word);
+  else
+    first_nonpositive_kernel<float><<<blocks, 256, 0, ctx->stream>>>(static_cast<const float*>(D), n, word);
+  GC_CHECK_LAUNCH("first_nonpositive_kernel");
+  unsigned long long* host = static_cast<unsigned long long*>(ctx->host_pinned) + 1;
+  GC_CUDA(cudaMemcpyAsync(host, word, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  *first = host[0] == ~0ULL ? -1 : static_cast<long long>(host[0]);
+  return GC_OK;
+}
+
+gc_status evaluate_any(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
+                       const gc_integrand* f, gc_sum sum, double* result) {
+  const long long n = static_cast<long long>(cells(g));
+  const double vol = g->hx * g->hy * g->hz;
+  if (f->kind == GC_INTEGRAND_PSI && dt == GC_F64) {
+    double s = 0.0;
+    gc_status st = sum_any(ctx, dt, psi, n, sum, &s);
+    *result = vol * s;
+    return st;
+  }
+  void* buf = nullptr;
+  gc_status st = scratch_get(ctx, kSlotIntegrand, sizeof(double) * static_cast<size_t>(n), &buf);
+  if (st != GC_OK) return st;
+  double* integrand = static_cast<double*>(buf);
+  const int blocks = ctx->num_sms * 8;
+  if (dt == GC_F64)
+    integrand_kernel<double><<<blocks, 256, 0, ctx->stream>>>(static_cast<const double*>(psi), g->nx, g->ny, g->nz,
+                                                              1.0 / g->hx, 1.0 / g->hy, 1.0 / g->hz, f->kind, f->kappa, integrand);
+  else
+    integrand_kernel<float><<<blocks, 256, 0, ctx->stream>>>(static_cast<const float*>(psi), g->nx, g->ny, g->nz,
+                                                             1.0 / g->hx, 1.0 / g->hy, 1.0 / g->hz, f->kind, f->kappa, integrand);
+  GC_CHECK_LAUNCH("integrand_kernel");
+  double s = 0.0;
+  st = sum_any(ctx, GC_F64, integrand, n, sum, &s);
+  *result = vol * s;
+  return st;
+}
+
+}  // namespace gcb
+
+using namespace gcb;
+
+extern "C" {
+
+GC_API gc_status gc_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in,
+                              gc_sum sum, double* result) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (!in || !result) return fail(GC_ERR_INVALID_ARG, "gc_integrate: null pointer");
+  if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gc_integrate: unknown dtype");
+  double total = 0.0;
+  s = sum_any(ctx, dt, in, static_cast<long long>(cells(g)), sum, &total);
+  if (s != GC_OK) return s;
+  *result = (g->hx * g->hy * g->hz) * total;
+  return GC_OK;
+}
+
+GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
+                             const gc_integrand* f, gc_sum sum, double* result) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (!psi || !f || !result) return fail(GC_ERR_INVALID_ARG, "gc_evaluate: null pointer");
+  if (f->kind < GC_INTEGRAND_PSI || f->kind > GC_INTEGRAND_GRAD_SQUARED)
+    return fail(GC_ERR_INVALID_ARG, "gc_evaluate: unknown integrand kind");
+  if (f->kind >= GC_INTEGRAND_CH_FREE_ENERGY && (s = require_axes(g, 1)) != GC_OK) return s;
+  return evaluate_any(ctx, g, dt, psi, f, sum, result);
+}
+
+GC_API gc_status gc_d_max_face(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D,
+                               double* result) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (!D || !result) return fail(GC_ERR_INVALID_ARG, "gc_d_max_face: null pointer");
+  return d_max_face_any(ctx, g, dt, D, result);
+}
+
+}  // extern "C"

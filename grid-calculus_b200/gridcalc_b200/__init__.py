@@ -1,0 +1,367 @@
+"""Python mirror of the gridcalc hot-path API over the gridcalc_b200 C ABI.
+
+The reference (gridcalc 0.15.1) is header-only C++; its C++ drop-in lives in
+``grid-calculus_b200/include/gridcalc``.  This module exposes the same
+functions to Python callers (the tests and the benchmark) with the same names,
+argument meaning and error behaviour: a violated precondition raises
+``ValueError`` (the reference throws ``std::invalid_argument``) carrying the
+library's message.
+
+Device memory is a ``torch.Tensor`` on a CUDA device (float64 or float32,
+contiguous, i-fastest: shape ``(nz, ny, nx)``).  Every computation runs in
+``libgridcalc_b200.so``; there is no CPU path, and importing this module
+fails if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+__all__ = [
+    "lib", "Grid", "Context", "context", "GcError", "F64", "F32",
+    "Pairwise", "Kahan", "RK4", "ExplicitEuler", "CahnHilliardRhs",
+    "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
+    "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
+    "d_max_face", "version",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libgridcalc_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"gridcalc_b200: {LIB_PATH} is missing; build it with "
+        "`python grid-calculus_b200/build.py` (there is no CPU fallback)")
+
+lib = C.CDLL(LIB_PATH)
+
+F64, F32 = 0, 1
+GC_OK = 0
+STATUS = {
+    0: "GC_OK", 1: "GC_ERR_INVALID_ARG", 2: "GC_ERR_AXIS_EXTENT", 3: "GC_ERR_GRID_MISMATCH",
+    4: "GC_ERR_NONPOSITIVE_D", 5: "GC_ERR_CFL", 6: "GC_ERR_CUDA", 7: "GC_ERR_TIMEOUT",
+    8: "GC_ERR_NONFINITE", 9: "GC_ERR_UNSUPPORTED",
+}
+
+
+class gc_grid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double)]
+
+
+class gc_ch_params(C.Structure):
+    _fields_ = [("mobility", C.c_double), ("kappa", C.c_double), ("order", C.c_int32)]
+
+
+class gc_integrand(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("kappa", C.c_double)]
+
+
+_vp, _gp, _i32, _dbl = C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_double
+_SIGS = {
+    "gc_context_create": [C.POINTER(C.c_void_p), _i32, _vp],
+    "gc_context_destroy": [_vp],
+    "gc_synchronize": [_vp],
+    "gc_malloc": [_vp, C.c_size_t, C.POINTER(C.c_void_p)],
+    "gc_free": [_vp, _vp],
+    "gc_memcpy_h2d": [_vp, _vp, _vp, C.c_size_t],
+    "gc_memcpy_d2h": [_vp, _vp, _vp, C.c_size_t],
+    "gc_laplacian": [_vp, _gp, _i32, _i32, _vp, _vp],
+    "gc_gradient": [_vp, _gp, _i32, _i32, _vp, _vp],
+    "gc_divergence": [_vp, _gp, _i32, _i32, _vp, _vp],
+    "gc_biharmonic": [_vp, _gp, _i32, _i32, _vp, _vp],
+    "gc_cell_laplacian": [_vp, _gp, _i32, _vp, _vp, _vp, C.POINTER(C.c_int64)],
+    "gc_integrate": [_vp, _gp, _i32, _vp, _i32, C.POINTER(C.c_double)],
+    "gc_evaluate": [_vp, _gp, _i32, _vp, C.POINTER(gc_integrand), _i32, C.POINTER(C.c_double)],
+    "gc_ch_rhs": [_vp, _gp, _i32, C.POINTER(gc_ch_params), _vp, _vp],
+    "gc_ch_integrate": [_vp, _gp, _i32, C.POINTER(gc_ch_params), _vp, _dbl, _i32, _i32],
+    "gc_diffuse": [_vp, _gp, _i32, _vp, _dbl, _dbl, _i32, _i32],
+    "gc_diffuse_fvm": [_vp, _gp, _i32, _vp, _vp, _dbl, _i32, _i32, C.POINTER(C.c_int64)],
+    "gc_d_max_face": [_vp, _gp, _i32, _vp, C.POINTER(C.c_double)],
+}
+for _name, _args in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = C.c_int
+lib.gc_last_error.restype = C.c_char_p
+lib.gc_last_error.argtypes = []
+lib.gc_version.restype = C.c_char_p
+lib.gc_status_string.restype = C.c_char_p
+lib.gc_status_string.argtypes = [C.c_int]
+
+
+class GcError(ValueError):
+    """A precondition the reference enforces with std::invalid_argument, or a
+    device error.  ``status`` is the gc_status name."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = STATUS.get(status, str(status))
+
+
+def _check(status: int) -> None:
+    if status != GC_OK:
+        raise GcError(status, lib.gc_last_error().decode())
+
+
+def version() -> str:
+    return lib.gc_version().decode()
+
+
+@dataclass(frozen=True)
+class Grid:
+    """core::Grid (core/Grid.hpp:28-148): extents and per-axis cell size."""
+    nx: int
+    ny: int
+    nz: int
+    hx: float = 1.0
+    hy: float = 1.0
+    hz: float = 1.0
+
+    def __post_init__(self):
+        if self.nx <= 0 or self.ny <= 0 or self.nz <= 0:
+            raise ValueError(f"Grid: extents (Nx, Ny, Nz) must be > 0; got ({self.nx}, {self.ny}, {self.nz})")
+        if not (self.hx > 0 and self.hy > 0 and self.hz > 0):
+            raise ValueError(f"Grid: cell_size components must be > 0; got ({self.hx}, {self.hy}, {self.hz})")
+
+    @property
+    def size(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def shape(self) -> tuple:
+        return (self.nz, self.ny, self.nx)
+
+    @property
+    def cell_volume(self) -> float:
+        return self.hx * self.hy * self.hz
+
+    def c(self) -> gc_grid:
+        return gc_grid(self.nx, self.ny, self.nz, self.hx, self.hy, self.hz)
+
+
+class Context:
+    """A gc_context: one CUDA stream plus cached scratch and graphs."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = C.c_void_p()
+        _check(lib.gc_context_create(C.byref(h), device, stream))
+        self.handle = h
+        self.device = device
+
+    def synchronize(self) -> None:
+        _check(lib.gc_synchronize(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib.gc_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: Context | None = None
+
+
+def context() -> Context:
+    """The module's default context on the current CUDA device, bound to
+    torch's current stream."""
+    global _default
+    if _default is None:
+        import torch
+        # Enqueue on torch's current stream so that tensors produced by torch
+        # are complete before our kernels read them (stream order).
+        _default = Context(torch.cuda.current_device(), torch.cuda.current_stream().cuda_stream)
+    return _default
+
+
+# --- tags ---------------------------------------------------------------
+class Pairwise:  # func::Pairwise
+    code = 0
+
+
+class Kahan:  # func::Kahan
+    code = 1
+
+
+class RK4:  # solve::RK4
+    code = 1
+    diffusionCFLLimit = 0.6963
+
+
+class ExplicitEuler:  # solve::ExplicitEuler
+    code = 0
+    diffusionCFLLimit = 0.5
+
+
+@dataclass(frozen=True)
+class CahnHilliardRhs:
+    """Device RHS functor M lap(-psi + psi^3 - kappa lap psi)
+    (examples/common/cahn_hilliard.hpp:38-59) at Laplacian order 2, 4 or 6."""
+    mobility: float = 1.0
+    kappa: float = 1.0
+    order: int = 2
+
+    def c(self) -> gc_ch_params:
+        return gc_ch_params(self.mobility, self.kappa, self.order)
+
+
+# --- helpers ------------------------------------------------------------
+def _dtype_code(t) -> int:
+    import torch
+    if t.dtype == torch.float64:
+        return F64
+    if t.dtype == torch.float32:
+        return F32
+    raise ValueError(f"gridcalc_b200: fields must be float64 or float32, got {t.dtype}")
+
+
+def _require(t, grid: Grid, comps: int = 1):
+    if not t.is_cuda:
+        raise ValueError("gridcalc_b200: fields must live on a CUDA device")
+    if not t.is_contiguous():
+        raise ValueError("gridcalc_b200: fields must be contiguous")
+    if t.numel() != comps * grid.size:
+        raise ValueError(f"gridcalc_b200: field has {t.numel()} values, grid needs {comps * grid.size}")
+
+
+def _ctx(ctx):
+    return (ctx or context()).handle
+
+
+def _empty_like_grid(t, grid: Grid, comps: int = 1):
+    import torch
+    shape = grid.shape if comps == 1 else (comps,) + grid.shape
+    return torch.empty(shape, dtype=t.dtype, device=t.device)
+
+
+# --- diff:: -------------------------------------------------------------
+def laplacian(field, grid: Grid, order: int = 2, out=None, ctx=None):
+    """diff::laplacian<Order> (diff/Laplacian.hpp:44-75)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    _check(lib.gc_laplacian(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order,
+                            field.data_ptr(), out.data_ptr()))
+    return out
+
+
+def gradient(field, grid: Grid, order: int = 2, out=None, ctx=None):
+    """diff::gradient<Order> scalar -> vector (diff/Gradient.hpp:43-74); out
+    has shape (3, nz, ny, nx)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid, 3) if out is None else out
+    _check(lib.gc_gradient(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order,
+                           field.data_ptr(), out.data_ptr()))
+    return out
+
+
+def divergence(vfield, grid: Grid, order: int = 2, out=None, ctx=None):
+    """diff::divergence<Order> vector -> scalar (diff/Divergence.hpp:43-74)."""
+    _require(vfield, grid, 3)
+    out = _empty_like_grid(vfield, grid) if out is None else out
+    _check(lib.gc_divergence(_ctx(ctx), C.byref(grid.c()), _dtype_code(vfield), order,
+                             vfield.data_ptr(), out.data_ptr()))
+    return out
+
+
+def biharmonic(field, grid: Grid, order: int = 2, out=None, ctx=None):
+    """diff::biharmonic<Order> (diff/Biharmonic.hpp:48-104)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    _check(lib.gc_biharmonic(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order,
+                             field.data_ptr(), out.data_ptr()))
+    return out
+
+
+d4 = biharmonic  # diff::d4 (diff/Biharmonic.hpp:116-119)
+
+
+# --- fvm:: --------------------------------------------------------------
+def cell_laplacian(psi, D, grid: Grid, out=None, ctx=None):
+    """fvm::cellLaplacian (fvm/CellLaplacian.hpp:91-143)."""
+    _require(psi, grid)
+    _require(D, grid)
+    if D.dtype != psi.dtype:
+        raise ValueError("gridcalc_b200: psi and D must share a dtype")
+    out = _empty_like_grid(psi, grid) if out is None else out
+    bad = C.c_int64(-1)
+    _check(lib.gc_cell_laplacian(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), psi.data_ptr(),
+                                 D.data_ptr(), out.data_ptr(), C.byref(bad)))
+    return out
+
+
+# --- func:: -------------------------------------------------------------
+def integrate(field, grid: Grid, tag=Pairwise, ctx=None) -> float:
+    """func::integrate(field, Pairwise|Kahan) (func/Integrate.hpp:116-135)."""
+    _require(field, grid)
+    r = C.c_double()
+    _check(lib.gc_integrate(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                            tag.code, C.byref(r)))
+    return r.value
+
+
+INTEGRANDS = {"psi": 0, "psi_squared": 1, "ch_free_energy": 2, "grad_squared": 3}
+
+
+def evaluate(psi, grid: Grid, integrand: str, kappa: float = 0.0, tag=Pairwise, ctx=None) -> float:
+    """func::evaluate(psi, f, tag) (func/Functional.hpp:88-148) for the
+    integrands of the hot path: 'psi', 'psi_squared', 'ch_free_energy'
+    (-psi^2/2 + psi^4/4 + kappa/2 |grad psi|^2) and 'grad_squared'."""
+    _require(psi, grid)
+    f = gc_integrand(INTEGRANDS[integrand], kappa)
+    r = C.c_double()
+    _check(lib.gc_evaluate(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), psi.data_ptr(),
+                           C.byref(f), tag.code, C.byref(r)))
+    return r.value
+
+
+# --- solve:: ------------------------------------------------------------
+def ch_rhs(psi, grid: Grid, rhs: CahnHilliardRhs, out=None, ctx=None):
+    """One evaluation of the Cahn-Hilliard RHS (cahn_hilliard.hpp:38-59)."""
+    _require(psi, grid)
+    out = _empty_like_grid(psi, grid) if out is None else out
+    _check(lib.gc_ch_rhs(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), C.byref(rhs.c()),
+                         psi.data_ptr(), out.data_ptr()))
+    return out
+
+
+def ch_integrate(psi, grid: Grid, rhs: CahnHilliardRhs, dt: float, n_steps: int, tag=RK4, ctx=None):
+    """solve::integrate(psi, rhs, dt, n_steps, RK4|ExplicitEuler)
+    (solve/RK4.hpp:99-154) with the device Cahn-Hilliard RHS; psi in place."""
+    _require(psi, grid)
+    _check(lib.gc_ch_integrate(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), C.byref(rhs.c()),
+                               psi.data_ptr(), dt, n_steps, tag.code))
+    return psi
+
+
+def diffuse(psi, grid: Grid, D, dt: float, n_steps: int, tag=ExplicitEuler, ctx=None):
+    """solve::diffuse (solve/Diffusion.hpp:89-216): D a float (constant) or a
+    field (FVM, harmonic-mean faces); psi advanced in place."""
+    _require(psi, grid)
+    if isinstance(D, (int, float)):
+        _check(lib.gc_diffuse(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), psi.data_ptr(),
+                              float(D), dt, n_steps, tag.code))
+    else:
+        _require(D, grid)
+        if D.dtype != psi.dtype:
+            raise ValueError("gridcalc_b200: psi and D must share a dtype")
+        bad = C.c_int64(-1)
+        _check(lib.gc_diffuse_fvm(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), psi.data_ptr(),
+                                  D.data_ptr(), dt, n_steps, tag.code, C.byref(bad)))
+    return psi
+
+
+diffuse_fvm = diffuse
+
+
+def d_max_face(D, grid: Grid, ctx=None) -> float:
+    """Largest harmonic-mean face D (solve/Diffusion.hpp:187-207)."""
+    _require(D, grid)
+    r = C.c_double()
+    _check(lib.gc_d_max_face(_ctx(ctx), C.byref(grid.c()), _dtype_code(D), D.data_ptr(), C.byref(r)))
+    return r.value

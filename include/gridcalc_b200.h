@@ -1,0 +1,191 @@
+/* gridcalc_b200 — C ABI of the B200 (sm_100a) periodic-grid operator and
+ * time-stepping library.
+ *
+ * The reference gridcalc 0.15.1 is a header-only C++17 library with no FFI:
+ * its interface is templated free functions over core::Field<double>.  Each
+ * entry point below replaces one of those functions (cited per declaration)
+ * with a call over raw device buffers, so a C, C++, ctypes or any FFI caller
+ * can bind it; the C++ drop-in headers in grid-calculus_b200/include/gridcalc
+ * rebuild the reference signatures on top of it.
+ *
+ * Conventions
+ *  - Buffers are DEVICE pointers owned by the caller, laid out i-fastest:
+ *    cell (i, j, k) at i + Nx*(j + Ny*k) (reference core/Grid.hpp:132-137).
+ *    Vector fields are three consecutive planes (x, y, z components, N
+ *    values each), the coalescing-friendly layout; the C++ drop-in converts
+ *    from the reference's interleaved Field<Vec3d>.
+ *  - dtype selects the storage type of every field argument of a call:
+ *    GC_F64 (double) or GC_F32 (float).  F64 arithmetic follows the
+ *    reference tap order without FMA contraction; F32 computes stencils in
+ *    float and every integral (integrate, evaluate, mass, energy) in double.
+ *  - Work is stream-ordered with the caller's stream.  Calls that return a host
+ *    scalar or report a data-dependent error (integrate, evaluate, the D > 0
+ *    check, the CFL check of diffuse_fvm) synchronise that stream; the
+ *    others return after enqueueing.  gc_synchronize() waits for all work.
+ *  - Scratch is allocated on first use and kept by the context (cudaMalloc
+ *    happens only when a call needs more than the context already holds).
+ *  - No entry point throws.  A non-GC_OK status comes with a message from
+ *    gc_last_error() (thread-local) that carries the reference's wording:
+ *    "axis x|y|z" for extents, "flat index" for D <= 0, "solve::diffuse" for
+ *    CFL, "k1".."k4" never arise (device RHS functors cannot change grids).
+ *  - One context per host thread; a context is not thread-safe.
+ */
+#ifndef GRIDCALC_B200_H
+#define GRIDCALC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GC_API __attribute__((visibility("default")))
+#else
+#define GC_API
+#endif
+
+typedef enum gc_status {
+  GC_OK = 0,
+  GC_ERR_INVALID_ARG = 1,   /* std::invalid_argument in the reference */
+  GC_ERR_AXIS_EXTENT = 2,   /* diff/detail/PreconditionAxisExtent.hpp:64-79 */
+  GC_ERR_GRID_MISMATCH = 3, /* solve/detail/RhsGridCheck.hpp:42-64 */
+  GC_ERR_NONPOSITIVE_D = 4, /* fvm/CellLaplacian.hpp:100-109 */
+  GC_ERR_CFL = 5,           /* solve/Diffusion.hpp:45-59 */
+  GC_ERR_CUDA = 6,          /* a CUDA runtime call failed */
+  GC_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+  GC_ERR_NONFINITE = 8,     /* a non-finite value was detected in the state */
+  GC_ERR_UNSUPPORTED = 9    /* (order, dtype, shape) combination not built */
+} gc_status;
+
+typedef enum gc_dtype { GC_F64 = 0, GC_F32 = 1 } gc_dtype;
+
+/* func::Pairwise / func::Kahan (func/Integrate.hpp:43,52). */
+typedef enum gc_sum { GC_SUM_PAIRWISE = 0, GC_SUM_KAHAN = 1 } gc_sum;
+
+/* solve::ExplicitEuler / solve::RK4 tags (solve/ExplicitEuler.hpp:37-41,
+ * solve/RK4.hpp:30-35). */
+typedef enum gc_integrator { GC_EXPLICIT_EULER = 0, GC_RK4 = 1 } gc_integrator;
+
+/* core::Grid (core/Grid.hpp:28-148): extents and per-axis cell size. */
+typedef struct gc_grid {
+  int32_t nx, ny, nz;
+  double hx, hy, hz;
+} gc_grid;
+
+typedef struct gc_context gc_context;
+
+/* ---- context, errors, memory ------------------------------------------- */
+
+/* Creates a context on `device` for callers working on `stream` (a
+ * cudaStream_t; NULL = the default stream).  The context runs its kernels on
+ * a stream of its own (so that step sequences can be captured into CUDA
+ * graphs) and orders every call after prior work on `stream` and later work
+ * on `stream` after the call.  It owns its scratch (RK stage buffers,
+ * reduction partials, captured graphs). */
+GC_API gc_status gc_context_create(gc_context** out, int device, void* stream);
+GC_API gc_status gc_context_destroy(gc_context* ctx);
+GC_API gc_status gc_synchronize(gc_context* ctx);
+GC_API const char* gc_last_error(void);
+GC_API const char* gc_status_string(gc_status s);
+/* gridcalc::version() (include/gridcalc/version.hpp.in:16-18). */
+GC_API const char* gc_version(void);
+/* Device memory helpers for callers without a CUDA runtime binding. */
+GC_API gc_status gc_malloc(gc_context* ctx, size_t bytes, void** dev);
+GC_API gc_status gc_free(gc_context* ctx, void* dev);
+GC_API gc_status gc_memcpy_h2d(gc_context* ctx, void* dev, const void* host, size_t bytes);
+GC_API gc_status gc_memcpy_d2h(gc_context* ctx, void* host, const void* dev, size_t bytes);
+
+/* ---- operators (diff::, fvm::) ------------------------------------------ */
+
+/* diff::laplacian<Order> (diff/Laplacian.hpp:44-75); order 2, 4 or 6. */
+GC_API gc_status gc_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                              const void* in, void* out);
+/* diff::gradient<Order>, scalar -> vector (diff/Gradient.hpp:43-74). */
+GC_API gc_status gc_gradient(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                             const void* in, void* out3);
+/* diff::divergence<Order>, vector -> scalar (diff/Divergence.hpp:43-74). */
+GC_API gc_status gc_divergence(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                               const void* in3, void* out);
+/* diff::biharmonic<Order> / diff::d4 (diff/Biharmonic.hpp:48-119). */
+GC_API gc_status gc_biharmonic(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                               const void* in, void* out);
+/* fvm::cellLaplacian (fvm/CellLaplacian.hpp:91-143).  Checks D > 0 first;
+ * on violation returns GC_ERR_NONPOSITIVE_D and the first flat index in
+ * *bad_index (may be NULL). */
+GC_API gc_status gc_cell_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype dt,
+                                   const void* psi, const void* D, void* out,
+                                   int64_t* bad_index);
+
+/* ---- integrals (func::) -------------------------------------------------- */
+
+/* func::integrate(field, Pairwise|Kahan) (func/Integrate.hpp:116-135):
+ * cell volume times the sum.  GC_SUM_PAIRWISE reproduces the reference's
+ * recursive pairwise tree (base case 64) exactly, so F64 results are
+ * bit-identical; GC_SUM_KAHAN is a deterministic compensated parallel sum. */
+GC_API gc_status gc_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in,
+                              gc_sum sum, double* result);
+
+/* Integrands for func::evaluate (func/Functional.hpp:88-148), one per
+ * use of the reference's callable forms on the hot path. */
+typedef enum gc_integrand_kind {
+  GC_INTEGRAND_PSI = 0,             /* f(psi) = psi        (cahn_hilliard.hpp:111) */
+  GC_INTEGRAND_PSI_SQUARED = 1,     /* f(psi) = psi^2      (heterogeneous_diffusion.hpp:82) */
+  GC_INTEGRAND_CH_FREE_ENERGY = 2,  /* -psi^2/2 + psi^4/4 + kappa/2 |grad psi|^2 (cahn_hilliard.hpp:64-68) */
+  GC_INTEGRAND_GRAD_SQUARED = 3     /* |grad psi|^2        (cahn_hilliard.hpp:73-77) */
+} gc_integrand_kind;
+
+typedef struct gc_integrand {
+  int32_t kind;  /* gc_integrand_kind */
+  double kappa;  /* GC_INTEGRAND_CH_FREE_ENERGY only */
+} gc_integrand;
+
+/* func::evaluate(psi, f, tag): the integrand is formed on the device from
+ * psi and its order-2 gradient (the reference's default) and reduced in FP64. */
+GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
+                             const gc_integrand* f, gc_sum sum, double* result);
+
+/* ---- time integration (solve::) ----------------------------------------- */
+
+/* Cahn-Hilliard right-hand side M lap(-psi + psi^3 - kappa lap psi)
+ * (examples/common/cahn_hilliard.hpp:38-59) at Laplacian order 2, 4 or 6. */
+typedef struct gc_ch_params {
+  double mobility;
+  double kappa;
+  int32_t order;
+} gc_ch_params;
+
+/* One evaluation of the Cahn-Hilliard RHS (computeRhs). */
+GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt,
+                           const gc_ch_params* p, const void* psi, void* out);
+
+/* solve::integrate(psi, computeRhs, dt, n_steps, RK4|ExplicitEuler)
+ * (solve/RK4.hpp:99-154, solve/ExplicitEuler.hpp:79-112) with the
+ * Cahn-Hilliard RHS, psi advanced in place.  RK4 runs four fused stage
+ * kernels per step (each reads and writes every field once); the steps are
+ * replayed from a captured CUDA graph. */
+GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
+                                 const gc_ch_params* p, void* psi, double dt_step,
+                                 int n_steps, gc_integrator integrator);
+
+/* solve::diffuse(psi, double D, dt, n_steps, tag) (solve/Diffusion.hpp:89-112):
+ * constant-D heat equation with the order-2 Laplacian and the tag's CFL check. */
+GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi,
+                            double D, double dt_step, int n_steps, gc_integrator integrator);
+
+/* solve::diffuse(psi, Field D, dt, n_steps, tag) (solve/Diffusion.hpp:161-216):
+ * FVM heat equation.  The largest harmonic face D is found on the device,
+ * the CFL check and the D > 0 check run once before the first step. */
+GC_API gc_status gc_diffuse_fvm(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi,
+                                const void* D, double dt_step, int n_steps,
+                                gc_integrator integrator, int64_t* bad_index);
+
+/* Largest harmonic-mean face D over +x/+y/+z faces (solve/Diffusion.hpp:187-207). */
+GC_API gc_status gc_d_max_face(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D,
+                               double* result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRIDCALC_B200_H */

@@ -1,0 +1,76 @@
+/* CPU oracle for the gridcalc periodic-grid hot path: a plain-C restatement
+ * of the reference algorithms, used ONLY as test infrastructure (the parity
+ * checker in tests/, the smoke check, and the CPU baseline leg of bench.py).
+ * The product path never links or calls it.
+ *
+ * Every routine follows the reference arithmetic order tap by tap (no FMA
+ * contraction: build with -ffp-contract=off), so on identical inputs it
+ * reproduces the reference bit for bit; tests/test_oracle.py pins that
+ * against the reference compiled from its own headers and against the
+ * committed golden vectors in tests/golden/.
+ *
+ * Layout: i-fastest linear index i + Nx*(j + Ny*k) (core/Grid.hpp:132-137).
+ * Vector fields: three planes (x, y, z component), N values each.
+ * Order 6 has no reference counterpart (the reference specialises only
+ * orders 2 and 4); its weight tables are the standard central-difference
+ * ones and are pinned by the Taylor-moment and convergence tests instead.
+ *
+ * Return codes: 0 ok; 1 invalid argument (message via oc_last_error()).
+ */
+#ifndef GC_ORACLE_H
+#define GC_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char* oc_last_error(void);
+
+/* Stencil weight tables (unscaled).  kind: 1 = first derivative,
+ * 2 = second derivative, 3 = third derivative, 4 = fourth derivative.
+ * Returns the radius, or -1 for an unknown (kind, order); fills
+ * weights[0 .. 2*radius]. */
+int oc_weights(int kind, int order, double* weights);
+
+int oc_laplacian(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                 const double* in, double* out);
+int oc_gradient(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                const double* in, double* out3);
+int oc_divergence(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                  const double* in3, double* out);
+int oc_biharmonic(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                  const double* in, double* out);
+/* Returns 0, 1 (axis extent) or 2 (D not strictly positive; *bad_index set). */
+int oc_cell_laplacian(int nx, int ny, int nz, double hx, double hy, double hz,
+                      const double* psi, const double* D, double* out, int64_t* bad_index);
+
+double oc_sum_pairwise(const double* x, size_t n);
+double oc_sum_neumaier(const double* x, size_t n);
+double oc_integrate(int nx, int ny, int nz, double hx, double hy, double hz,
+                    const double* in, int kahan);
+
+int oc_ch_rhs(int order, double M, double kappa, int nx, int ny, int nz, double hx,
+              double hy, double hz, const double* psi, double* out);
+/* integrator: 0 = explicit Euler, 1 = RK4.  psi advanced in place. */
+int oc_ch_integrate(int order, double M, double kappa, int nx, int ny, int nz, double hx,
+                    double hy, double hz, double* psi, double dt, int n_steps, int integrator);
+double oc_ch_free_energy(int nx, int ny, int nz, double hx, double hy, double hz,
+                         const double* psi, double kappa);
+double oc_ch_gradient_energy(int nx, int ny, int nz, double hx, double hy, double hz,
+                             const double* psi);
+double oc_ch_mean(int nx, int ny, int nz, double hx, double hy, double hz, const double* psi);
+
+/* Largest harmonic-mean face D over the +x/+y/+z faces (solve/Diffusion.hpp:187-207). */
+double oc_d_max_face(int nx, int ny, int nz, const double* D);
+int oc_diffuse_const(int nx, int ny, int nz, double hx, double hy, double hz, double* psi,
+                     double D, double dt, int n_steps, int integrator);
+int oc_diffuse_fvm(int nx, int ny, int nz, double hx, double hy, double hz, double* psi,
+                   const double* D, double dt, int n_steps, int integrator);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,249 @@
+// Test infrastructure: a C harness over the reference gridcalc headers,
+// compiled from the reference tree where it lies (never copied) by
+// oracle/Makefile into oracle/_ref/libgcref.so.  It pins the C restatement
+// in oracle/gc_oracle.c and serves as the timed CPU baseline.  Nothing on
+// the product path links or loads it.
+//
+// Every function takes a raw buffer in the reference memory layout
+// (i fastest, core/Grid.hpp:132-137), builds a reference Field from it,
+// calls the reference function and copies the result out.  Vector fields
+// cross this boundary as three planes (x, y, z components, N values each).
+// std::invalid_argument is caught and turned into return code 1 with the
+// message available from ref_last_error().
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include <gridcalc/core/Field.hpp>
+#include <gridcalc/core/Grid.hpp>
+#include <gridcalc/diff/Biharmonic.hpp>
+#include <gridcalc/diff/Divergence.hpp>
+#include <gridcalc/diff/Gradient.hpp>
+#include <gridcalc/diff/Laplacian.hpp>
+#include <gridcalc/func/Functional.hpp>
+#include <gridcalc/func/Integrate.hpp>
+#include <gridcalc/fvm/CellLaplacian.hpp>
+#include <gridcalc/solve/Diffusion.hpp>
+#include <gridcalc/solve/Integrator.hpp>
+
+#include <common/cahn_hilliard.hpp>
+
+namespace {
+
+using gridcalc::core::Field;
+using gridcalc::core::Grid;
+using gridcalc::core::Vec3d;
+namespace ch = gridcalc::examples::cahn_hilliard;
+
+thread_local std::string g_err;
+
+Grid makeGrid(int nx, int ny, int nz, double hx, double hy, double hz) {
+  return Grid(nx, ny, nz, Vec3d(hx, hy, hz));
+}
+
+Field<double> load(const Grid& g, const double* p) {
+  Field<double> f(g);
+  std::memcpy(f.data(), p, sizeof(double) * g.getSize());
+  return f;
+}
+
+void store(const Field<double>& f, double* p) {
+  std::memcpy(p, f.data(), sizeof(double) * f.getSize());
+}
+
+template <class Fn>
+int guarded(Fn&& fn) {
+  try {
+    fn();
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_err = e.what();
+    return 1;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return 2;
+  }
+}
+
+// Cahn-Hilliard RHS at a selectable Laplacian order.  Order 2 calls the
+// reference function itself (examples/common/cahn_hilliard.hpp:38-59);
+// order 4 is the same three statements with laplacian<4>, because the
+// reference hard-codes the default order there.
+template <int Order>
+Field<double> chRhs(const Field<double>& psi, double M, double kappa) {
+  if constexpr (Order == 2) {
+    return ch::computeRhs(psi, M, kappa);
+  } else {
+    auto lap_psi = gridcalc::diff::laplacian<Order>(psi);
+    Field<double> mu(psi.getGrid());
+    const std::size_t n = psi.getSize();
+    const double* p_psi = psi.data();
+    const double* p_lap = lap_psi.data();
+    double* p_mu = mu.data();
+    for (std::size_t idx = 0; idx < n; ++idx) {
+      const double p = p_psi[idx];
+      p_mu[idx] = -p + p * p * p - kappa * p_lap[idx];
+    }
+    auto rhs = gridcalc::diff::laplacian<Order>(mu);
+    double* p_rhs = rhs.data();
+    for (std::size_t idx = 0; idx < n; ++idx) p_rhs[idx] *= M;
+    return rhs;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_err.c_str(); }
+
+int ref_laplacian(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                  const double* in, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, in);
+    if (order == 2) store(gridcalc::diff::laplacian<2>(f), out);
+    else if (order == 4) store(gridcalc::diff::laplacian<4>(f), out);
+    else throw std::invalid_argument("ref: laplacian order must be 2 or 4");
+  });
+}
+
+int ref_gradient(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                 const double* in, double* out3) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, in);
+    Field<Vec3d> r(g);
+    if (order == 2) r = gridcalc::diff::gradient<2>(f);
+    else if (order == 4) r = gridcalc::diff::gradient<4>(f);
+    else throw std::invalid_argument("ref: gradient order must be 2 or 4");
+    const std::size_t n = g.getSize();
+    for (std::size_t i = 0; i < n; ++i) {
+      const Vec3d& v = r.data()[i];
+      out3[i] = v(0);
+      out3[n + i] = v(1);
+      out3[2 * n + i] = v(2);
+    }
+  });
+}
+
+int ref_divergence(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                   const double* in3, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<Vec3d> v(g);
+    const std::size_t n = g.getSize();
+    for (std::size_t i = 0; i < n; ++i) v.data()[i] = Vec3d(in3[i], in3[n + i], in3[2 * n + i]);
+    if (order == 2) store(gridcalc::diff::divergence<2>(v), out);
+    else if (order == 4) store(gridcalc::diff::divergence<4>(v), out);
+    else throw std::invalid_argument("ref: divergence order must be 2 or 4");
+  });
+}
+
+int ref_biharmonic(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                   const double* in, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, in);
+    if (order == 2) store(gridcalc::diff::biharmonic<2>(f), out);
+    else if (order == 4) store(gridcalc::diff::biharmonic<4>(f), out);
+    else throw std::invalid_argument("ref: biharmonic order must be 2 or 4");
+  });
+}
+
+int ref_cell_laplacian(int nx, int ny, int nz, double hx, double hy, double hz,
+                       const double* psi, const double* D, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    store(gridcalc::fvm::cellLaplacian(load(g, psi), load(g, D)), out);
+  });
+}
+
+double ref_integrate(int nx, int ny, int nz, double hx, double hy, double hz,
+                     const double* in, int kahan) {
+  const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+  const Field<double> f = load(g, in);
+  return kahan ? gridcalc::func::integrate(f, gridcalc::func::Kahan{})
+               : gridcalc::func::integrate(f, gridcalc::func::Pairwise{});
+}
+
+int ref_ch_rhs(int order, double M, double kappa, int nx, int ny, int nz, double hx,
+               double hy, double hz, const double* psi, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, psi);
+    if (order == 2) store(chRhs<2>(f, M, kappa), out);
+    else if (order == 4) store(chRhs<4>(f, M, kappa), out);
+    else throw std::invalid_argument("ref: CH order must be 2 or 4");
+  });
+}
+
+// integrator: 0 = ExplicitEuler, 1 = RK4 (solve/ExplicitEuler.hpp:79,
+// solve/RK4.hpp:99).  psi is advanced in place.
+int ref_ch_integrate(int order, double M, double kappa, int nx, int ny, int nz, double hx,
+                     double hy, double hz, double* psi, double dt, int n_steps,
+                     int integrator) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<double> f = load(g, psi);
+    auto run = [&](auto rhs) {
+      if (integrator == 1) gridcalc::solve::integrate(f, rhs, dt, n_steps, gridcalc::solve::RK4{});
+      else gridcalc::solve::integrate(f, rhs, dt, n_steps, gridcalc::solve::ExplicitEuler{});
+    };
+    if (order == 2) run([&](const Field<double>& p) { return chRhs<2>(p, M, kappa); });
+    else if (order == 4) run([&](const Field<double>& p) { return chRhs<4>(p, M, kappa); });
+    else throw std::invalid_argument("ref: CH order must be 2 or 4");
+    store(f, psi);
+  });
+}
+
+double ref_ch_free_energy(int nx, int ny, int nz, double hx, double hy, double hz,
+                          const double* psi, double kappa) {
+  const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+  return ch::computeFreeEnergy(load(g, psi), kappa);
+}
+
+double ref_ch_gradient_energy(int nx, int ny, int nz, double hx, double hy, double hz,
+                              const double* psi) {
+  const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+  return ch::computeGradientEnergy(load(g, psi));
+}
+
+double ref_ch_mean(int nx, int ny, int nz, double hx, double hy, double hz, const double* psi) {
+  const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+  return ch::computeMean(load(g, psi));
+}
+
+void ref_make_random_ic(int nx, int ny, int nz, double hx, double hy, double hz,
+                        uint64_t seed, double amplitude, double* out) {
+  const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+  store(ch::makeRandomIc(g, seed, amplitude), out);
+}
+
+// Constant-D heat equation, solve/Diffusion.hpp:89-112.
+int ref_diffuse_const(int nx, int ny, int nz, double hx, double hy, double hz, double* psi,
+                      double D, double dt, int n_steps, int integrator) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<double> f = load(g, psi);
+    if (integrator == 1) gridcalc::solve::diffuse(f, D, dt, n_steps, gridcalc::solve::RK4{});
+    else gridcalc::solve::diffuse(f, D, dt, n_steps, gridcalc::solve::ExplicitEuler{});
+    store(f, psi);
+  });
+}
+
+// Heterogeneous-D FVM heat equation, solve/Diffusion.hpp:161-216.
+int ref_diffuse_fvm(int nx, int ny, int nz, double hx, double hy, double hz, double* psi,
+                    const double* D, double dt, int n_steps, int integrator) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<double> f = load(g, psi);
+    const Field<double> d = load(g, D);
+    if (integrator == 1) gridcalc::solve::diffuse(f, d, dt, n_steps, gridcalc::solve::RK4{});
+    else gridcalc::solve::diffuse(f, d, dt, n_steps, gridcalc::solve::ExplicitEuler{});
+    store(f, psi);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,170 @@
+"""ctypes access to the CPU oracle (test infrastructure).
+
+``oracle/liboracle.so`` is the plain-C restatement of the reference hot path
+(oracle/gc_oracle.c); ``oracle/_ref/libgcref.so`` is the reference headers
+themselves compiled from the reference tree (present only where that tree was
+available at build time).  Only tests, the smoke check and the benchmark's
+CPU-baseline leg use this module; it is never on the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_SO = os.path.join(ORACLE_DIR, "_ref", "libgcref.so")
+
+_P = C.POINTER(C.c_double)
+_d = C.c_double
+_i = C.c_int
+
+
+def _ensure_built() -> None:
+    src = os.path.join(ORACLE_DIR, "gc_oracle.c")
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, "liboracle.so"], check=True)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_P)
+
+
+class _Lib:
+    """Common numpy front end over either library (prefix oc_ or ref_)."""
+
+    def __init__(self, path: str, prefix: str):
+        self.lib = C.CDLL(path)
+        self.p = prefix
+        for nm in ("integrate", "ch_free_energy", "ch_gradient_energy", "ch_mean"):
+            getattr(self.lib, prefix + nm).restype = _d
+        err = getattr(self.lib, prefix + "last_error")
+        err.restype = C.c_char_p
+
+    def _f(self, name):
+        return getattr(self.lib, self.p + name)
+
+    def error(self) -> str:
+        return self._f("last_error")().decode()
+
+    def _g(self, shape, h):
+        nz, ny, nx = shape
+        return (nx, ny, nz, _d(h[0]), _d(h[1]), _d(h[2]))
+
+    def _rc(self, rc):
+        if rc != 0:
+            raise ValueError(self.error())
+
+    def op(self, name: str, order: int, f: np.ndarray, h=(1.0, 1.0, 1.0)) -> np.ndarray:
+        """laplacian / gradient / divergence / biharmonic on an (nz, ny, nx)
+        array (vector fields: (3, nz, ny, nx))."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        shape = f.shape[-3:]
+        out_shape = (3,) + shape if name == "gradient" else shape
+        out = np.zeros(out_shape)
+        self._rc(self._f(name)(order, *self._g(shape, h), _ptr(f), _ptr(out)))
+        return out
+
+    def cell_laplacian(self, psi, D, h=(1.0, 1.0, 1.0)):
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        out = np.zeros(psi.shape)
+        if self.p == "oc_":
+            bad = C.c_int64(-1)
+            self._rc(self._f("cell_laplacian")(*self._g(psi.shape, h), _ptr(psi), _ptr(D), _ptr(out), C.byref(bad)))
+        else:
+            self._rc(self._f("cell_laplacian")(*self._g(psi.shape, h), _ptr(psi), _ptr(D), _ptr(out)))
+        return out
+
+    def integrate(self, f, h=(1.0, 1.0, 1.0), kahan=False) -> float:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        return self._f("integrate")(*self._g(f.shape, h), _ptr(f), int(kahan))
+
+    def ch_rhs(self, order, M, kappa, psi, h=(1.0, 1.0, 1.0)):
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        out = np.zeros(psi.shape)
+        self._rc(self._f("ch_rhs")(order, _d(M), _d(kappa), *self._g(psi.shape, h), _ptr(psi), _ptr(out)))
+        return out
+
+    def ch_integrate(self, order, M, kappa, psi, dt, n_steps, rk4=True, h=(1.0, 1.0, 1.0)):
+        psi = np.array(psi, dtype=np.float64, order="C", copy=True)
+        self._rc(self._f("ch_integrate")(order, _d(M), _d(kappa), *self._g(psi.shape, h), _ptr(psi),
+                                         _d(dt), n_steps, int(rk4)))
+        return psi
+
+    def ch_free_energy(self, psi, kappa, h=(1.0, 1.0, 1.0)) -> float:
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        return self._f("ch_free_energy")(*self._g(psi.shape, h), _ptr(psi), _d(kappa))
+
+    def ch_gradient_energy(self, psi, h=(1.0, 1.0, 1.0)) -> float:
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        return self._f("ch_gradient_energy")(*self._g(psi.shape, h), _ptr(psi))
+
+    def ch_mean(self, psi, h=(1.0, 1.0, 1.0)) -> float:
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        return self._f("ch_mean")(*self._g(psi.shape, h), _ptr(psi))
+
+    def diffuse_const(self, psi, D, dt, n_steps, rk4=True, h=(1.0, 1.0, 1.0)):
+        psi = np.array(psi, dtype=np.float64, order="C", copy=True)
+        self._rc(self._f("diffuse_const")(*self._g(psi.shape, h), _ptr(psi), _d(D), _d(dt), n_steps, int(rk4)))
+        return psi
+
+    def diffuse_fvm(self, psi, D, dt, n_steps, rk4=True, h=(1.0, 1.0, 1.0)):
+        psi = np.array(psi, dtype=np.float64, order="C", copy=True)
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        self._rc(self._f("diffuse_fvm")(*self._g(psi.shape, h), _ptr(psi), _ptr(D), _d(dt), n_steps, int(rk4)))
+        return psi
+
+
+class Oracle(_Lib):
+    def __init__(self):
+        _ensure_built()
+        super().__init__(ORACLE_SO, "oc_")
+        self.lib.oc_sum_pairwise.restype = _d
+        self.lib.oc_sum_neumaier.restype = _d
+        self.lib.oc_d_max_face.restype = _d
+
+    def weights(self, kind: int, order: int):
+        buf = (C.c_double * 17)()
+        r = self.lib.oc_weights(kind, order, buf)
+        return None if r < 0 else np.array(buf[: 2 * r + 1])
+
+    def sum_pairwise(self, x) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.oc_sum_pairwise(_ptr(x), C.c_size_t(x.size))
+
+    def sum_neumaier(self, x) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.oc_sum_neumaier(_ptr(x), C.c_size_t(x.size))
+
+    def d_max_face(self, D) -> float:
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        nz, ny, nx = D.shape
+        return self.lib.oc_d_max_face(nx, ny, nz, _ptr(D))
+
+
+class Reference(_Lib):
+    def __init__(self):
+        super().__init__(REF_SO, "ref_")
+
+    def make_random_ic(self, shape, seed: int, amplitude: float, h=(1.0, 1.0, 1.0)):
+        out = np.zeros(shape)
+        self.lib.ref_make_random_ic(*self._g(shape, h), C.c_uint64(seed), _d(amplitude), _ptr(out))
+        return out
+
+
+def oracle() -> Oracle:
+    return Oracle()
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def reference() -> Reference:
+    return Reference()

@@ -1,0 +1,173 @@
+"""Cahn-Hilliard time stepping on the GPU against the oracle.
+
+The double path is bit-identical to the reference: RHS, RK4 and explicit
+Euler trajectories (golden vectors from the reference, plus the oracle on
+the plain-method workload: 128 x 128, dt = 0.01, 2000 RK4 steps).  The float
+path is compared with the double oracle and its error is stated in the
+assertion.  Physics acceptance follows test/cahn_hilliard_test.cpp:101-184.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.npz")
+
+
+def dev(a, dtype=None):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype or torch.float64)
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.double().cpu().numpy()
+
+
+def grid_of(gc, shape, h=(1.0, 1.0, 1.0)):
+    nz, ny, nx = shape
+    return gc.Grid(nx, ny, nz, *h)
+
+
+def uniform_ic(shape, seed, amp=0.05, mean=0.0):
+    """The plain-method initial condition: mean + U[-amp, amp] i.i.d.,
+    generated once on the host and fed identically to both sides."""
+    rng = np.random.default_rng(seed)
+    return mean + amp * (2.0 * rng.random(shape) - 1.0)
+
+
+def test_rhs_golden(gc):
+    golden = np.load(GOLDEN)
+    for name in sorted({k.split("/")[0] for k in golden.files if k.endswith("/f")}):
+        f, h = golden[f"{name}/f"], tuple(golden[f"{name}/h"])
+        for order in (2, 4):
+            got = host(gc.ch_rhs(dev(0.1 * f), grid_of(gc, f.shape, h), gc.CahnHilliardRhs(1.3, 0.7, order)))
+            assert np.array_equal(got, golden[f"{name}/ch_rhs{order}"]), (name, order)
+
+
+def test_trajectories_golden(gc):
+    golden = np.load(GOLDEN)
+    psi0 = golden["ch2d/psi0"]
+    g = grid_of(gc, psi0.shape)
+    for order in (2, 4):
+        t = dev(psi0)
+        gc.ch_integrate(t, g, gc.CahnHilliardRhs(1.0, 1.0, order), 0.01, 40, gc.RK4)
+        assert np.array_equal(host(t), golden[f"ch2d/rk4_order{order}"]), order
+        t = dev(psi0)
+        gc.ch_integrate(t, g, gc.CahnHilliardRhs(1.0, 1.0, order), 0.005, 40, gc.ExplicitEuler)
+        assert np.array_equal(host(t), golden[f"ch2d/euler_order{order}"]), order
+    p3 = golden["ch3d/psi0"]
+    t = dev(p3)
+    gc.ch_integrate(t, grid_of(gc, p3.shape), gc.CahnHilliardRhs(1.0, 0.5, 2), 0.005, 20, gc.RK4)
+    assert np.array_equal(host(t), golden["ch3d/rk4_order2"])
+
+
+def test_plain_method_128_bit_exact(gc, oracle):
+    """128 x 128, M = kappa = 1, order 2, dt = 0.01, 2000 RK4 steps, FP64:
+    every 500 steps the state is bit-identical to the oracle, and so are the
+    free energy (BASELINE convention F_ref + V/4) and the mass."""
+    shape = (1, 128, 128)
+    psi0 = uniform_ic(shape, 42)
+    g = grid_of(gc, shape)
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
+    t = dev(psi0)
+    cpu = psi0.copy()
+    mass0 = gc.integrate(t, g, gc.Kahan)
+    for _ in range(4):
+        gc.ch_integrate(t, g, rhs, 0.01, 500, gc.RK4)
+        cpu = oracle.ch_integrate(2, 1.0, 1.0, cpu, 0.01, 500)
+        assert np.array_equal(host(t), cpu)
+        assert gc.evaluate(t, g, "ch_free_energy", kappa=1.0) == oracle.ch_free_energy(cpu, 1.0)
+    assert abs(gc.integrate(t, g, gc.Kahan) - mass0) < 1e-10
+
+
+@pytest.mark.parametrize("order", [2, 4, 6])
+@pytest.mark.parametrize("steps", [1, 3, 66, 131])
+def test_rk4_orders_and_step_counts(gc, oracle, order, steps):
+    """Odd counts and counts beyond one captured graph (64 steps) exercise
+    graph replay, direct leftover steps and the final buffer copy."""
+    shape = (1, 40, 56)
+    psi0 = uniform_ic(shape, order * 100 + steps)
+    dt = {2: 0.01, 4: 0.005, 6: 0.004}[order]
+    t = dev(psi0)
+    gc.ch_integrate(t, grid_of(gc, shape), gc.CahnHilliardRhs(1.0, 1.0, order), dt, steps, gc.RK4)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 1.0, 1.0, psi0, dt, steps))
+
+
+def test_3d_and_anisotropic(gc, oracle):
+    shape = (12, 10, 14)
+    h = (0.9, 1.1, 1.3)
+    psi0 = uniform_ic(shape, 8)
+    for order, dt in ((2, 0.01), (4, 0.004)):
+        t = dev(psi0)
+        gc.ch_integrate(t, grid_of(gc, shape, h), gc.CahnHilliardRhs(0.8, 1.2, order), dt, 25, gc.RK4)
+        assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.2, psi0, dt, 25, h=h)), order
+
+
+def test_float32_error_vs_double_oracle(gc, oracle):
+    """FP32 storage and stencils: error against the FP64 oracle after 1000
+    steps of the plain method at 128 x 128 (t = 10), stated as relative L2."""
+    import torch
+    shape = (1, 128, 128)
+    psi0 = uniform_ic(shape, 42).astype(np.float32).astype(np.float64)
+    t = dev(psi0, torch.float32)
+    g = grid_of(gc, shape)
+    gc.ch_integrate(t, g, gc.CahnHilliardRhs(1.0, 1.0, 2), 0.01, 1000, gc.RK4)
+    want = oracle.ch_integrate(2, 1.0, 1.0, psi0, 0.01, 1000)
+    got = host(t)
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 1e-3, err
+    f_gpu = gc.evaluate(t, g, "ch_free_energy", kappa=1.0)
+    f_ref = oracle.ch_free_energy(want, 1.0)
+    v4 = g.size * g.cell_volume / 4.0
+    assert abs((f_gpu + v4) - (f_ref + v4)) / abs(f_ref + v4) < 1e-3
+
+
+def test_acceptance_3d_coarsening(gc, oracle):
+    """test/cahn_hilliard_test.cpp:95-184 restated: 24^3, dt = 0.02,
+    kappa = 0.5, amplitude 0.1 (mean removed), snapshots after 0, 500, 1000,
+    1500 and 2500 RK4 steps: F non-increasing (tolerance 1e-6 |F0| + 1e-9),
+    the gradient energy drops by more than 3 % between the last two
+    snapshots, the mean moves by less than 1e-10; and the final state is
+    bit-identical to the oracle."""
+    shape = (24, 24, 24)
+    psi0 = uniform_ic(shape, 42, amp=0.1)
+    psi0 -= psi0.mean()
+    g = grid_of(gc, shape)
+    t = dev(psi0)
+    rhs = gc.CahnHilliardRhs(1.0, 0.5, 2)
+    vol = g.size * g.cell_volume
+    F = [gc.evaluate(t, g, "ch_free_energy", kappa=0.5)]
+    E = [gc.evaluate(t, g, "grad_squared")]
+    m0 = gc.evaluate(t, g, "psi") / vol
+    for seg in (500, 500, 500, 1000):
+        gc.ch_integrate(t, g, rhs, 0.02, seg, gc.RK4)
+        F.append(gc.evaluate(t, g, "ch_free_energy", kappa=0.5))
+        E.append(gc.evaluate(t, g, "grad_squared"))
+    tol = 1e-6 * abs(F[0]) + 1e-9
+    assert all(b <= a + tol for a, b in zip(F, F[1:])), F
+    assert (E[3] - E[4]) / E[3] > 0.03, E
+    assert abs(gc.evaluate(t, g, "psi") / vol - m0) < 1e-10
+    assert np.array_equal(host(t), oracle.ch_integrate(2, 1.0, 0.5, psi0, 0.02, 2500))
+
+
+def test_constant_field_zero_rhs(gc):
+    """test/cahn_hilliard_test.cpp:47-58."""
+    g = gc.Grid(16, 16, 16)
+    t = dev(np.full(g.shape, 0.3))
+    out = host(gc.ch_rhs(t, g, gc.CahnHilliardRhs(1.0, 1.0, 2)))
+    assert np.abs(out).max() < 1e-12
+
+
+def test_errors(gc):
+    g = gc.Grid(16, 16, 1)
+    t = dev(np.zeros(g.shape))
+    with pytest.raises(ValueError, match="n_steps must be >= 0"):
+        gc.ch_integrate(t, g, gc.CahnHilliardRhs(), 0.01, -1, gc.RK4)
+    with pytest.raises(ValueError, match="dt must be >= 0"):
+        gc.ch_integrate(t, g, gc.CahnHilliardRhs(), -0.01, 1, gc.RK4)
+    with pytest.raises(ValueError, match="axis x"):
+        gc.ch_integrate(dev(np.zeros((1, 16, 4))), gc.Grid(4, 16, 1), gc.CahnHilliardRhs(order=4), 0.01, 1)
