@@ -127,6 +127,23 @@ GC_API gc_status gc_cell_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype d
 GC_API gc_status gc_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in,
                               gc_sum sum, double* result);
 
+/* Allocation-free variant of gc_integrate with the Pairwise tag (no
+ * counterpart in the reference, which has no device memory at all).  For
+ * callers that cannot allocate device memory: applications whose device
+ * memory belongs entirely to another allocator, plug-in hosts that only
+ * hand over buffers, loops that forbid allocation once running.  It needs
+ * no context: it runs on `stream` (a cudaStream_t, NULL = default stream)
+ * and writes cell volume times the exact pairwise sum (bit-identical to
+ * gc_integrate) to the device double *result_dev, stream-ordered, without
+ * synchronising.  Its scratch is a fixed 525 KB device array inside the
+ * library, held by every GPU that loads it until exit, which limits the
+ * field to 2^29 cells (larger fields get GC_ERR_INVALID_ARG).  All calls
+ * share that array: calls that overlap on the GPU race, so keep them on one
+ * stream.  The first call on each device (with that device current) looks
+ * up the array's device address; make it before any stream capture. */
+GC_API gc_status gc_integrate_noalloc(const gc_grid* g, gc_dtype dt, const void* in,
+                                      double* result_dev, void* stream);
+
 /* Integrands for func::evaluate (func/Functional.hpp:88-148), one per
  * use of the reference's callable forms on the hot path. */
 typedef enum gc_integrand_kind {
