@@ -174,7 +174,7 @@ def run_ours(args, rank: int, world: int, local: int):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    g = gc.Grid(NX, NY, 1)
+    g = gc.Grid(args.grid, args.grid, 1)
     rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
     rng = np.random.default_rng(1000 + rank)
     psi0 = 0.05 * (2.0 * rng.random(g.shape) - 1.0)
@@ -249,7 +249,7 @@ def run_ours(args, rank: int, world: int, local: int):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "ch2d-rk4-fp64-order2", "grid": f"{NX}x{NY}", "dt": DT, "kappa": 1.0,
+            "config": {"workload": "ch2d-rk4-fp64-order2", "grid": f"{g.nx}x{g.ny}", "dt": DT, "kappa": 1.0,
                        "mobility": 1.0, "ic": "U[-0.05,0.05] seeded", "l2": "fields 512 MiB each > L2 (no flush)",
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -275,6 +275,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -149,13 +149,163 @@ gc_status launch_stage(gc_context* ctx, const StageParams<T>& p) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// 2-D stage kernel (Nz == 1), the production path of the plain method.
+// The three phases of the generic kernel above, arranged so that shared
+// memory carries only what must cross threads.  64 x 4 threads; the mu
+// region is exactly 64 columns wide (output tile 64 - 2R columns by 16
+// rows).  In phases 2 and 3 a thread owns one column and a strip of
+// consecutive rows: the y-direction taps come from a register window of
+// its own column (one new shared-memory value per row), only the x taps
+// are read from neighbouring columns.  In double precision every
+// warp-wide shared read is two wavefronts, and this layout halves the
+// shared-memory reads per cell, which bound the earlier layout.  Wrapped
+// columns are formed once per thread, wrapped rows once per row.  In the
+// last RK4 stage the k1 and k2 lines of the tile are prefetched into L2 at
+// the start.
+constexpr int kT2W = 64;   // mu-region columns = threads in x
+constexpr int kT2Y = 16;   // output rows
+constexpr int kT2TY = 4;   // thread rows
+
+template <class T, int ORDER, int MODE>
+__global__ void __launch_bounds__(kT2W * kT2TY) ch_tile2d_kernel(const StageParams<T> p) {
+  constexpr int R = W<2, ORDER>::R;
+  constexpr int TX = kT2W - 2 * R, TY = kT2Y, NTY = kT2TY;
+  constexpr int YX = TX + 4 * R, YY = TY + 4 * R;   // y region (tile + 2R halo)
+  constexpr int MX = kT2W, MY = TY + 2 * R;         // mu region (tile + R halo)
+  constexpr int NW = 2 * R + 1;
+  constexpr int MS = (MY + NTY - 1) / NTY;          // mu rows per thread strip
+  constexpr int OS = TY / NTY;                      // output rows per thread strip
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T (*ys)[YX] = reinterpret_cast<T (*)[YX]>(smem_raw);
+  T (*ms)[MX] = reinterpret_cast<T (*)[MX]>(smem_raw + sizeof(T) * YX * YY);
+
+  const int nx = p.nx, ny = p.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+
+  if constexpr (MODE == MODE_RK4_FINAL) {
+    if (tx < TX && x0 + tx < nx) {
+#pragma unroll
+      for (int k = 0; k < OS; ++k) {
+        const int oy = ty * OS + k;
+        if (y0 + oy < ny) {
+          const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k1 + gi));
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k2 + gi));
+        }
+      }
+    }
+  }
+
+  // Phase 1: y = psi + a k_prev on the tile + 2R halo (YX = 64 + 2R columns).
+  const int gxa = wrap(x0 - 2 * R + tx, nx);
+  const bool has_b = tx < YX - kT2W;
+  const int gxb = wrap(x0 - 2 * R + kT2W + tx, nx);
+  const bool has_kin = p.kin != nullptr;
+#pragma unroll
+  for (int ry = ty; ry < YY; ry += NTY) {
+    const size_t row = static_cast<size_t>(wrap(y0 - 2 * R + ry, ny)) * nx;
+    T v = __ldg(p.psi + row + gxa);
+    if (has_kin) v = Ar<T>::add(v, Ar<T>::mul(p.a, __ldg(p.kin + row + gxa)));
+    ys[ry][tx] = v;
+    if (has_b) {
+      T w = __ldg(p.psi + row + gxb);
+      if (has_kin) w = Ar<T>::add(w, Ar<T>::mul(p.a, __ldg(p.kin + row + gxb)));
+      ys[ry][kT2W + tx] = w;
+    }
+  }
+  __syncthreads();
+
+  // Phase 2: mu at mu-row strip [m0, m1), column tx (y column tx + R).
+  {
+    const int m0 = ty * MS;
+    const int m1 = min(m0 + MS, MY);
+    const int cx = tx + R;
+    T win[NW];  // y at rows m .. m + 2R (y space), column cx
+#pragma unroll
+    for (int k = 0; k < 2 * R; ++k) win[k + 1] = ys[m0 + k][cx];
+#pragma unroll
+    for (int k = 0; k < MS; ++k) {
+      const int m = m0 + k;
+      if (m < m1) {
+#pragma unroll
+        for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
+        win[NW - 1] = ys[m + 2 * R][cx];
+        const T yc = win[R];
+        const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? yc : ys[m + R][cx + o]; });
+        const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+        T lap = Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+        if constexpr (ORDER != 2) {
+          // Degenerate z axis: the z taps all read the centre value.
+          lap = Ar<T>::add(lap, Ar<T>::mul(tap_sum<T, 2, ORDER>([&](int) { return yc; }), p.ihz2));
+        }
+        ms[m][tx] = Ar<T>::sub(Ar<T>::add(-yc, Ar<T>::mul(Ar<T>::mul(yc, yc), yc)), Ar<T>::mul(p.kappa, lap));
+      }
+    }
+  }
+  __syncthreads();
+
+  // Phase 3: k_s = M lap(mu) at output-row strip [o0, o0 + OS), column tx.
+  if (tx >= TX || x0 + tx >= nx) return;
+  const int o0 = ty * OS;
+  const int cx = tx + R;
+  T win[NW];  // mu at rows o .. o + 2R (mu space), column cx
+#pragma unroll
+  for (int k = 0; k < 2 * R; ++k) win[k + 1] = ms[o0 + k][cx];
+#pragma unroll
+  for (int k = 0; k < OS; ++k) {
+    const int oy = o0 + k;
+#pragma unroll
+    for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
+    win[NW - 1] = ms[oy + 2 * R][cx];
+    if (y0 + oy >= ny) break;
+    const T mc = win[R];
+    const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? mc : ms[oy + R][cx + o]; });
+    const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+    T lap = Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+    if constexpr (ORDER != 2) {
+      lap = Ar<T>::add(lap, Ar<T>::mul(tap_sum<T, 2, ORDER>([&](int) { return mc; }), p.ihz2));
+    }
+    const T rhs = Ar<T>::mul(lap, p.mob);
+    const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
+    if constexpr (MODE == MODE_RHS) {
+      p.out[gi] = rhs;
+    } else if constexpr (MODE == MODE_RK4_FINAL) {
+      const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
+      const T s23 = Ar<T>::add(__ldg(p.k2 + gi), __ldg(p.k3 + gi));
+      p.out[gi] = Ar<T>::add(__ldg(p.psi + gi), Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+    } else {
+      p.out[gi] = Ar<T>::add(ys[oy + 2 * R][tx + 2 * R], Ar<T>::mul(p.c6, rhs));
+    }
+  }
+}
+
+template <class T, int ORDER, int MODE>
+gc_status launch_tile2d(gc_context* ctx, const StageParams<T>& p) {
+  constexpr int R = W<2, ORDER>::R;
+  constexpr int TX = kT2W - 2 * R;
+  constexpr size_t smem = sizeof(T) * (static_cast<size_t>(TX + 4 * R) * (kT2Y + 4 * R) +
+                                       static_cast<size_t>(kT2W) * (kT2Y + 2 * R));
+  auto kern = ch_tile2d_kernel<T, ORDER, MODE>;
+  static bool attr = false;  // one instantiation per (T, ORDER, MODE)
+  if (!attr) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr = true;
+  }
+  dim3 grid(div_up(p.nx, TX), div_up(p.ny, kT2Y), 1), block(kT2W, kT2TY);
+  kern<<<grid, block, smem, ctx->stream>>>(p);
+  GC_CHECK_LAUNCH("ch_tile2d_kernel");
+  return GC_OK;
+}
+
 template <class T, int MODE>
 gc_status launch_mode(gc_context* ctx, int order, const StageParams<T>& p) {
   const bool z3 = p.nz > 1;
   switch (order) {
-    case 2: return z3 ? launch_stage<T, 2, true, MODE>(ctx, p) : launch_stage<T, 2, false, MODE>(ctx, p);
-    case 4: return z3 ? launch_stage<T, 4, true, MODE>(ctx, p) : launch_stage<T, 4, false, MODE>(ctx, p);
-    case 6: return z3 ? launch_stage<T, 6, true, MODE>(ctx, p) : launch_stage<T, 6, false, MODE>(ctx, p);
+    case 2: return z3 ? launch_stage<T, 2, true, MODE>(ctx, p) : launch_tile2d<T, 2, MODE>(ctx, p);
+    case 4: return z3 ? launch_stage<T, 4, true, MODE>(ctx, p) : launch_tile2d<T, 4, MODE>(ctx, p);
+    case 6: return z3 ? launch_stage<T, 6, true, MODE>(ctx, p) : launch_tile2d<T, 6, MODE>(ctx, p);
   }
   return fail(GC_ERR_UNSUPPORTED, "gridcalc_b200: Cahn-Hilliard order must be 2, 4 or 6");
 }
