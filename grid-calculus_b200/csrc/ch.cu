@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "stepper.cuh"
+#include "tma.cuh"
 
 namespace gcb {
 namespace {
@@ -44,7 +45,29 @@ struct StageParams {
   T mob, kappa;
   T ihx2, ihy2, ihz2;
   int nx, ny, nz;
+  // Exact shortcuts: x * 1 == x, so a unit spacing, mobility or kappa
+  // skips its multiply without changing a bit.
+  bool unit_h, unit_m, unit_k;
 };
+
+// (ax / hx^2 + ay / hy^2) [+ az / hz^2], as the reference combines the axes.
+template <class T>
+__device__ __forceinline__ T lap_xy(const StageParams<T>& p, T ax, T ay) {
+  return p.unit_h ? Ar<T>::add(ax, ay) : Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+}
+template <class T>
+__device__ __forceinline__ T lap_z(const StageParams<T>& p, T lap, T az) {
+  return Ar<T>::add(lap, p.unit_h ? az : Ar<T>::mul(az, p.ihz2));
+}
+// mu = -y + y^3 - kappa lap(y)
+template <class T>
+__device__ __forceinline__ T chem_pot(const StageParams<T>& p, T y, T lap) {
+  return Ar<T>::sub(Ar<T>::add(-y, Ar<T>::mul(Ar<T>::mul(y, y), y)), p.unit_k ? lap : Ar<T>::mul(p.kappa, lap));
+}
+template <class T>
+__device__ __forceinline__ T mobility(const StageParams<T>& p, T lap) {
+  return p.unit_m ? lap : Ar<T>::mul(lap, p.mob);
+}
 
 template <class T, int ORDER, bool Z3>
 struct Tile;
@@ -99,9 +122,9 @@ __global__ void __launch_bounds__(kThreads) ch_stage_kernel(const StageParams<T>
     const T ax = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + o]; });
     const T ay = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + o * YX]; });
     const T az = tap_sum<T, 2, ORDER>([&](int o) { return ys[c + (Z3 ? o : 0) * YX * YY]; });
-    const T lap = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+    const T lap = lap_z(p, lap_xy(p, ax, ay), az);
     const T y = ys[c];
-    ms[e] = Ar<T>::sub(Ar<T>::add(-y, Ar<T>::mul(Ar<T>::mul(y, y), y)), Ar<T>::mul(p.kappa, lap));
+    ms[e] = chem_pot(p, y, lap);
   }
   __syncthreads();
 
@@ -117,8 +140,8 @@ __global__ void __launch_bounds__(kThreads) ch_stage_kernel(const StageParams<T>
     const T ax = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + o]; });
     const T ay = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + o * MX]; });
     const T az = tap_sum<T, 2, ORDER>([&](int o) { return ms[c + (Z3 ? o : 0) * MX * MY]; });
-    const T lap = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
-    const T rhs = Ar<T>::mul(lap, p.mob);
+    const T lap = lap_z(p, lap_xy(p, ax, ay), az);
+    const T rhs = mobility(p, lap);
     const size_t gi = static_cast<size_t>(gz) * plane + static_cast<size_t>(gy) * nx + gx;
     if constexpr (MODE == MODE_RHS) {
       p.out[gi] = rhs;
@@ -235,12 +258,12 @@ __global__ void __launch_bounds__(kT2W * kT2TY) ch_tile2d_kernel(const StagePara
         const T yc = win[R];
         const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? yc : ys[m + R][cx + o]; });
         const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
-        T lap = Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+        T lap = lap_xy(p, ax, ay);
         if constexpr (ORDER != 2) {
           // Degenerate z axis: the z taps all read the centre value.
-          lap = Ar<T>::add(lap, Ar<T>::mul(tap_sum<T, 2, ORDER>([&](int) { return yc; }), p.ihz2));
+          lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return yc; }));
         }
-        ms[m][tx] = Ar<T>::sub(Ar<T>::add(-yc, Ar<T>::mul(Ar<T>::mul(yc, yc), yc)), Ar<T>::mul(p.kappa, lap));
+        ms[m][tx] = chem_pot(p, yc, lap);
       }
     }
   }
@@ -263,11 +286,11 @@ __global__ void __launch_bounds__(kT2W * kT2TY) ch_tile2d_kernel(const StagePara
     const T mc = win[R];
     const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? mc : ms[oy + R][cx + o]; });
     const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
-    T lap = Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+    T lap = lap_xy(p, ax, ay);
     if constexpr (ORDER != 2) {
-      lap = Ar<T>::add(lap, Ar<T>::mul(tap_sum<T, 2, ORDER>([&](int) { return mc; }), p.ihz2));
+      lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return mc; }));
     }
-    const T rhs = Ar<T>::mul(lap, p.mob);
+    const T rhs = mobility(p, lap);
     const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
     if constexpr (MODE == MODE_RHS) {
       p.out[gi] = rhs;
@@ -299,13 +322,293 @@ gc_status launch_tile2d(gc_context* ctx, const StageParams<T>& p) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent TMA-pipelined 2-D stage kernel (double precision, Nz == 1).
+// Same tile geometry and the same arithmetic as ch_tile2d_kernel; what
+// changes is how the inputs arrive.  Each CTA loops over tiles; while it
+// computes tile i, one thread has already issued the TMA loads
+// (cp.async.bulk.tensor.2d) of tile i+1 -- psi and k_prev on the y region,
+// and k1, k2 on the output tile in the last RK4 stage -- into the other
+// half of a double-buffered shared-memory ring, completing an mbarrier
+// with the bytes delivered.  Waits on the mbarrier are bounded by a clock
+// budget: on expiry the CTA records GC_ERR_TIMEOUT in the context's status
+// word and leaves.  TMA has no periodic wrap, so tiles whose y region
+// crosses the domain edge (a few percent at large sizes) are loaded with
+// ordinary wrapped loads instead; their barrier phase is still completed
+// by a plain arrive so the parity sequence stays regular.
+constexpr int kTmaThreads = kT2W * kT2TY;
+constexpr long long kWaitBudgetCycles = 4000000000LL;  // about 2 s at 2 GHz
+
+template <class T, int ORDER, int MODE, bool KIN>
+struct TmaLayout {
+  static constexpr int R = W<2, ORDER>::R;
+  static constexpr int TX = kT2W - 2 * R, TY = kT2Y;
+  static constexpr int YX = TX + 4 * R, YY = TY + 4 * R;
+  static constexpr int MX = kT2W, MY = TY + 2 * R;
+  // k1, k2 of the last RK4 stage are read once per output cell, so they are
+  // fetched into registers rather than staged (keeps three CTAs per SM).
+  static constexpr bool K12 = false;
+  static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
+  static constexpr size_t YB = al(sizeof(T) * YX * YY);   // one y-region field
+  static constexpr size_t OB = al(sizeof(T) * TX * TY);   // one output-tile field
+  static constexpr size_t BUF = YB + (KIN ? YB : 0) + (K12 ? 2 * OB : 0);
+  static constexpr size_t OFF_BUF = 128;                  // after the barriers
+  static constexpr size_t OFF_YS = OFF_BUF + 2 * BUF;
+  static constexpr size_t OFF_MS = OFF_YS + (KIN ? YB : 0);
+  static constexpr size_t BYTES = OFF_MS + al(sizeof(T) * MX * MY) + 128;  // + alignment slack
+  static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(T) * YX * YY * (KIN ? 2 : 1) +
+                                                             (K12 ? 2 * sizeof(T) * TX * TY : 0));
+};
+
+template <class T, int ORDER, int MODE, bool KIN>
+__global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
+    const StageParams<T> p, const __grid_constant__ CUtensorMap m_psi, const __grid_constant__ CUtensorMap m_kin,
+    const __grid_constant__ CUtensorMap m_k1, const __grid_constant__ CUtensorMap m_k2, const int tiles_x,
+    const int tiles_y, int* status) {
+  using L = TmaLayout<T, ORDER, MODE, KIN>;
+  constexpr int R = L::R, TX = L::TX, TY = L::TY, YX = L::YX, YY = L::YY, MX = L::MX, MY = L::MY;
+  constexpr int NW = 2 * R + 1;
+  constexpr int MS = (MY + kT2TY - 1) / kT2TY;
+  constexpr int OS = TY / kT2TY;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+  int* s_abort = reinterpret_cast<int*>(base + 64);
+  auto buf_psi = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF); };
+  auto buf_kin = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + L::YB); };
+  auto buf_k1 = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + (KIN ? 2 : 1) * L::YB); };
+  auto buf_k2 = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + (KIN ? 2 : 1) * L::YB + L::OB); };
+  T* ms = reinterpret_cast<T*>(base + L::OFF_MS);
+
+  const int nx = p.nx, ny = p.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kT2W + tx;
+  const int ntiles = tiles_x * tiles_y;
+
+  auto tile_origin = [&](int tl, int& x0, int& y0) {
+    x0 = (tl % tiles_x) * TX;
+    y0 = (tl / tiles_x) * TY;
+  };
+  auto interior = [&](int x0, int y0) {
+    return x0 - 2 * R >= 0 && x0 - 2 * R + YX <= nx && y0 - 2 * R >= 0 && y0 - 2 * R + YY <= ny;
+  };
+  auto issue = [&](int tl, int b) {  // one thread
+    int x0, y0;
+    tile_origin(tl, x0, y0);
+    if (interior(x0, y0)) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&bar[b], L::TX_BYTES);
+      tma_load_2d(buf_psi(b), &m_psi, x0 - 2 * R, y0 - 2 * R, &bar[b]);
+      if constexpr (KIN) tma_load_2d(buf_kin(b), &m_kin, x0 - 2 * R, y0 - 2 * R, &bar[b]);
+      if constexpr (L::K12) {
+        tma_load_2d(buf_k1(b), &m_k1, x0, y0, &bar[b]);
+        tma_load_2d(buf_k2(b), &m_k2, x0, y0, &bar[b]);
+      }
+    } else {
+      mbar_arrive(&bar[b]);
+    }
+  };
+
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    *s_abort = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+
+  int i = 0;
+  for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++i) {
+    const int b = i & 1;
+    if (tid == 0 && tl + static_cast<int>(gridDim.x) < ntiles) issue(tl + gridDim.x, b ^ 1);
+    int x0, y0;
+    tile_origin(tl, x0, y0);
+    // Last RK4 stage: k1 and k2 at this thread's output cells, issued before
+    // the wait so that they travel while the tile's TMA completes.
+    T r_k1[OS], r_k2[OS];
+    if constexpr (MODE == MODE_RK4_FINAL) {
+#pragma unroll
+      for (int k = 0; k < OS; ++k) {
+        const int oy = ty * OS + k;
+        const bool in = tx < TX && x0 + tx < nx && y0 + oy < ny;
+        const size_t gi = in ? static_cast<size_t>(y0 + oy) * nx + (x0 + tx) : 0;
+        r_k1[k] = in ? __ldg(p.k1 + gi) : T(0);
+        r_k2[k] = in ? __ldg(p.k2 + gi) : T(0);
+      }
+    }
+    const long long t_start = clock64();
+    while (!mbar_try_wait(&bar[b], (i >> 1) & 1)) {
+      if (clock64() - t_start > kWaitBudgetCycles) {
+        *s_abort = 1;
+        atomicExch(status, static_cast<int>(GC_ERR_TIMEOUT));
+        break;
+      }
+    }
+    T* ps = buf_psi(b);
+    if (!interior(x0, y0)) {
+      // Wrapped y region (and output tile) with ordinary loads.
+      T* ks = buf_kin(b);
+      for (int e = tid; e < YX * YY; e += kTmaThreads) {
+        const int r = e / YX, cc = e - r * YX;
+        const size_t gi = static_cast<size_t>(wrap(y0 - 2 * R + r, ny)) * nx + wrap(x0 - 2 * R + cc, nx);
+        ps[e] = p.psi[gi];
+        if constexpr (KIN) ks[e] = p.kin[gi];
+      }
+      if constexpr (L::K12) {
+        T* a1 = buf_k1(b);
+        T* a2 = buf_k2(b);
+        for (int e = tid; e < TX * TY; e += kTmaThreads) {
+          const int r = e / TX, cc = e - r * TX;
+          const bool in = x0 + cc < nx && y0 + r < ny;
+          const size_t gi = in ? static_cast<size_t>(y0 + r) * nx + (x0 + cc) : 0;
+          a1[e] = in ? p.k1[gi] : T(0);
+          a2[e] = in ? p.k2[gi] : T(0);
+        }
+      }
+    }
+    __syncthreads();
+    if (*s_abort) {
+      // Let the prefetch of the next tile land (bounded) before leaving.
+      if (tid == 0 && tl + static_cast<int>(gridDim.x) < ntiles) {
+        const long long t_drain = clock64();
+        while (!mbar_try_wait(&bar[b ^ 1], ((i + 1) >> 1) & 1) && clock64() - t_drain < kWaitBudgetCycles) {
+        }
+      }
+      break;
+    }
+
+    // y = psi + a k_prev (stage 1 and Euler read psi directly).
+    const T* ys = ps;
+    if constexpr (KIN) {
+      T* yw = reinterpret_cast<T*>(base + L::OFF_YS);
+      const T* ks = buf_kin(b);
+      for (int e = tid; e < YX * YY; e += kTmaThreads) yw[e] = Ar<T>::add(ps[e], Ar<T>::mul(p.a, ks[e]));
+      __syncthreads();
+      ys = yw;
+    }
+
+    // Phase 2: mu at mu-row strip [m0, m1), column tx (y column tx + R).
+    {
+      const int m0 = ty * MS;
+      const int m1 = min(m0 + MS, MY);
+      const int cx = tx + R;
+      T win[NW];
+#pragma unroll
+      for (int k = 0; k < 2 * R; ++k) win[k + 1] = ys[(m0 + k) * YX + cx];
+#pragma unroll
+      for (int k = 0; k < MS; ++k) {
+        const int m = m0 + k;
+        if (m < m1) {
+#pragma unroll
+          for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
+          win[NW - 1] = ys[(m + 2 * R) * YX + cx];
+          const T yc = win[R];
+          const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? yc : ys[(m + R) * YX + cx + o]; });
+          const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+          T lap = lap_xy(p, ax, ay);
+          if constexpr (ORDER != 2) {
+            lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return yc; }));
+          }
+          ms[m * MX + tx] = chem_pot(p, yc, lap);
+        }
+      }
+    }
+    __syncthreads();
+
+    // Phase 3: output strip.
+    if (tx < TX && x0 + tx < nx) {
+      const int o0 = ty * OS;
+      const int cx = tx + R;
+      T win[NW];
+#pragma unroll
+      for (int k = 0; k < 2 * R; ++k) win[k + 1] = ms[(o0 + k) * MX + cx];
+#pragma unroll
+      for (int k = 0; k < OS; ++k) {
+        const int oy = o0 + k;
+#pragma unroll
+        for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
+        win[NW - 1] = ms[(oy + 2 * R) * MX + cx];
+        if (y0 + oy >= ny) break;
+        const T mc = win[R];
+        const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? mc : ms[(oy + R) * MX + cx + o]; });
+        const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+        T lap = lap_xy(p, ax, ay);
+        if constexpr (ORDER != 2) {
+          lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return mc; }));
+        }
+        const T rhs = mobility(p, lap);
+        const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
+        const int yc_idx = (oy + 2 * R) * YX + (tx + 2 * R);
+        if constexpr (MODE == MODE_RHS) {
+          p.out[gi] = rhs;
+        } else if constexpr (MODE == MODE_RK4_FINAL) {
+          const T s14 = Ar<T>::add(r_k1[k], rhs);
+          const T s23 = Ar<T>::add(r_k2[k], buf_kin(b)[yc_idx]);
+          p.out[gi] = Ar<T>::add(ps[yc_idx], Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+        } else {
+          p.out[gi] = Ar<T>::add(ps[yc_idx], Ar<T>::mul(p.c6, rhs));
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Launches the TMA kernel when its layout rules hold; GC_ERR_UNSUPPORTED
+// (nothing launched) otherwise, and the caller uses ch_tile2d_kernel.
+template <class T, int ORDER, int MODE, bool KIN>
+gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
+  using L = TmaLayout<T, ORDER, MODE, KIN>;
+  if (p.nx < L::YX || p.ny < L::YY) return GC_ERR_UNSUPPORTED;
+  CUtensorMap mpsi{}, mkin{}, mk1{}, mk2{};
+  const int eb = static_cast<int>(sizeof(T));
+  if (!make_tensor_map_2d(&mpsi, p.psi, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
+  if (KIN && !make_tensor_map_2d(&mkin, p.kin, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
+  if (L::K12) {
+    if (!make_tensor_map_2d(&mk1, p.k1, p.nx, p.ny, eb, L::TX, L::TY)) return GC_ERR_UNSUPPORTED;
+    if (!make_tensor_map_2d(&mk2, p.k2, p.nx, p.ny, eb, L::TX, L::TY)) return GC_ERR_UNSUPPORTED;
+  }
+  auto kern = ch_tma_kernel<T, ORDER, MODE, KIN>;
+  static int ctas_per_sm = 0;  // one instantiation per template argument set
+  if (ctas_per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::BYTES)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kTmaThreads, L::BYTES));
+    if (ctas_per_sm < 1) ctas_per_sm = 1;
+  }
+  const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
+  const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
+  const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
+  kern<<<grid, dim3(kT2W, kT2TY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, mk1, mk2, tiles_x, tiles_y,
+                                                           ctx->device_status);
+  GC_CHECK_LAUNCH("ch_tma_kernel");
+  return GC_OK;
+}
+
+// 2-D dispatch: TMA pipeline for double when its rules hold, else the
+// strip kernel.
+template <class T, int ORDER, int MODE>
+gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
+  if constexpr (sizeof(T) == 8) {
+    gc_status s;
+    if constexpr (MODE == MODE_RHS) {
+      s = p.kin ? launch_tma<T, ORDER, MODE, true>(ctx, p) : launch_tma<T, ORDER, MODE, false>(ctx, p);
+    } else if constexpr (MODE == MODE_RK4_FINAL) {
+      s = launch_tma<T, ORDER, MODE, true>(ctx, p);
+    } else {
+      s = launch_tma<T, ORDER, MODE, false>(ctx, p);
+    }
+    if (s != GC_ERR_UNSUPPORTED) return s;
+  }
+  return launch_tile2d<T, ORDER, MODE>(ctx, p);
+}
+
 template <class T, int MODE>
 gc_status launch_mode(gc_context* ctx, int order, const StageParams<T>& p) {
   const bool z3 = p.nz > 1;
   switch (order) {
-    case 2: return z3 ? launch_stage<T, 2, true, MODE>(ctx, p) : launch_tile2d<T, 2, MODE>(ctx, p);
-    case 4: return z3 ? launch_stage<T, 4, true, MODE>(ctx, p) : launch_tile2d<T, 4, MODE>(ctx, p);
-    case 6: return z3 ? launch_stage<T, 6, true, MODE>(ctx, p) : launch_tile2d<T, 6, MODE>(ctx, p);
+    case 2: return z3 ? launch_stage<T, 2, true, MODE>(ctx, p) : launch_2d<T, 2, MODE>(ctx, p);
+    case 4: return z3 ? launch_stage<T, 4, true, MODE>(ctx, p) : launch_2d<T, 4, MODE>(ctx, p);
+    case 6: return z3 ? launch_stage<T, 6, true, MODE>(ctx, p) : launch_2d<T, 6, MODE>(ctx, p);
   }
   return fail(GC_ERR_UNSUPPORTED, "gridcalc_b200: Cahn-Hilliard order must be 2, 4 or 6");
 }
@@ -319,6 +622,9 @@ StageParams<T> base_params(const gc_grid* g, const gc_ch_params* cp) {
   p.ihz2 = static_cast<T>(1.0 / (g->hz * g->hz));
   p.mob = static_cast<T>(cp->mobility);
   p.kappa = static_cast<T>(cp->kappa);
+  p.unit_h = p.ihx2 == T(1) && p.ihy2 == T(1) && p.ihz2 == T(1);
+  p.unit_m = p.mob == T(1);
+  p.unit_k = p.kappa == T(1);
   return p;
 }
 

@@ -50,6 +50,9 @@ struct gc_context {
   gcb::Scratch scratch[16];
   // Pinned host word(s) for small device->host results.
   void* host_pinned = nullptr;
+  // Device status word: kernels with bounded waits set it when a wait gives
+  // up (GC_ERR_TIMEOUT); gc_synchronize() reports and clears it.
+  int* device_status = nullptr;
   // Small cache of captured step graphs, keyed by everything the captured
   // kernels bake in; least recently used entry is replaced.
   static constexpr int kGraphSlots = 6;
@@ -221,16 +224,20 @@ __host__ __device__ constexpr bool zero_weight(int m) {
 // acc = ((w0 v0 + w1 v1) + ...) accumulated left to right, as the reference
 // loops `acc += w[m] * field(...)`.  Zero-weight taps are skipped (that only
 // changes the sign of an exactly-zero sum) and unit weights skip the multiply.
+// The reference starts from 0.0; starting from the first tap instead
+// differs only when that tap is -0 (the sum's sign of zero).
 template <class T, int Kind, int Order, class Get>
 __device__ __forceinline__ T tap_sum(Get get) {
   constexpr int R = W<Kind, Order>::R;
   T acc = T(0);
+  bool first = true;
 #pragma unroll
   for (int m = 0; m <= 2 * R; ++m) {
     if (zero_weight<Kind, Order>(m)) continue;
     const T v = get(m - R);
-    if (unit_weight<Kind, Order>(m)) acc = Ar<T>::add(acc, v);
-    else acc = Ar<T>::mac(acc, wt<T, Kind, Order>(m), v);
+    const T term = unit_weight<Kind, Order>(m) ? v : Ar<T>::mul(wt<T, Kind, Order>(m), v);
+    acc = first ? term : Ar<T>::add(acc, term);
+    first = false;
   }
   return acc;
 }

@@ -142,7 +142,11 @@ GC_API gc_status gc_context_create(gc_context** out, int device, void* stream) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->host_pinned, 4096);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->device_status, 256);
+  if (e == cudaSuccess) e = cudaMemset(ctx->device_status, 0, 256);
   if (e != cudaSuccess) {
+    if (ctx->device_status) cudaFree(ctx->device_status);
+    if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
     if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
     if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -162,6 +166,7 @@ GC_API gc_status gc_context_destroy(gc_context* ctx) {
   for (auto& s : ctx->scratch)
     if (s.ptr) cudaFree(s.ptr);
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->device_status) cudaFree(ctx->device_status);
   if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
   if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
   cudaStreamDestroy(ctx->stream);
@@ -173,7 +178,15 @@ GC_API gc_status gc_synchronize(gc_context* ctx) {
   Call call(ctx);
   gc_status s = call.st;
   if (s != GC_OK) return s;
+  int* host = static_cast<int*>(ctx->host_pinned) + 64;
+  GC_CUDA(cudaMemcpyAsync(host, ctx->device_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*host != 0) {
+    GC_CUDA(cudaMemsetAsync(ctx->device_status, 0, sizeof(int), ctx->stream));
+    GC_CUDA(cudaStreamSynchronize(ctx->stream));
+    return fail(GC_ERR_TIMEOUT, "gridcalc_b200: a bounded device wait gave up (TMA tile not delivered); "
+                                "the results of the affected calls are undefined");
+  }
   return GC_OK;
 }
 

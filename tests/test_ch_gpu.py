@@ -97,6 +97,27 @@ def test_rk4_orders_and_step_counts(gc, oracle, order, steps):
     assert np.array_equal(host(t), oracle.ch_integrate(order, 1.0, 1.0, psi0, dt, steps))
 
 
+@pytest.mark.parametrize("shape", [(1, 200, 266), (1, 97, 300), (1, 131, 250), (1, 64, 66)])
+@pytest.mark.parametrize("order", [2, 4, 6])
+def test_2d_tma_tiles_interior_edge_partial(gc, oracle, shape, order):
+    """Even-width 2-D grids large enough for interior tiles take the
+    TMA-pipelined kernel (interior tiles by TMA, edge and partial tiles by
+    wrapped loads); odd widths take the strip kernel.  Both must stay
+    bit-identical, for RK4 (all four stage kinds) and Euler, and over enough
+    steps that every CTA processes several tiles."""
+    psi0 = uniform_ic(shape, 7 * order + shape[2])
+    dt = {2: 0.01, 4: 0.005, 6: 0.004}[order]
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, order)
+    g = grid_of(gc, shape)
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt, 18, gc.RK4)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 1.0, 1.0, psi0, dt, 18))
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt / 2, 5, gc.ExplicitEuler)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 1.0, 1.0, psi0, dt / 2, 5, rk4=False))
+    gc.context().synchronize()  # reports a timed-out device wait, if any
+
+
 def test_3d_and_anisotropic(gc, oracle):
     shape = (12, 10, 14)
     h = (0.9, 1.1, 1.3)
