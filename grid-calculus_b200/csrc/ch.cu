@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "ch_tile.cuh"
 #include "common.cuh"
 #include "stepper.cuh"
 #include "tma.cuh"
@@ -29,45 +30,6 @@ namespace gcb {
 namespace {
 
 constexpr int kThreads = 256;
-
-enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
-
-template <class T>
-struct StageParams {
-  const T* psi;    // state
-  const T* kin;    // previous stage (y = psi + a kin), nullptr for y = psi
-  T a;             // stage coefficient
-  T* out;          // k_s (MODE_RHS) or psi' (final modes)
-  const T* k1;     // MODE_RK4_FINAL only
-  const T* k2;
-  const T* k3;
-  T c6, c3;        // dt/6, dt/3 (RK4 final) ; c6 = dt (Euler final)
-  T mob, kappa;
-  T ihx2, ihy2, ihz2;
-  int nx, ny, nz;
-  // Exact shortcuts: x * 1 == x, so a unit spacing, mobility or kappa
-  // skips its multiply without changing a bit.
-  bool unit_h, unit_m, unit_k;
-};
-
-// (ax / hx^2 + ay / hy^2) [+ az / hz^2], as the reference combines the axes.
-template <class T>
-__device__ __forceinline__ T lap_xy(const StageParams<T>& p, T ax, T ay) {
-  return p.unit_h ? Ar<T>::add(ax, ay) : Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
-}
-template <class T>
-__device__ __forceinline__ T lap_z(const StageParams<T>& p, T lap, T az) {
-  return Ar<T>::add(lap, p.unit_h ? az : Ar<T>::mul(az, p.ihz2));
-}
-// mu = -y + y^3 - kappa lap(y)
-template <class T>
-__device__ __forceinline__ T chem_pot(const StageParams<T>& p, T y, T lap) {
-  return Ar<T>::sub(Ar<T>::add(-y, Ar<T>::mul(Ar<T>::mul(y, y), y)), p.unit_k ? lap : Ar<T>::mul(p.kappa, lap));
-}
-template <class T>
-__device__ __forceinline__ T mobility(const StageParams<T>& p, T lap) {
-  return p.unit_m ? lap : Ar<T>::mul(lap, p.mob);
-}
 
 template <class T, int ORDER, bool Z3>
 struct Tile;
@@ -169,156 +131,6 @@ gc_status launch_stage(gc_context* ctx, const StageParams<T>& p) {
   dim3 grid(div_up(p.nx, TL::TX), div_up(p.ny, TL::TY), Z3 ? div_up(p.nz, TL::TZ) : 1);
   kern<<<grid, kThreads, smem, ctx->stream>>>(p);
   GC_CHECK_LAUNCH("ch_stage_kernel");
-  return GC_OK;
-}
-
-// ---------------------------------------------------------------------------
-// 2-D stage kernel (Nz == 1), the production path of the plain method.
-// The three phases of the generic kernel above, arranged so that shared
-// memory carries only what must cross threads.  64 x 4 threads; the mu
-// region is exactly 64 columns wide (output tile 64 - 2R columns by 16
-// rows).  In phases 2 and 3 a thread owns one column and a strip of
-// consecutive rows: the y-direction taps come from a register window of
-// its own column (one new shared-memory value per row), only the x taps
-// are read from neighbouring columns.  In double precision every
-// warp-wide shared read is two wavefronts, and this layout halves the
-// shared-memory reads per cell, which bound the earlier layout.  Wrapped
-// columns are formed once per thread, wrapped rows once per row.  In the
-// last RK4 stage the k1 and k2 lines of the tile are prefetched into L2 at
-// the start.
-constexpr int kT2W = 64;   // mu-region columns = threads in x
-constexpr int kT2Y = 16;   // output rows
-constexpr int kT2TY = 4;   // thread rows
-
-template <class T, int ORDER, int MODE>
-__global__ void __launch_bounds__(kT2W * kT2TY) ch_tile2d_kernel(const StageParams<T> p) {
-  constexpr int R = W<2, ORDER>::R;
-  constexpr int TX = kT2W - 2 * R, TY = kT2Y, NTY = kT2TY;
-  constexpr int YX = TX + 4 * R, YY = TY + 4 * R;   // y region (tile + 2R halo)
-  constexpr int MX = kT2W, MY = TY + 2 * R;         // mu region (tile + R halo)
-  constexpr int NW = 2 * R + 1;
-  constexpr int MS = (MY + NTY - 1) / NTY;          // mu rows per thread strip
-  constexpr int OS = TY / NTY;                      // output rows per thread strip
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T (*ys)[YX] = reinterpret_cast<T (*)[YX]>(smem_raw);
-  T (*ms)[MX] = reinterpret_cast<T (*)[MX]>(smem_raw + sizeof(T) * YX * YY);
-
-  const int nx = p.nx, ny = p.ny;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-
-  if constexpr (MODE == MODE_RK4_FINAL) {
-    if (tx < TX && x0 + tx < nx) {
-#pragma unroll
-      for (int k = 0; k < OS; ++k) {
-        const int oy = ty * OS + k;
-        if (y0 + oy < ny) {
-          const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k1 + gi));
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k2 + gi));
-        }
-      }
-    }
-  }
-
-  // Phase 1: y = psi + a k_prev on the tile + 2R halo (YX = 64 + 2R columns).
-  const int gxa = wrap(x0 - 2 * R + tx, nx);
-  const bool has_b = tx < YX - kT2W;
-  const int gxb = wrap(x0 - 2 * R + kT2W + tx, nx);
-  const bool has_kin = p.kin != nullptr;
-#pragma unroll
-  for (int ry = ty; ry < YY; ry += NTY) {
-    const size_t row = static_cast<size_t>(wrap(y0 - 2 * R + ry, ny)) * nx;
-    T v = __ldg(p.psi + row + gxa);
-    if (has_kin) v = Ar<T>::add(v, Ar<T>::mul(p.a, __ldg(p.kin + row + gxa)));
-    ys[ry][tx] = v;
-    if (has_b) {
-      T w = __ldg(p.psi + row + gxb);
-      if (has_kin) w = Ar<T>::add(w, Ar<T>::mul(p.a, __ldg(p.kin + row + gxb)));
-      ys[ry][kT2W + tx] = w;
-    }
-  }
-  __syncthreads();
-
-  // Phase 2: mu at mu-row strip [m0, m1), column tx (y column tx + R).
-  {
-    const int m0 = ty * MS;
-    const int m1 = min(m0 + MS, MY);
-    const int cx = tx + R;
-    T win[NW];  // y at rows m .. m + 2R (y space), column cx
-#pragma unroll
-    for (int k = 0; k < 2 * R; ++k) win[k + 1] = ys[m0 + k][cx];
-#pragma unroll
-    for (int k = 0; k < MS; ++k) {
-      const int m = m0 + k;
-      if (m < m1) {
-#pragma unroll
-        for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
-        win[NW - 1] = ys[m + 2 * R][cx];
-        const T yc = win[R];
-        const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? yc : ys[m + R][cx + o]; });
-        const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
-        T lap = lap_xy(p, ax, ay);
-        if constexpr (ORDER != 2) {
-          // Degenerate z axis: the z taps all read the centre value.
-          lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return yc; }));
-        }
-        ms[m][tx] = chem_pot(p, yc, lap);
-      }
-    }
-  }
-  __syncthreads();
-
-  // Phase 3: k_s = M lap(mu) at output-row strip [o0, o0 + OS), column tx.
-  if (tx >= TX || x0 + tx >= nx) return;
-  const int o0 = ty * OS;
-  const int cx = tx + R;
-  T win[NW];  // mu at rows o .. o + 2R (mu space), column cx
-#pragma unroll
-  for (int k = 0; k < 2 * R; ++k) win[k + 1] = ms[o0 + k][cx];
-#pragma unroll
-  for (int k = 0; k < OS; ++k) {
-    const int oy = o0 + k;
-#pragma unroll
-    for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
-    win[NW - 1] = ms[oy + 2 * R][cx];
-    if (y0 + oy >= ny) break;
-    const T mc = win[R];
-    const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? mc : ms[oy + R][cx + o]; });
-    const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
-    T lap = lap_xy(p, ax, ay);
-    if constexpr (ORDER != 2) {
-      lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return mc; }));
-    }
-    const T rhs = mobility(p, lap);
-    const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + tx);
-    if constexpr (MODE == MODE_RHS) {
-      p.out[gi] = rhs;
-    } else if constexpr (MODE == MODE_RK4_FINAL) {
-      const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
-      const T s23 = Ar<T>::add(__ldg(p.k2 + gi), __ldg(p.k3 + gi));
-      p.out[gi] = Ar<T>::add(__ldg(p.psi + gi), Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
-    } else {
-      p.out[gi] = Ar<T>::add(ys[oy + 2 * R][tx + 2 * R], Ar<T>::mul(p.c6, rhs));
-    }
-  }
-}
-
-template <class T, int ORDER, int MODE>
-gc_status launch_tile2d(gc_context* ctx, const StageParams<T>& p) {
-  constexpr int R = W<2, ORDER>::R;
-  constexpr int TX = kT2W - 2 * R;
-  constexpr size_t smem = sizeof(T) * (static_cast<size_t>(TX + 4 * R) * (kT2Y + 4 * R) +
-                                       static_cast<size_t>(kT2W) * (kT2Y + 2 * R));
-  auto kern = ch_tile2d_kernel<T, ORDER, MODE>;
-  static bool attr = false;  // one instantiation per (T, ORDER, MODE)
-  if (!attr) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    attr = true;
-  }
-  dim3 grid(div_up(p.nx, TX), div_up(p.ny, kT2Y), 1), block(kT2W, kT2TY);
-  kern<<<grid, block, smem, ctx->stream>>>(p);
-  GC_CHECK_LAUNCH("ch_tile2d_kernel");
   return GC_OK;
 }
 
@@ -584,8 +396,48 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
   return GC_OK;
 }
 
-// 2-D dispatch: TMA pipeline for double when its rules hold, else the
-// strip kernel.
+// Single-grid work source for the cp.async-pipelined persistent loop.
+template <class T>
+struct GridSource {
+  StageParams<T> p;
+  int tiles_x, n_tiles, tile_w, tile_h;
+  __device__ int count() const { return n_tiles; }
+  __device__ void get(int k, StageParams<T>& q, int& x0, int& y0) const {
+    q = p;
+    x0 = (k % tiles_x) * tile_w;
+    y0 = (k / tiles_x) * tile_h;
+  }
+};
+
+template <class T, int ORDER, int MODE>
+__global__ void __launch_bounds__(kT2W * kT2TY) ch_pipe_kernel(const StageParams<T> p, int tiles_x, int n_tiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TX = kT2W - 2 * W<2, ORDER>::R;
+  const GridSource<T> src{p, tiles_x, n_tiles, TX, kT2Y};
+  pipelined_tiles<T, ORDER, MODE, kT2W, kT2Y, kT2TY>(src, smem_raw);
+}
+
+template <class T, int ORDER, int MODE>
+gc_status launch_pipe(gc_context* ctx, const StageParams<T>& p) {
+  constexpr int TX = kT2W - 2 * W<2, ORDER>::R;
+  constexpr size_t smem = pipe_smem<T, ORDER, kT2W, kT2Y>();
+  auto kern = ch_pipe_kernel<T, ORDER, MODE>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT2W * kT2TY, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int tiles_x = div_up(p.nx, TX), tiles_y = div_up(p.ny, kT2Y);
+  const int n_tiles = tiles_x * tiles_y;
+  const int grid = std::max(1, std::min(n_tiles, per_sm * ctx->num_sms));
+  kern<<<grid, dim3(kT2W, kT2TY), smem, ctx->stream>>>(p, tiles_x, n_tiles);
+  GC_CHECK_LAUNCH("ch_pipe_kernel");
+  return GC_OK;
+}
+
+// 2-D dispatch: TMA pipeline for double when its rules hold, the
+// cp.async-pipelined persistent loop otherwise.
 template <class T, int ORDER, int MODE>
 gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
   if constexpr (sizeof(T) == 8) {
@@ -599,7 +451,7 @@ gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
     }
     if (s != GC_ERR_UNSUPPORTED) return s;
   }
-  return launch_tile2d<T, ORDER, MODE>(ctx, p);
+  return launch_pipe<T, ORDER, MODE>(ctx, p);
 }
 
 template <class T, int MODE>

@@ -1,0 +1,587 @@
+// Batched Cahn-Hilliard ensemble: many independent 2-D grids of uneven size,
+// each with its own kappa, mobility and time step, advanced together.
+//
+// All members' fields live packed in one buffer per RK slot (state, second
+// state, k1, k2, k3), member i at element offset off_i (a multiple of 64).
+// A work list holds one entry per (member, tile); one persistent launch per
+// RK stage walks the whole list with grid-stride CTAs, reading the member's
+// extents, offsets and coefficients from a device table, and runs the same
+// strip tile as the single-grid path (ch_tile.cuh) -- so a step is four
+// launches for the whole ensemble however many members it has, and the
+// steps are captured into a CUDA graph and replayed.  The tile shape comes
+// from a small set of compiled candidates; gc_ch_batch_autotune times each
+// on the actual ensemble and keeps the fastest (optionally recorded in a
+// JSON file keyed by device and ensemble).  Mass and free energy are
+// reduced per member in double with compensated sums in a fixed order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ch_tile.cuh"
+#include "common.cuh"
+#include "stepper.cuh"
+
+namespace gcb {
+namespace {
+
+template <class T>
+struct Member {
+  int nx, ny;
+  long long off;
+  T dt, half, sixth, third;
+  T kappa, mob;
+  bool unit_m, unit_k;
+};
+
+template <class T>
+struct BatchBuffers {
+  const T* psi;
+  T* dst;
+  T* k1;
+  T* k2;
+  T* k3;
+};
+
+// Tile-shape candidates: mu-region width (threads in x), output rows,
+// thread rows.
+struct TileShape {
+  int tw, ty, nty;
+};
+constexpr TileShape kShapes[] = {{32, 16, 4}, {64, 8, 4}, {64, 16, 4}, {64, 32, 8}};
+constexpr int kNumShapes = 4;
+
+// Work source of the ensemble: item k is (member, tile origin); the stage
+// selects the RK slots and coefficient (1..3 = RK4 stages writing k1..k3,
+// 4 = last RK4 stage, 0 = Euler).
+template <class T>
+struct BatchSource {
+  const Member<T>* members;
+  const int4* items;
+  int n_items;
+  BatchBuffers<T> buf;
+  int stage;
+  __device__ int count() const { return n_items; }
+  __device__ void get(int k, StageParams<T>& p, int& x0, int& y0) const {
+    const int4 w = items[k];
+    const Member<T> m = members[w.x];
+    x0 = w.y;
+    y0 = w.z;
+    p.nx = m.nx;
+    p.ny = m.ny;
+    p.nz = 1;
+    p.ihx2 = p.ihy2 = p.ihz2 = T(1);
+    p.unit_h = true;
+    p.mob = m.mob;
+    p.kappa = m.kappa;
+    p.unit_m = m.unit_m;
+    p.unit_k = m.unit_k;
+    p.psi = buf.psi + m.off;
+    p.k1 = p.k2 = p.k3 = nullptr;
+    p.a = p.c6 = p.c3 = T(0);
+    if (stage == 0) {
+      p.kin = nullptr;
+      p.out = buf.dst + m.off;
+      p.c6 = m.dt;
+    } else if (stage == 1) {
+      p.kin = nullptr;
+      p.out = buf.k1 + m.off;
+    } else if (stage == 2) {
+      p.kin = buf.k1 + m.off;
+      p.a = m.half;
+      p.out = buf.k2 + m.off;
+    } else if (stage == 3) {
+      p.kin = buf.k2 + m.off;
+      p.a = m.half;
+      p.out = buf.k3 + m.off;
+    } else {
+      p.kin = buf.k3 + m.off;
+      p.a = m.dt;
+      p.out = buf.dst + m.off;
+      p.k1 = buf.k1 + m.off;
+      p.k2 = buf.k2 + m.off;
+      p.k3 = buf.k3 + m.off;
+      p.c6 = m.sixth;
+      p.c3 = m.third;
+    }
+  }
+};
+
+template <class T, int ORDER, int MODE, int TW, int TY, int NTY>
+__global__ void __launch_bounds__(TW * NTY) ch_batch_kernel(const Member<T>* __restrict__ members,
+                                                            const int4* __restrict__ items, int n_items,
+                                                            const BatchBuffers<T> buf, int stage) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const BatchSource<T> src{members, items, n_items, buf, stage};
+  pipelined_tiles<T, ORDER, MODE, TW, TY, NTY>(src, smem_raw);
+}
+
+// ---- per-member FP64 diagnostics -----------------------------------------
+struct SumC {
+  double s, c;
+};
+__device__ __forceinline__ SumC two_sum_merge(SumC a, SumC b) {
+  const double t = __dadd_rn(a.s, b.s);
+  const double bp = __dsub_rn(t, a.s);
+  const double err = __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, bp)), __dsub_rn(b.s, bp));
+  return SumC{t, __dadd_rn(__dadd_rn(a.c, b.c), err)};
+}
+__device__ __forceinline__ SumC neumaier(SumC a, double v) {
+  const double t = __dadd_rn(a.s, v);
+  if (fabs(a.s) >= fabs(v)) a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, t), v));
+  else a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(v, t), a.s));
+  a.s = t;
+  return a;
+}
+
+constexpr int kDiagChunk = 8192;
+constexpr int kDiagThreads = 256;
+
+// items: (member, chunk index); out: per item 4 doubles (mass s, c, F s, c).
+template <class T>
+__global__ void __launch_bounds__(kDiagThreads) batch_diag_kernel(const Member<T>* __restrict__ members,
+                                                                  const int2* __restrict__ items, int n_items,
+                                                                  const T* __restrict__ psi,
+                                                                  double* __restrict__ out) {
+  __shared__ SumC sm[kDiagThreads], sf[kDiagThreads];
+  for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int2 w = items[it];
+    const Member<T> m = members[w.x];
+    const T* f = psi + m.off;
+    const long long n = static_cast<long long>(m.nx) * m.ny;
+    const long long c0 = static_cast<long long>(w.y) * kDiagChunk;
+    const long long c1 = c0 + kDiagChunk < n ? c0 + kDiagChunk : n;
+    const double kap = static_cast<double>(m.kappa);
+    SumC am{0, 0}, af{0, 0};
+    for (long long c = c0 + threadIdx.x; c < c1; c += kDiagThreads) {
+      const int i = static_cast<int>(c % m.nx), j = static_cast<int>(c / m.nx);
+      const int ip = i + 1 == m.nx ? 0 : i + 1, im = i == 0 ? m.nx - 1 : i - 1;
+      const int jp = j + 1 == m.ny ? 0 : j + 1, jm = j == 0 ? m.ny - 1 : j - 1;
+      const double p = static_cast<double>(f[c]);
+      // Order-2 gradient, h = 1 (the reference's default in evaluate).
+      const double gx = __dadd_rn(__dmul_rn(-0.5, static_cast<double>(f[static_cast<size_t>(j) * m.nx + im])),
+                                  __dmul_rn(0.5, static_cast<double>(f[static_cast<size_t>(j) * m.nx + ip])));
+      const double gy = __dadd_rn(__dmul_rn(-0.5, static_cast<double>(f[static_cast<size_t>(jm) * m.nx + i])),
+                                  __dmul_rn(0.5, static_cast<double>(f[static_cast<size_t>(jp) * m.nx + i])));
+      const double sq = __dadd_rn(__dmul_rn(gx, gx), __dmul_rn(gy, gy));
+      const double fe = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(-0.5, p), p),
+                                            __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.25, p), p), p), p)),
+                                  __dmul_rn(__dmul_rn(0.5, kap), sq));
+      am = neumaier(am, p);
+      af = neumaier(af, fe);
+    }
+    sm[threadIdx.x] = am;
+    sf[threadIdx.x] = af;
+    __syncthreads();
+    for (int s = kDiagThreads / 2; s >= 1; s >>= 1) {
+      if (threadIdx.x < s) {
+        sm[threadIdx.x] = two_sum_merge(sm[threadIdx.x], sm[threadIdx.x + s]);
+        sf[threadIdx.x] = two_sum_merge(sf[threadIdx.x], sf[threadIdx.x + s]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      out[4 * it + 0] = sm[0].s;
+      out[4 * it + 1] = sm[0].c;
+      out[4 * it + 2] = sf[0].s;
+      out[4 * it + 3] = sf[0].c;
+    }
+    __syncthreads();
+  }
+}
+
+// One thread per member: merges its chunk partials in chunk order.
+__global__ void batch_diag_final(const int* __restrict__ first_item, int n_members,
+                                 const double* __restrict__ part, double* __restrict__ result) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n_members) return;
+  SumC am{0, 0}, af{0, 0};
+  for (int it = first_item[m]; it < first_item[m + 1]; ++it) {
+    am = two_sum_merge(am, SumC{part[4 * it], part[4 * it + 1]});
+    af = two_sum_merge(af, SumC{part[4 * it + 2], part[4 * it + 3]});
+  }
+  result[2 * m] = __dadd_rn(am.s, am.c);
+  result[2 * m + 1] = __dadd_rn(af.s, af.c);
+}
+
+}  // namespace
+}  // namespace gcb
+
+using namespace gcb;
+
+struct gc_ch_batch {
+  gc_context* ctx = nullptr;
+  int n = 0;
+  int order = 4;
+  gc_dtype dtype = GC_F32;
+  std::vector<gc_ch_member> members;
+  std::vector<long long> offsets;  // n + 1
+  long long total = 0;
+  void* slots[5] = {};             // state, second state, k1, k2, k3
+  void* member_table = nullptr;
+  void* items = nullptr;           // int4 work list for the current shape
+  int n_items = 0;
+  int shape = 2;                   // index into kShapes
+  int items_shape = -1;
+  void* diag_items = nullptr;
+  int n_diag_items = 0;
+  void* diag_first = nullptr;
+  void* diag_part = nullptr;
+  void* diag_result = nullptr;
+  std::string tune_report;
+};
+
+namespace gcb {
+namespace {
+
+template <class T, int ORDER, int MODE, int TW, int TY, int NTY>
+gc_status launch_batch_shape(gc_ch_batch* b, const BatchBuffers<T>& buf, int stage) {
+  constexpr size_t smem = pipe_smem<T, ORDER, TW, TY>();
+  auto kern = ch_batch_kernel<T, ORDER, MODE, TW, TY, NTY>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TW * NTY, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int grid = std::max(1, std::min(b->n_items, per_sm * b->ctx->num_sms));
+  kern<<<grid, dim3(TW, NTY), smem, b->ctx->stream>>>(static_cast<const Member<T>*>(b->member_table),
+                                                     static_cast<const int4*>(b->items), b->n_items, buf, stage);
+  GC_CHECK_LAUNCH("ch_batch_kernel");
+  return GC_OK;
+}
+
+template <class T, int ORDER, int MODE>
+gc_status launch_batch(gc_ch_batch* b, const BatchBuffers<T>& buf, int stage) {
+  switch (b->shape) {
+    case 0: return launch_batch_shape<T, ORDER, MODE, 32, 16, 4>(b, buf, stage);
+    case 1: return launch_batch_shape<T, ORDER, MODE, 64, 8, 4>(b, buf, stage);
+    case 2: return launch_batch_shape<T, ORDER, MODE, 64, 16, 4>(b, buf, stage);
+    default: return launch_batch_shape<T, ORDER, MODE, 64, 32, 8>(b, buf, stage);
+  }
+}
+
+template <class T, int MODE>
+gc_status launch_batch_order(gc_ch_batch* b, const BatchBuffers<T>& buf, int stage) {
+  switch (b->order) {
+    case 2: return launch_batch<T, 2, MODE>(b, buf, stage);
+    case 4: return launch_batch<T, 4, MODE>(b, buf, stage);
+    default: return launch_batch<T, 6, MODE>(b, buf, stage);
+  }
+}
+
+template <class T>
+gc_status batch_step(gc_ch_batch* b, const T* src, T* dst) {
+  BatchBuffers<T> buf{src, dst, static_cast<T*>(b->slots[2]), static_cast<T*>(b->slots[3]),
+                      static_cast<T*>(b->slots[4])};
+  gc_status s;
+  for (int stage = 1; stage <= 3; ++stage)
+    if ((s = launch_batch_order<T, MODE_RHS>(b, buf, stage)) != GC_OK) return s;
+  return launch_batch_order<T, MODE_RK4_FINAL>(b, buf, 4);
+}
+
+// (Re)builds the (member, tile) work list for the current shape.
+gc_status build_items(gc_ch_batch* b) {
+  if (b->items_shape == b->shape) return GC_OK;
+  const TileShape sh = kShapes[b->shape];
+  const int R = b->order / 2;
+  const int tx = sh.tw - 2 * R;
+  std::vector<int4> items;
+  for (int m = 0; m < b->n; ++m) {
+    const int nx = b->members[m].nx, ny = b->members[m].ny;
+    for (int y0 = 0; y0 < ny; y0 += sh.ty)
+      for (int x0 = 0; x0 < nx; x0 += tx) items.push_back(make_int4(m, x0, y0, 0));
+  }
+  if (b->items) GC_CUDA(cudaFree(b->items));
+  b->items = nullptr;
+  GC_CUDA(cudaMalloc(&b->items, sizeof(int4) * items.size()));
+  GC_CUDA(cudaMemcpy(b->items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+  b->n_items = static_cast<int>(items.size());
+  b->items_shape = b->shape;
+  return GC_OK;
+}
+
+template <class T>
+gc_status upload_members(gc_ch_batch* b) {
+  std::vector<Member<T>> tab(b->n);
+  for (int m = 0; m < b->n; ++m) {
+    const gc_ch_member& s = b->members[m];
+    Member<T>& d = tab[m];
+    d.nx = s.nx;
+    d.ny = s.ny;
+    d.off = b->offsets[m];
+    d.dt = static_cast<T>(s.dt);
+    d.half = static_cast<T>(0.5 * s.dt);
+    d.sixth = static_cast<T>(s.dt / 6.0);
+    d.third = static_cast<T>(s.dt / 3.0);
+    d.kappa = static_cast<T>(s.kappa);
+    d.mob = static_cast<T>(s.mobility);
+    d.unit_m = d.mob == T(1);
+    d.unit_k = d.kappa == T(1);
+  }
+  GC_CUDA(cudaMalloc(&b->member_table, sizeof(Member<T>) * b->n));
+  GC_CUDA(cudaMemcpy(b->member_table, tab.data(), sizeof(Member<T>) * b->n, cudaMemcpyHostToDevice));
+  return GC_OK;
+}
+
+template <class T>
+gc_status run_batch(gc_ch_batch* b, int n_steps) {
+  gc_status s = build_items(b);
+  if (s != GC_OK) return s;
+  T* state = static_cast<T*>(b->slots[0]);
+  T* other = static_cast<T*>(b->slots[1]);
+  const uint64_t key[8] = {reinterpret_cast<uint64_t>(b) ^ 0xBA7C4ULL, reinterpret_cast<uint64_t>(state),
+                           reinterpret_cast<uint64_t>(b->items), static_cast<uint64_t>(b->n_items),
+                           static_cast<uint64_t>(b->shape), static_cast<uint64_t>(b->order),
+                           sizeof(T), 0xBAULL << 56};
+  return run_steps<T>(b->ctx, state, other, sizeof(T) * b->total, n_steps, key,
+                      [&](const T* src, T* dst) { return batch_step<T>(b, src, dst); });
+}
+
+template <class T>
+gc_status diag_batch(gc_ch_batch* b, double* mass, double* energy) {
+  if (!b->diag_items) {
+    std::vector<int2> items;
+    std::vector<int> first(b->n + 1, 0);
+    for (int m = 0; m < b->n; ++m) {
+      first[m] = static_cast<int>(items.size());
+      const long long cells = static_cast<long long>(b->members[m].nx) * b->members[m].ny;
+      const int chunks = static_cast<int>((cells + kDiagChunk - 1) / kDiagChunk);
+      for (int c = 0; c < chunks; ++c) items.push_back(make_int2(m, c));
+    }
+    first[b->n] = static_cast<int>(items.size());
+    b->n_diag_items = static_cast<int>(items.size());
+    GC_CUDA(cudaMalloc(&b->diag_items, sizeof(int2) * items.size()));
+    GC_CUDA(cudaMemcpy(b->diag_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+    GC_CUDA(cudaMalloc(&b->diag_first, sizeof(int) * first.size()));
+    GC_CUDA(cudaMemcpy(b->diag_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    GC_CUDA(cudaMalloc(&b->diag_part, sizeof(double) * 4 * items.size()));
+    GC_CUDA(cudaMalloc(&b->diag_result, sizeof(double) * 2 * b->n));
+  }
+  const int grid = std::min(b->n_diag_items, b->ctx->num_sms * 8);
+  batch_diag_kernel<T><<<grid, kDiagThreads, 0, b->ctx->stream>>>(
+      static_cast<const Member<T>*>(b->member_table), static_cast<const int2*>(b->diag_items), b->n_diag_items,
+      static_cast<const T*>(b->slots[0]), static_cast<double*>(b->diag_part));
+  GC_CHECK_LAUNCH("batch_diag_kernel");
+  batch_diag_final<<<div_up(b->n, 128), 128, 0, b->ctx->stream>>>(
+      static_cast<const int*>(b->diag_first), b->n, static_cast<const double*>(b->diag_part),
+      static_cast<double*>(b->diag_result));
+  GC_CHECK_LAUNCH("batch_diag_final");
+  std::vector<double> r(2 * b->n);
+  GC_CUDA(cudaMemcpyAsync(r.data(), b->diag_result, sizeof(double) * 2 * b->n, cudaMemcpyDeviceToHost,
+                          b->ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(b->ctx->stream));
+  for (int m = 0; m < b->n; ++m) {
+    if (mass) mass[m] = r[2 * m];        // h = 1: cell volume 1
+    if (energy) energy[m] = r[2 * m + 1];
+  }
+  return GC_OK;
+}
+
+std::string signature(const gc_ch_batch* b) {
+  unsigned long long h = 1469598103934665603ULL;
+  auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ULL; };
+  mix(static_cast<unsigned long long>(b->n));
+  mix(static_cast<unsigned long long>(b->order));
+  mix(static_cast<unsigned long long>(b->dtype));
+  for (const auto& m : b->members) {
+    mix(static_cast<unsigned long long>(m.nx));
+    mix(static_cast<unsigned long long>(m.ny));
+  }
+  char buf[32];
+  std::snprintf(buf, sizeof buf, "%016llx", h);
+  return buf;
+}
+
+}  // namespace
+}  // namespace gcb
+
+extern "C" {
+
+GC_API gc_status gc_ch_batch_create(gc_context* ctx, int32_t n, const gc_ch_member* members, int32_t order,
+                                    gc_dtype dt, gc_ch_batch** out) {
+  Call call(ctx);
+  if (call.st != GC_OK) return call.st;
+  if (!out || !members || n <= 0) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_create: need n > 0 members");
+  *out = nullptr;
+  if (order != 2 && order != 4 && order != 6)
+    return fail(GC_ERR_UNSUPPORTED, "gc_ch_batch_create: order must be 2, 4 or 6");
+  if (dt != GC_F32 && dt != GC_F64) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_create: unknown dtype");
+  const int R = order / 2;
+  for (int m = 0; m < n; ++m) {
+    const gc_ch_member& s = members[m];
+    gc_grid g{s.nx, s.ny, 1, 1.0, 1.0, 1.0};
+    gc_status st = require_axes(&g, R);
+    if (st != GC_OK) return fail(st, "gc_ch_batch_create: member " + std::to_string(m) + ": " + gc_last_error());
+    if (!(s.dt >= 0.0)) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_create: member " + std::to_string(m) + ": dt must be >= 0");
+  }
+  gc_ch_batch* b = new gc_ch_batch();
+  b->ctx = ctx;
+  b->n = n;
+  b->order = order;
+  b->dtype = dt;
+  b->members.assign(members, members + n);
+  b->offsets.resize(n + 1);
+  long long off = 0;
+  for (int m = 0; m < n; ++m) {
+    b->offsets[m] = off;
+    const long long cells = static_cast<long long>(members[m].nx) * members[m].ny;
+    off += (cells + 63) / 64 * 64;
+  }
+  b->offsets[n] = off;
+  b->total = off;
+  const size_t es = dtype_size(dt);
+  for (int k = 0; k < 5; ++k) {
+    cudaError_t e = cudaMalloc(&b->slots[k], es * static_cast<size_t>(off));
+    if (e != cudaSuccess) {
+      for (int j = 0; j < k; ++j) cudaFree(b->slots[j]);
+      delete b;
+      return cuda_fail(e, "gc_ch_batch_create: cudaMalloc");
+    }
+  }
+  cudaMemsetAsync(b->slots[0], 0, es * static_cast<size_t>(off), ctx->stream);
+  gc_status st = dt == GC_F32 ? upload_members<float>(b) : upload_members<double>(b);
+  if (st != GC_OK) {
+    gc_ch_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return GC_OK;
+}
+
+GC_API gc_status gc_ch_batch_destroy(gc_ch_batch* b) {
+  if (!b) return GC_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  for (auto& p : b->slots)
+    if (p) cudaFree(p);
+  for (void* p : {b->member_table, b->items, b->diag_items, b->diag_first, b->diag_part, b->diag_result})
+    if (p) cudaFree(p);
+  delete b;
+  return GC_OK;
+}
+
+GC_API gc_status gc_ch_batch_offsets(gc_ch_batch* b, int64_t* offsets) {
+  if (!b || !offsets) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_offsets: null pointer");
+  for (int m = 0; m <= b->n; ++m) offsets[m] = b->offsets[m];
+  return GC_OK;
+}
+
+GC_API gc_status gc_ch_batch_state(gc_ch_batch* b, void** dev) {
+  if (!b || !dev) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_state: null pointer");
+  *dev = b->slots[0];
+  return GC_OK;
+}
+
+GC_API gc_status gc_ch_batch_run(gc_ch_batch* b, int32_t n_steps) {
+  if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_run: null batch");
+  Call call(b->ctx);
+  if (call.st != GC_OK) return call.st;
+  if (n_steps < 0) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_run: n_steps must be >= 0");
+  if (n_steps == 0) return GC_OK;
+  return b->dtype == GC_F32 ? run_batch<float>(b, n_steps) : run_batch<double>(b, n_steps);
+}
+
+GC_API gc_status gc_ch_batch_diagnostics(gc_ch_batch* b, double* mass, double* free_energy) {
+  if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_diagnostics: null batch");
+  Call call(b->ctx);
+  if (call.st != GC_OK) return call.st;
+  return b->dtype == GC_F32 ? diag_batch<float>(b, mass, free_energy) : diag_batch<double>(b, mass, free_energy);
+}
+
+GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, const char* cache_path,
+                                      char* report, size_t report_len) {
+  if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_autotune: null batch");
+  Call call(b->ctx);
+  if (call.st != GC_OK) return call.st;
+  char dev_name[256] = "unknown";
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, b->ctx->device) == cudaSuccess) std::snprintf(dev_name, sizeof dev_name, "%s", prop.name);
+  const std::string sig = signature(b);
+  // The cache is a JSON object {"<device>|<ensemble signature>": {"shape": k,
+  // "choice": "TWxTYxNTY", "trials_ms_per_step": {...}}, ...}; a matching
+  // entry skips the trials.
+  const std::string key = "\"" + std::string(dev_name) + "|" + sig + "\"";
+  std::string cache_text;
+  if (cache_path && *cache_path) {
+    if (FILE* f = std::fopen(cache_path, "r")) {
+      char chunk[4096];
+      size_t got;
+      while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) cache_text.append(chunk, got);
+      std::fclose(f);
+      const size_t pos = cache_text.find(key + ": {\"shape\": ");
+      if (pos != std::string::npos) {
+        const int shape = std::atoi(cache_text.c_str() + pos + key.size() + 12);
+        if (shape >= 0 && shape < kNumShapes) {
+          b->shape = shape;
+          b->tune_report = "{\"cached\": true, \"shape\": " + std::to_string(shape) + "}";
+          if (report && report_len) std::snprintf(report, report_len, "%s", b->tune_report.c_str());
+          return GC_OK;
+        }
+      }
+    }
+  }
+  const int steps = steps_per_trial > 0 ? steps_per_trial : 8;
+  const size_t bytes = dtype_size(b->dtype) * static_cast<size_t>(b->total);
+  void* saved = nullptr;
+  GC_CUDA(cudaMalloc(&saved, bytes));
+  GC_CUDA(cudaMemcpyAsync(saved, b->slots[0], bytes, cudaMemcpyDeviceToDevice, b->ctx->stream));
+  cudaEvent_t e0, e1;
+  GC_CUDA(cudaEventCreate(&e0));
+  GC_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_shape = b->shape;
+  std::string rep = "{";
+  gc_status st = GC_OK;
+  for (int shp = 0; shp < kNumShapes && st == GC_OK; ++shp) {
+    b->shape = shp;
+    // warm-up (captures the step graph for this shape), then a timed trial
+    st = b->dtype == GC_F32 ? run_batch<float>(b, steps) : run_batch<double>(b, steps);
+    if (st != GC_OK) break;
+    cudaEventRecord(e0, b->ctx->stream);
+    st = b->dtype == GC_F32 ? run_batch<float>(b, steps) : run_batch<double>(b, steps);
+    cudaEventRecord(e1, b->ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const TileShape s = kShapes[shp];
+    char item[128];
+    std::snprintf(item, sizeof item, "%s\"%dx%dx%d\": %.4f", shp ? ", " : "", s.tw, s.ty, s.nty, ms / steps);
+    rep += item;
+    if (ms < best) {
+      best = ms;
+      best_shape = shp;
+    }
+    GC_CUDA(cudaMemcpyAsync(b->slots[0], saved, bytes, cudaMemcpyDeviceToDevice, b->ctx->stream));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(b->ctx->stream);
+  cudaFree(saved);
+  if (st != GC_OK) return st;
+  b->shape = best_shape;
+  const TileShape s = kShapes[best_shape];
+  char tail[160];
+  std::snprintf(tail, sizeof tail, "}, \"choice\": \"%dx%dx%d\", \"ms_per_step\": %.4f}", s.tw, s.ty, s.nty,
+                best / steps);
+  b->tune_report = "{\"trials_ms_per_step\": " + rep + tail;
+  if (cache_path && *cache_path) {
+    const std::string entry = key + ": {\"shape\": " + std::to_string(best_shape) + ", \"choice\": \"" +
+                              std::to_string(s.tw) + "x" + std::to_string(s.ty) + "x" + std::to_string(s.nty) +
+                              "\", \"trials_ms_per_step\": " + rep + "}}";
+    const size_t close = cache_text.rfind('}');
+    std::string text;
+    if (close == std::string::npos || cache_text.find('{') == std::string::npos) text = "{\n" + entry + "\n}\n";
+    else text = cache_text.substr(0, close) + ",\n" + entry + "\n}\n";
+    if (FILE* f = std::fopen(cache_path, "w")) {
+      std::fwrite(text.data(), 1, text.size(), f);
+      std::fclose(f);
+    }
+  }
+  if (report && report_len) std::snprintf(report, report_len, "%s", b->tune_report.c_str());
+  return GC_OK;
+}
+
+}  // extern "C"

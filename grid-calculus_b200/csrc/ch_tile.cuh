@@ -1,0 +1,235 @@
+// Cahn-Hilliard stage building blocks shared by the single-grid drivers
+// (ch.cu) and the batched ensemble (ch_batch.cu): stage parameters, the
+// reference-ordered RHS arithmetic, the 2-D strip-tile geometry and the
+// cp.async-pipelined persistent tile loop.
+#pragma once
+
+#include "common.cuh"
+
+namespace gcb {
+namespace {
+
+enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+
+template <class T>
+struct StageParams {
+  const T* psi;    // state
+  const T* kin;    // previous stage (y = psi + a kin), nullptr for y = psi
+  T a;             // stage coefficient
+  T* out;          // k_s (MODE_RHS) or psi' (final modes)
+  const T* k1;     // MODE_RK4_FINAL only
+  const T* k2;
+  const T* k3;
+  T c6, c3;        // dt/6, dt/3 (RK4 final) ; c6 = dt (Euler final)
+  T mob, kappa;
+  T ihx2, ihy2, ihz2;
+  int nx, ny, nz;
+  // Exact shortcuts: x * 1 == x, so a unit spacing, mobility or kappa
+  // skips its multiply without changing a bit.
+  bool unit_h, unit_m, unit_k;
+};
+
+// (ax / hx^2 + ay / hy^2) [+ az / hz^2], as the reference combines the axes.
+template <class T>
+__device__ __forceinline__ T lap_xy(const StageParams<T>& p, T ax, T ay) {
+  return p.unit_h ? Ar<T>::add(ax, ay) : Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2));
+}
+template <class T>
+__device__ __forceinline__ T lap_z(const StageParams<T>& p, T lap, T az) {
+  return Ar<T>::add(lap, p.unit_h ? az : Ar<T>::mul(az, p.ihz2));
+}
+// mu = -y + y^3 - kappa lap(y)
+template <class T>
+__device__ __forceinline__ T chem_pot(const StageParams<T>& p, T y, T lap) {
+  return Ar<T>::sub(Ar<T>::add(-y, Ar<T>::mul(Ar<T>::mul(y, y), y)), p.unit_k ? lap : Ar<T>::mul(p.kappa, lap));
+}
+template <class T>
+__device__ __forceinline__ T mobility(const StageParams<T>& p, T lap) {
+  return p.unit_m ? lap : Ar<T>::mul(lap, p.mob);
+}
+
+// ---------------------------------------------------------------------------
+// 2-D strip-tile geometry (Nz == 1), used by the TMA kernel (ch.cu), the
+// cp.async-pipelined loop below and the ensemble.  64 x 4 threads; the mu
+// region is exactly 64 columns wide (output tile 64 - 2R columns by 16
+// rows).  In the mu and output phases a thread owns one column and a strip
+// of consecutive rows: y-direction taps come from a register window of its
+// own column (one new shared-memory value per row), only the x taps are
+// read from neighbouring columns -- in double precision every warp-wide
+// shared read is two wavefronts, and this halves the shared-memory reads
+// per cell that bounded a plain tiled layout.
+constexpr int kT2W = 64;   // mu-region columns = threads in x
+constexpr int kT2Y = 16;   // output rows
+constexpr int kT2TY = 4;   // thread rows
+
+// ---------------------------------------------------------------------------
+// Software-pipelined persistent tile loop.  A CTA walks a list of work
+// items (a grid tile, or a (member, tile) of an ensemble); before computing
+// item k it issues cp.async copies of item k+1's y-region inputs (psi and
+// k_prev, wrapped per element) into the other half of a double buffer, so
+// global-memory latency overlaps the previous item's arithmetic.  Each
+// thread forms y from exactly the elements it copied, so its own
+// cp.async.wait_group suffices before that pass.  Arithmetic as strip_tile.
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem, int bytes) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class T, int ORDER, int TW, int TY>
+constexpr size_t pipe_smem() {
+  constexpr int R = W<2, ORDER>::R;
+  constexpr size_t yn = static_cast<size_t>(TW + 2 * R) * (TY + 4 * R);
+  return sizeof(T) * (4 * yn + yn + static_cast<size_t>(TW) * (TY + 2 * R));
+}
+
+// Source: get(k, p, x0, y0) fills the stage parameters and tile origin of
+// item k; count() is the number of items.
+template <class T, int ORDER, int MODE, int TW, int TY, int NTY, class Source>
+__device__ __forceinline__ void pipelined_tiles(const Source& src, unsigned char* smem) {
+  constexpr int R = W<2, ORDER>::R;
+  constexpr int TX = TW - 2 * R;
+  constexpr int YX = TX + 4 * R, YY = TY + 4 * R;
+  constexpr int MX = TW, MY = TY + 2 * R;
+  constexpr int NW = 2 * R + 1;
+  constexpr int MS = (MY + NTY - 1) / NTY;
+  constexpr int OS = (TY + NTY - 1) / NTY;
+  constexpr int YN = YX * YY;
+  T* raw = reinterpret_cast<T*>(smem);            // [2 buffers][psi, kin][YY][YX]
+  T* ysb = raw + 4 * YN;                          // y region
+  T* ms = ysb + YN;                               // mu region [MY][MX]
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int n_items = src.count();
+
+  auto issue = [&](int k, int b) {
+    StageParams<T> p;
+    int x0, y0;
+    src.get(k, p, x0, y0);
+    T* rp = raw + (2 * b) * YN;
+    T* rk = raw + (2 * b + 1) * YN;
+    const int gxa = wrap(x0 - 2 * R + tx, p.nx);
+    const bool has_b = tx < YX - TW;
+    const int gxb = wrap(x0 - 2 * R + TW + tx, p.nx);
+#pragma unroll
+    for (int ry = ty; ry < YY; ry += NTY) {
+      const size_t row = static_cast<size_t>(wrap(y0 - 2 * R + ry, p.ny)) * p.nx;
+      cp_async_elem(rp + ry * YX + tx, p.psi + row + gxa, sizeof(T));
+      if (p.kin) cp_async_elem(rk + ry * YX + tx, p.kin + row + gxa, sizeof(T));
+      if (has_b) {
+        cp_async_elem(rp + ry * YX + TW + tx, p.psi + row + gxb, sizeof(T));
+        if (p.kin) cp_async_elem(rk + ry * YX + TW + tx, p.kin + row + gxb, sizeof(T));
+      }
+    }
+    if constexpr (MODE == MODE_RK4_FINAL) {
+      // k1, k2 at this thread's output cells of item k: into L2 now.
+      if (tx < TX && x0 + tx < p.nx) {
+#pragma unroll
+        for (int q = 0; q < OS; ++q) {
+          const int oy = ty * OS + q;
+          if (oy < TY && y0 + oy < p.ny) {
+            const size_t gi = static_cast<size_t>(y0 + oy) * p.nx + (x0 + tx);
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k1 + gi));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(p.k2 + gi));
+          }
+        }
+      }
+    }
+  };
+
+  if (blockIdx.x < n_items) issue(blockIdx.x, 0);
+  cp_async_commit();
+  int i = 0;
+  for (int k = blockIdx.x; k < n_items; k += gridDim.x, ++i) {
+    const int b = i & 1;
+    if (k + static_cast<int>(gridDim.x) < n_items) issue(k + gridDim.x, b ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();  // this item's copies (this thread's) have landed
+    StageParams<T> p;
+    int x0, y0;
+    src.get(k, p, x0, y0);
+    const T* rp = raw + (2 * b) * YN;
+    const T* rk = raw + (2 * b + 1) * YN;
+    const T* ys = rp;
+    if (p.kin) {
+      const bool has_b = tx < YX - TW;
+#pragma unroll
+      for (int ry = ty; ry < YY; ry += NTY) {
+        const int e = ry * YX + tx;
+        ysb[e] = Ar<T>::add(rp[e], Ar<T>::mul(p.a, rk[e]));
+        if (has_b) ysb[e + TW] = Ar<T>::add(rp[e + TW], Ar<T>::mul(p.a, rk[e + TW]));
+      }
+      ys = ysb;
+    }
+    __syncthreads();
+
+    // Phase 2: mu.
+    {
+      const int m0 = ty * MS;
+      const int m1 = min(m0 + MS, MY);
+      const int cx = tx + R;
+      T win[NW];
+      if (m0 < MY) {
+#pragma unroll
+        for (int q = 0; q < 2 * R; ++q) win[q + 1] = ys[(m0 + q) * YX + cx];
+      }
+#pragma unroll
+      for (int q = 0; q < MS; ++q) {
+        const int m = m0 + q;
+        if (m < m1) {
+#pragma unroll
+          for (int z = 0; z + 1 < NW; ++z) win[z] = win[z + 1];
+          win[NW - 1] = ys[(m + 2 * R) * YX + cx];
+          const T yc = win[R];
+          const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? yc : ys[(m + R) * YX + cx + o]; });
+          const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+          T lap = lap_xy(p, ax, ay);
+          if constexpr (ORDER != 2) lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return yc; }));
+          ms[m * MX + tx] = chem_pot(p, yc, lap);
+        }
+      }
+    }
+    __syncthreads();
+
+    // Phase 3: output strip.
+    const int o0 = ty * OS;
+    if (tx < TX && x0 + tx < p.nx && o0 < TY) {
+      const int cx = tx + R;
+      T win[NW];
+#pragma unroll
+      for (int q = 0; q < 2 * R; ++q) win[q + 1] = ms[(o0 + q) * MX + cx];
+#pragma unroll
+      for (int q = 0; q < OS; ++q) {
+        const int oy = o0 + q;
+        if (oy >= TY) break;
+#pragma unroll
+        for (int z = 0; z + 1 < NW; ++z) win[z] = win[z + 1];
+        win[NW - 1] = ms[(oy + 2 * R) * MX + cx];
+        if (y0 + oy >= p.ny) break;
+        const T mc = win[R];
+        const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? mc : ms[(oy + R) * MX + cx + o]; });
+        const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+        T lap = lap_xy(p, ax, ay);
+        if constexpr (ORDER != 2) lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return mc; }));
+        const T rhs = mobility(p, lap);
+        const size_t gi = static_cast<size_t>(y0 + oy) * p.nx + (x0 + tx);
+        const int yc_idx = (oy + 2 * R) * YX + (tx + 2 * R);
+        if constexpr (MODE == MODE_RHS) {
+          p.out[gi] = rhs;
+        } else if constexpr (MODE == MODE_RK4_FINAL) {
+          const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
+          const T s23 = Ar<T>::add(__ldg(p.k2 + gi), rk[yc_idx]);
+          p.out[gi] = Ar<T>::add(rp[yc_idx], Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+        } else {
+          p.out[gi] = Ar<T>::add(rp[yc_idx], Ar<T>::mul(p.c6, rhs));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+}  // namespace
+}  // namespace gcb

@@ -23,7 +23,7 @@ __all__ = [
     "Pairwise", "Kahan", "RK4", "ExplicitEuler", "CahnHilliardRhs",
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
-    "d_max_face", "version",
+    "d_max_face", "version", "ChBatch",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -80,6 +80,22 @@ _SIGS = {
     "gc_diffuse_fvm": [_vp, _gp, _i32, _vp, _vp, _dbl, _i32, _i32, C.POINTER(C.c_int64)],
     "gc_d_max_face": [_vp, _gp, _i32, _vp, C.POINTER(C.c_double)],
 }
+
+
+class gc_ch_member(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("mobility", C.c_double),
+                ("kappa", C.c_double), ("dt", C.c_double)]
+
+
+_SIGS.update({
+    "gc_ch_batch_create": [_vp, C.c_int32, C.POINTER(gc_ch_member), C.c_int32, _i32, C.POINTER(C.c_void_p)],
+    "gc_ch_batch_destroy": [_vp],
+    "gc_ch_batch_offsets": [_vp, C.POINTER(C.c_int64)],
+    "gc_ch_batch_state": [_vp, C.POINTER(C.c_void_p)],
+    "gc_ch_batch_run": [_vp, C.c_int32],
+    "gc_ch_batch_diagnostics": [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    "gc_ch_batch_autotune": [_vp, C.c_int32, C.c_char_p, C.c_char_p, C.c_size_t],
+})
 for _name, _args in _SIGS.items():
     _f = getattr(lib, _name)
     _f.argtypes = _args
@@ -365,3 +381,79 @@ def d_max_face(D, grid: Grid, ctx=None) -> float:
     r = C.c_double()
     _check(lib.gc_d_max_face(_ctx(ctx), C.byref(grid.c()), _dtype_code(D), D.data_ptr(), C.byref(r)))
     return r.value
+
+
+class ChBatch:
+    """Batched Cahn-Hilliard ensemble (gc_ch_batch_*): independent 2-D members
+    of uneven size, each with its own mobility, kappa and dt, advanced
+    together.  `members` is a list of (nx, ny, mobility, kappa, dt)."""
+
+    def __init__(self, members, order: int = 4, dtype=None, ctx=None):
+        import torch
+        dtype = dtype or torch.float32
+        self.ctx = ctx or context()
+        self.dtype = dtype
+        self.members = [tuple(m) for m in members]
+        arr = (gc_ch_member * len(members))(*[gc_ch_member(int(a), int(b), float(c), float(d), float(e))
+                                              for a, b, c, d, e in self.members])
+        h = C.c_void_p()
+        _check(lib.gc_ch_batch_create(self.ctx.handle, len(members), arr, order,
+                                      F64 if dtype == torch.float64 else F32, C.byref(h)))
+        self.handle = h
+        offs = (C.c_int64 * (len(members) + 1))()
+        _check(lib.gc_ch_batch_offsets(h, offs))
+        self.offsets = list(offs)
+        ptr = C.c_void_p()
+        _check(lib.gc_ch_batch_state(h, C.byref(ptr)))
+        self.state_ptr = ptr.value
+
+    def set_member(self, i: int, values) -> None:
+        """Copies a (ny, nx) host or device array into member i."""
+        import torch
+        t = torch.as_tensor(values, dtype=self.dtype).contiguous()
+        n = self.members[i][0] * self.members[i][1]
+        assert t.numel() == n
+        esize = t.element_size()
+        dst = self.state_ptr + self.offsets[i] * esize
+        host = t.cpu().contiguous()
+        _check(lib.gc_memcpy_h2d(self.ctx.handle, dst, host.data_ptr(), n * esize))
+        self.ctx.synchronize()
+
+    def get_member(self, i: int):
+        """Member i as a (ny, nx) float64 numpy array."""
+        import numpy as np
+        import torch
+        nx, ny = self.members[i][0], self.members[i][1]
+        out = torch.empty((ny, nx), dtype=self.dtype)
+        esize = out.element_size()
+        _check(lib.gc_memcpy_d2h(self.ctx.handle, out.data_ptr(), self.state_ptr + self.offsets[i] * esize,
+                                 nx * ny * esize))
+        return out.double().numpy()
+
+    def run(self, n_steps: int) -> None:
+        _check(lib.gc_ch_batch_run(self.handle, n_steps))
+
+    def diagnostics(self):
+        """(mass, free_energy) per member, FP64 (reference convention)."""
+        n = len(self.members)
+        m = (C.c_double * n)()
+        f = (C.c_double * n)()
+        _check(lib.gc_ch_batch_diagnostics(self.handle, m, f))
+        return list(m), list(f)
+
+    def autotune(self, steps_per_trial: int = 8, cache_path: str | None = None) -> str:
+        buf = C.create_string_buffer(4096)
+        _check(lib.gc_ch_batch_autotune(self.handle, steps_per_trial,
+                                        cache_path.encode() if cache_path else None, buf, 4096))
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.gc_ch_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

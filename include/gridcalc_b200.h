@@ -202,6 +202,41 @@ GC_API gc_status gc_diffuse_fvm(gc_context* ctx, const gc_grid* g, gc_dtype dt, 
 GC_API gc_status gc_d_max_face(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* D,
                                double* result);
 
+/* ---- batched Cahn-Hilliard ensemble --------------------------------------
+ * No reference counterpart as one call: it replaces a loop over independent
+ * solve::integrate(psi_i, computeRhs, dt_i, n, RK4{}) runs
+ * (solve/RK4.hpp:99-154, examples/common/cahn_hilliard.hpp:38-59), each
+ * member on its own 2-D periodic grid with h = 1 and its own mobility, kappa
+ * and time step, all at one Laplacian order and storage type.  Members'
+ * fields are packed in one device buffer: member i occupies elements
+ * [offsets[i], offsets[i] + nx*ny) (i fastest) of gc_ch_batch_state(). */
+typedef struct gc_ch_member {
+  int32_t nx, ny;
+  double mobility, kappa, dt;
+} gc_ch_member;
+
+typedef struct gc_ch_batch gc_ch_batch;
+
+GC_API gc_status gc_ch_batch_create(gc_context* ctx, int32_t n, const gc_ch_member* members,
+                                    int32_t order, gc_dtype dt, gc_ch_batch** out);
+GC_API gc_status gc_ch_batch_destroy(gc_ch_batch* b);
+/* n + 1 element offsets of the members in the packed state. */
+GC_API gc_status gc_ch_batch_offsets(gc_ch_batch* b, int64_t* offsets);
+/* Device pointer to the packed state (fill it with gc_memcpy_h2d). */
+GC_API gc_status gc_ch_batch_state(gc_ch_batch* b, void** dev);
+/* Advances every member by n_steps RK4 steps: four persistent launches per
+ * step cover the whole ensemble; steps replay from a captured CUDA graph. */
+GC_API gc_status gc_ch_batch_run(gc_ch_batch* b, int32_t n_steps);
+/* Per-member mass and free energy (reference convention, order-2 gradient),
+ * accumulated in double with compensated sums in a fixed order. */
+GC_API gc_status gc_ch_batch_diagnostics(gc_ch_batch* b, double* mass, double* free_energy);
+/* Times each compiled tile shape on the ensemble (steps_per_trial steps each,
+ * state restored afterwards) and keeps the fastest; with cache_path, reuses
+ * or records the choice in a JSON file keyed by device and ensemble.  A JSON
+ * report of the trials is written to report. */
+GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, const char* cache_path,
+                                      char* report, size_t report_len);
+
 #ifdef __cplusplus
 }
 #endif

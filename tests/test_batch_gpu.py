@@ -1,0 +1,107 @@
+"""Batched Cahn-Hilliard ensemble: members of uneven size, each with its own
+kappa, mobility and dt.  In double the ensemble runs the same tile
+arithmetic as the single-grid path, so every member must be bit-identical
+to the oracle run on that member alone; in float the error against the
+double oracle is bounded; per-member FP64 mass and free energy agree with
+the oracle; the autotuner picks a shape and records it in a JSON cache."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [  # (nx, ny, mobility, kappa, dt)
+    (16, 16, 1.0, 1.0, 0.004), (80, 48, 1.0, 0.5, 0.008), (64, 64, 0.7, 2.0, 0.002),
+    (33, 17, 1.0, 1.3, 0.003), (144, 96, 1.0, 0.9, 0.005), (1, 40, 1.0, 1.0, 0.004),
+]
+
+
+def stable_dt(kappa, order=4):
+    lam = 2 * (16 / 3 if order == 4 else 4.0)
+    return 0.5 * 2.7853 / (lam * (kappa * lam + 2))
+
+
+def ics(members, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for nx, ny, *_ in members:
+        cbar = rng.uniform(-0.4, 0.4)
+        out.append(cbar + 0.05 * (2 * rng.random((ny, nx)) - 1))
+    return out
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_f64_ensemble_bit_exact_per_member(gc, oracle, order):
+    import torch
+    b = gc.ChBatch(MEMBERS, order=order, dtype=torch.float64)
+    init = ics(MEMBERS)
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    b.run(37)
+    for i, (nx, ny, mob, kap, dt) in enumerate(MEMBERS):
+        want = oracle.ch_integrate(order, mob, kap, init[i].reshape(1, ny, nx), dt, 37)
+        assert np.array_equal(b.get_member(i), want.reshape(ny, nx)), i
+    b.close()
+
+
+def test_f32_ensemble_error_and_diagnostics(gc, oracle):
+    import torch
+    members = [(nx, ny, 1.0, kap, stable_dt(kap)) for nx, ny, kap in
+               [(64, 64, 0.5), (96, 80, 1.2), (128, 128, 2.0), (48, 112, 0.8)]]
+    b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    init = [c.astype(np.float32).astype(np.float64) for c in ics(members, seed=11)]
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    steps = 300
+    b.run(steps)
+    mass, energy = b.diagnostics()
+    for i, (nx, ny, mob, kap, dt) in enumerate(members):
+        want = oracle.ch_integrate(4, mob, kap, init[i].reshape(1, ny, nx), dt, steps)
+        got = b.get_member(i).reshape(1, ny, nx)
+        l2 = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert l2 < 1e-4, (i, l2)
+        f_ref = oracle.ch_free_energy(want, kap)
+        v4 = nx * ny / 4.0
+        # BASELINE convention F + V/4 (f = (c^2 - 1)^2 / 4)
+        assert abs((energy[i] + v4) - (f_ref + v4)) / abs(f_ref + v4) < 1e-4, (i, energy[i], f_ref)
+        m_ref = float(init[i].sum())
+        assert abs(mass[i] - m_ref) < 1e-6 * nx * ny, (i, mass[i], m_ref)  # mean drift < 1e-6
+    b.close()
+
+
+def test_diagnostics_match_oracle_f64(gc, oracle):
+    import torch
+    b = gc.ChBatch(MEMBERS[:5], order=4, dtype=torch.float64)
+    init = ics(MEMBERS[:5], seed=5)
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    mass, energy = b.diagnostics()
+    for i, (nx, ny, mob, kap, dt) in enumerate(MEMBERS[:5]):
+        c = init[i].reshape(1, ny, nx)
+        assert abs(mass[i] - oracle.integrate(c)) <= 1e-13 * np.abs(c).sum()
+        f = oracle.ch_free_energy(c, kap)
+        assert abs(energy[i] - f) <= 1e-13 * max(1.0, abs(f))
+    b.close()
+
+
+def test_autotune_and_cache(gc, oracle, tmp_path):
+    import torch
+    members = [(nx, nx, 1.0, 1.0, stable_dt(1.0)) for nx in (64, 96, 160, 256)]
+    b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    init = ics(members, seed=2)
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    cache = str(tmp_path / "tune.json")
+    report = json.loads(b.autotune(steps_per_trial=4, cache_path=cache))
+    assert set(report["trials_ms_per_step"]) == {"32x16x4", "64x8x4", "64x16x4", "64x32x8"}
+    assert report["choice"] in report["trials_ms_per_step"]
+    # tuning restored the state
+    assert np.array_equal(b.get_member(2), init[2].astype(np.float32).astype(np.float64))
+    cached = json.loads(open(cache).read())
+    assert len(cached) == 1
+    b2 = gc.ChBatch(members, order=4, dtype=torch.float32)
+    assert json.loads(b2.autotune(steps_per_trial=4, cache_path=cache))["cached"] is True
+    b.close()
+    b2.close()
