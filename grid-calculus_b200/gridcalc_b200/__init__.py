@@ -23,7 +23,7 @@ __all__ = [
     "Pairwise", "Kahan", "RK4", "ExplicitEuler", "CahnHilliardRhs",
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
-    "d_max_face", "version", "ChBatch",
+    "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -450,6 +450,124 @@ class ChBatch:
     def close(self) -> None:
         if getattr(self, "handle", None):
             lib.gc_ch_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class gc_corrector_policy(C.Structure):
+    _fields_ = [("dt_fine", C.c_double), ("fine_per_coarse", C.c_int32),
+                ("residual_tol", C.c_double), ("energy_tol", C.c_double)]
+
+
+class gc_corrector_stats(C.Structure):
+    _fields_ = [("accepted", C.c_int64), ("fallbacks", C.c_int64), ("last_residual", C.c_double)]
+
+
+for _name, _args in {
+    "gc_corrector_create": [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)],
+    "gc_corrector_destroy": [_vp],
+    "gc_corrector_set_params": [_vp, C.POINTER(C.c_float), C.c_int32, C.c_float],
+    "gc_corrector_get_params": [_vp, C.POINTER(C.c_float), C.c_int32],
+    "gc_corrector_forward": [_vp, C.c_int32, _i32, _vp, _vp],
+    "gc_corrector_gradient": [_vp, C.c_int32, _vp, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)],
+    "gc_corrector_train_step": [_vp, C.c_int32, _vp, _vp, C.c_float, C.POINTER(C.c_double)],
+    "gc_corrector_advance": [_vp, _gp, C.POINTER(gc_ch_params), _vp, C.c_int32,
+                             C.POINTER(gc_corrector_policy), C.POINTER(gc_corrector_stats)],
+}.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = C.c_int
+lib.gc_corrector_num_params.restype = C.c_int32
+lib.gc_corrector_num_params.argtypes = []
+
+CORRECTOR_LAYERS, CORRECTOR_CHANNELS = 6, 32
+
+
+def corrector_init_params(seed: int = 0, last_scale: float = 0.1):
+    """He-normal initial parameters (FP32) for the corrector: per layer
+    W[9][32 in][32 out] then b[32]; the first layer sees one input channel."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n_c = CORRECTOR_CHANNELS
+    out = []
+    for layer in range(CORRECTOR_LAYERS):
+        fan_in = 9 * (1 if layer == 0 else n_c)
+        w = rng.standard_normal((9, n_c, n_c)) * np.sqrt(2.0 / fan_in)
+        if layer == 0:
+            w[:, 1:, :] = 0.0
+        if layer == CORRECTOR_LAYERS - 1:
+            w *= last_scale
+            w[:, :, 1:] = 0.0
+        out.append(w.ravel())
+        out.append(np.zeros(n_c))
+    return np.concatenate(out).astype(np.float32)
+
+
+class Corrector:
+    """Learned coarse-step corrector (gc_corrector_*): 6-layer periodic 3x3
+    CNN, BF16 on tensor cores, trained by the library's own kernels."""
+
+    def __init__(self, height: int, width: int, max_batch: int = 1, ctx=None):
+        self.ctx = ctx or context()
+        self.shape = (height, width)
+        h = C.c_void_p()
+        _check(lib.gc_corrector_create(self.ctx.handle, height, width, max_batch, C.byref(h)))
+        self.handle = h
+        self.n_params = lib.gc_corrector_num_params()
+        self.s_out = 0.05
+
+    def set_params(self, params, s_out: float = 0.05) -> None:
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == self.n_params
+        self.s_out = s_out
+        _check(lib.gc_corrector_set_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size, s_out))
+
+    def get_params(self):
+        import numpy as np
+        p = np.empty(self.n_params, dtype=np.float32)
+        _check(lib.gc_corrector_get_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+        return p
+
+    def forward(self, c):
+        """Zero-mean correction for a (B, H, W) float32/float64 CUDA tensor."""
+        import torch
+        c = c.contiguous()
+        out = torch.empty(c.shape, dtype=torch.float32, device=c.device)
+        _check(lib.gc_corrector_forward(self.handle, c.shape[0], _dtype_code(c), c.data_ptr(), out.data_ptr()))
+        return out
+
+    def gradient(self, c, target):
+        import numpy as np
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        _check(lib.gc_corrector_gradient(self.handle, c.shape[0], c.contiguous().data_ptr(),
+                                         target.contiguous().data_ptr(),
+                                         g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, c, target, lr: float) -> float:
+        loss = C.c_double()
+        _check(lib.gc_corrector_train_step(self.handle, c.shape[0], c.contiguous().data_ptr(),
+                                           target.contiguous().data_ptr(), lr, C.byref(loss)))
+        return loss.value
+
+    def advance(self, psi, grid: Grid, rhs: "CahnHilliardRhs", n_coarse: int, dt_fine: float = 0.01,
+                fine_per_coarse: int = 16, residual_tol: float = 0.05, energy_tol: float = 0.0):
+        pol = gc_corrector_policy(dt_fine, fine_per_coarse, residual_tol, energy_tol)
+        st = gc_corrector_stats()
+        _check(lib.gc_corrector_advance(self.handle, C.byref(grid.c()), C.byref(rhs.c()), psi.data_ptr(),
+                                        n_coarse, C.byref(pol), C.byref(st)))
+        return {"accepted": st.accepted, "fallbacks": st.fallbacks, "last_residual": st.last_residual}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib.gc_corrector_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

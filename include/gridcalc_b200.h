@@ -237,6 +237,51 @@ GC_API gc_status gc_ch_batch_diagnostics(gc_ch_batch* b, double* mass, double* f
 GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, const char* cache_path,
                                       char* report, size_t report_len);
 
+/* ---- learned coarse-step corrector ---------------------------------------
+ * No reference counterpart.  A 6-layer periodic 3x3 CNN (32 channels, GELU,
+ * BF16 weights and activations, FP32 accumulation on the tensor cores)
+ * maps a 2-D Cahn-Hilliard field c to a zero-mean correction delta so that
+ * c + delta approximates fine_per_coarse plain RK4 steps.  Parameters are
+ * FP32 masters, per layer W[9 taps][32 in][32 out] then b[32], tap t at
+ * offset (t / 3 - 1, t % 3 - 1) in (y, x); delta = s_out (z6 - mean z6)
+ * with z6 the last layer's channel 0. */
+typedef struct gc_corrector gc_corrector;
+
+typedef struct gc_corrector_policy {
+  double dt_fine;           /* fine RK4 step (the plain method's dt) */
+  int32_t fine_per_coarse;  /* fine steps one coarse step replaces */
+  double residual_tol;      /* accept when the trapezoid residual is at most this */
+  double energy_tol;        /* accept when F rises by at most this */
+} gc_corrector_policy;
+
+typedef struct gc_corrector_stats {
+  int64_t accepted;         /* coarse steps taken by the network */
+  int64_t fallbacks;        /* coarse steps taken by plain RK4 instead */
+  double last_residual;
+} gc_corrector_stats;
+
+GC_API gc_status gc_corrector_create(gc_context* ctx, int32_t height, int32_t width, int32_t max_batch,
+                                     gc_corrector** out);
+GC_API gc_status gc_corrector_destroy(gc_corrector* c);
+GC_API int32_t gc_corrector_num_params(void);
+GC_API gc_status gc_corrector_set_params(gc_corrector* c, const float* host, int32_t n, float s_out);
+GC_API gc_status gc_corrector_get_params(gc_corrector* c, float* host, int32_t n);
+/* delta for `batch` fields (batch x height x width, dtype F32 or F64) into
+ * delta_out (device, float). */
+GC_API gc_status gc_corrector_forward(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
+                                      float* delta_out);
+/* Gradient of mean((c + delta(c) - target)^2) w.r.t. all parameters
+ * (host, num_params floats); parameters unchanged. */
+GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, const float* cin, const float* target,
+                                       float* grad_host, double* loss);
+/* One Adam step (beta 0.9 / 0.999) on that loss. */
+GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, const float* cin, const float* target,
+                                         float lr, double* loss);
+/* Learned coarse steps on one double field with the plain-RK4 fallback. */
+GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const gc_ch_params* cp, double* psi,
+                                      int32_t n_coarse, const gc_corrector_policy* pol,
+                                      gc_corrector_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif
