@@ -12,6 +12,15 @@ Multi-GPU (torchrun, one rank per GPU): every rank advances its own replica
 (the method has no data-path exchange at this size: replicas only, weak
 scaling); the time is the max over ranks.
 
+Besides the headline line's `value`, the default single-GPU run measures the
+other forms under "forms" (each outside the headline's timed region, with a
+bounded budget stated in its entry): the operator sweep on 256^3 / 512^3
+Fourier-mode fields with errors against the analytic derivatives, the FVM
+heterogeneous diffusion on 384^3 (FP32, FP64 mass), the batched ensemble of
+256 members (FP32, order 4) with its speedup over the plain path and its
+error against the FP64 oracle, and the learned corrector (training and
+held-out evaluation).  `--forms headline` skips them.
+
 The reference arm (--impl reference) times the reference's own CPU code
 (the reference headers compiled into oracle/_ref/libgcref.so; the C oracle
 port if that build is absent) on the box's host cores: independent replicas
@@ -40,9 +49,9 @@ DT = 0.01
 # k_prev and write k_s, stage 4 reads psi, k1, k2, k3 and writes psi').
 BYTES_PER_CELL_STEP = 13 * 8
 # DRAM bytes (read + write) per RK4 step per cell measured by ncu for the
-# four stage kernels on this workload's kernel (profiles/ch_rk4_fp64_8192.md);
-# None until a capture exists.
-NCU_TRAFFIC_PER_CELL_STEP = None
+# four stage kernels (profiles/ch_rk4_fp64_tma_4096.md: 1630.6 MB per step on
+# 4096^2, both sizes beyond L2, so it scales with the cell count).
+NCU_TRAFFIC_PER_CELL_STEP = 97.2
 
 
 def peaks():
@@ -162,6 +171,236 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Forms beyond the headline (single GPU).
+def _cuda_time(fn, reps=5):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def fourier_field(n, seed, device, dtype):
+    """Sum of 64 modes a cos(2 pi k.x + phi) on the unit cube, |k| <= 16
+    (integer k != 0 drawn uniformly), a ~ N(0, 1), phi ~ U[0, 2 pi); returns
+    the field and its analytic laplacian, biharmonic and gradient."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    modes = []
+    while len(modes) < 64:
+        k = rng.integers(-16, 17, size=3)
+        if 0 < np.dot(k, k) <= 256:
+            modes.append((k, rng.standard_normal(), rng.uniform(0, 2 * np.pi)))
+    x = torch.arange(n, device=device, dtype=torch.float64) / n
+    f = torch.zeros((n, n, n), device=device, dtype=torch.float64)
+    lap, bih = torch.zeros_like(f), torch.zeros_like(f)
+    grad = torch.zeros((3, n, n, n), device=device, dtype=torch.float64)
+    for k, a, phi in modes:
+        ex = torch.exp(1j * (2 * np.pi * k[0] * x + phi))
+        ey = torch.exp(1j * 2 * np.pi * k[1] * x)
+        ez = torch.exp(1j * 2 * np.pi * k[2] * x)
+        e = ez[:, None, None] * ey[None, :, None] * ex[None, None, :]
+        c, sn = e.real, e.imag
+        k2 = float((2 * np.pi) ** 2 * np.dot(k, k))
+        f += a * c
+        lap -= a * k2 * c
+        bih += a * k2 * k2 * c
+        for d, kd in enumerate((k[0], k[1], k[2])):
+            grad[d] -= a * 2 * np.pi * float(kd) * sn
+        del e, c, sn
+    return f.to(dtype), lap, bih, grad
+
+
+def form_operators(gc, peak):
+    import torch
+    out = {}
+    for n in (256, 512):
+        f64, lap_a, bih_a, grad_a = fourier_field(n, 2, "cuda", torch.float64)
+        vec64, div_a = [], torch.zeros_like(f64)
+        for d, sd in enumerate((3, 4, 5)):
+            comp, _, _, gcomp = fourier_field(n, sd, "cuda", torch.float64)
+            vec64.append(comp)
+            div_a += gcomp[d]
+            del gcomp
+        vec64 = torch.stack(vec64)
+        g = gc.Grid(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n)
+        cells = n ** 3
+        rel = lambda a, b: float(torch.linalg.norm(a.double() - b) / torch.linalg.norm(b))
+        for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
+            f, vec = f64.to(dtype), vec64.to(dtype)
+            o, o3 = torch.empty_like(f), torch.empty((3,) + g.shape, dtype=dtype, device="cuda")
+            es = f.element_size()
+            res = {}
+
+            def rec(name, bytes_per_cell, fn, result, analytic):
+                ms = _cuda_time(fn)
+                gbs = bytes_per_cell * es * cells / ms / 1e6
+                res[name] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak, "err_vs_analytic": rel(result, analytic)}
+
+            for order in (2, 4, 6):
+                rec(f"laplacian{order}", 2, lambda: gc.laplacian(f, g, order, o), o, lap_a)
+                rec(f"biharmonic{order}", 2, lambda: gc.biharmonic(f, g, order, o), o, bih_a)
+                rec(f"gradient{order}", 4, lambda: gc.gradient(f, g, order, o3), o3, grad_a)
+                rec(f"divergence{order}", 4, lambda: gc.divergence(vec, g, order, o), o, div_a)
+            ms = _cuda_time(lambda: gc.integrate(f, g))
+            gbs = es * cells / ms / 1e6
+            res["integrate"] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak,
+                                "abs_err_vs_exact_zero": abs(gc.integrate(f, g))}
+            out[f"{tag}_{n}"] = res
+            del f, vec, o, o3
+        del f64, lap_a, bih_a, grad_a, vec64, div_a
+        torch.cuda.empty_cache()
+    return {"workload": "operator sweep, 64 Fourier modes |k|<=16 on the unit cube (seed 2; vector field seeds 3,4,5)",
+            "bytes_per_cell": "laplacian/biharmonic 2s, gradient/divergence 4s, integrate 1s (s = 8 or 4)",
+            "results": out}
+
+
+def form_fvm(gc, peak, steps=500):
+    import numpy as np
+    import torch
+    n = 384
+    g = gc.Grid(n, n, n)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    w = torch.randn((n, n, n), generator=gen, device="cuda", dtype=torch.float64)
+    k = torch.fft.fftfreq(n, device="cuda", dtype=torch.float64) * 2 * np.pi
+    kr = torch.fft.rfftfreq(n, device="cuda", dtype=torch.float64) * 2 * np.pi
+    sigma = 4.0
+    filt = torch.exp(-0.5 * sigma ** 2 * (k[:, None, None] ** 2 + k[None, :, None] ** 2 + kr[None, None, :] ** 2))
+    gfield = torch.fft.irfftn(torch.fft.rfftn(w) * filt, s=(n, n, n))
+    gfield = (gfield - gfield.mean()) / gfield.std()
+    D = torch.exp(gfield).float().contiguous()
+    gen8 = torch.Generator(device="cuda").manual_seed(8)
+    x = torch.arange(n, device="cuda", dtype=torch.float64)
+    r2 = (x - n / 2)[:, None, None] ** 2 + (x - n / 2)[None, :, None] ** 2 + (x - n / 2)[None, None, :] ** 2
+    u = (torch.rand((n, n, n), generator=gen8, device="cuda", dtype=torch.float64) + torch.exp(-r2 / (2 * 16.0 ** 2))).float().contiguous()
+    del w, gfield, r2, filt
+    dmax = gc.d_max_face(D, g)
+    dt = 0.5 * 0.6963 / (dmax * 3.0)
+    m0 = gc.integrate(u, g, gc.Kahan)
+    gc.diffuse(u, g, D, dt, 16, gc.RK4)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    gc.diffuse(u, g, D, dt, steps, gc.RK4)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / steps
+    m1 = gc.integrate(u, g, gc.Kahan)
+    gbs = 68 * n ** 3 / ms / 1e6
+    return {"workload": "FVM heterogeneous diffusion 384^3 FP32, D = exp(GRF sigma 4 cells), RK4 dt = 0.5 CFL",
+            "steps": steps + 16, "dt": dt, "ms_per_step": ms, "Mcell-steps/s": n ** 3 / ms / 1e3,
+            "GB/s": gbs, "frac": gbs / peak, "bytes_per_cell_step": 68,
+            "mass_initial": m0, "mass_final": m1, "mass_drift_rel": (m1 - m0) / m0}
+
+
+def batch_members(seed=11, n=256):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    lam = 2 * 16.0 / 3.0
+    members, ics = [], []
+    for _ in range(n):
+        L = int(16 * round(64 * 16 ** rng.random() / 16))
+        cbar = rng.uniform(-0.4, 0.4)
+        kap = rng.uniform(0.5, 2.0)
+        dt = 0.5 * 2.7853 / (lam * (kap * lam + 2))
+        members.append((L, L, 1.0, kap, dt))
+        ics.append(cbar + 0.05 * (2 * rng.random((L, L)) - 1))
+    return members, ics
+
+
+def form_batched(gc, peak, steps=1000):
+    import numpy as np
+    import torch
+    import oracle_lib
+    members, ics = batch_members()
+    cells = sum(m[0] * m[1] for m in members)
+    b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    for i, c in enumerate(ics):
+        b.set_member(i, c)
+    tune = b.autotune(steps_per_trial=10)
+    for i, c in enumerate(ics):
+        b.set_member(i, c)
+    m0, f0 = b.diagnostics()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    b.run(steps)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / steps
+    m1, f1 = b.diagnostics()
+    rate = cells / ms / 1e3
+    # Plain path member by member (same members, 20 steps each).
+    plain = {}
+    for dtype, tag in ((torch.float32, "plain_f32"), (torch.float64, "plain_f64")):
+        tot = 0.0
+        for (nx, ny, mob, kap, dt), c in zip(members, ics):
+            t = torch.from_numpy(c).to("cuda", dtype)
+            gg = gc.Grid(nx, ny, 1)
+            r = gc.CahnHilliardRhs(mob, kap, 4)
+            gc.ch_integrate(t, gg, r, dt, 4, gc.RK4)
+            torch.cuda.synchronize()
+            s.record()
+            gc.ch_integrate(t, gg, r, dt, 20, gc.RK4)
+            e.record()
+            torch.cuda.synchronize()
+            tot += s.elapsed_time(e) / 20
+        plain[tag] = {"ms_per_step": tot, "Mcell-steps/s": cells / tot / 1e3}
+    # Accuracy against the FP64 oracle on the four smallest members.
+    oracle = oracle_lib.oracle()
+    idx = sorted(range(len(members)), key=lambda i: members[i][0])[:4]
+    errs = []
+    for i in idx:
+        nx, ny, mob, kap, dt = members[i]
+        c0 = ics[i].astype(np.float32).astype(np.float64).reshape(1, ny, nx)
+        want = oracle.ch_integrate(4, mob, kap, c0, dt, steps)
+        got = b.get_member(i).reshape(1, ny, nx)
+        fr = oracle.ch_free_energy(want, kap) + nx * ny / 4.0
+        errs.append({"member": i, "side": nx, "l2_err": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+                     "f_err": abs((f1[i] + nx * ny / 4.0) - fr) / abs(fr)})
+    b.close()
+    drift = max(abs(a - c) / max(1.0, abs(c)) for a, c in zip(m1, m0))
+    return {"workload": "256 CH members, sides log-uniform in [64, 1024] (x16), FP32, order 4, own dt per member",
+            "cells": cells, "steps": steps, "ms_per_step": ms, "Mcell-steps/s": rate,
+            "GB/s": 52 * cells / ms / 1e6, "frac": 52 * cells / ms / 1e6 / peak, "autotune": tune,
+            "plain": plain, "speedup_vs_plain_f32": rate / plain["plain_f32"]["Mcell-steps/s"],
+            "speedup_vs_plain_f64": rate / plain["plain_f64"]["Mcell-steps/s"],
+            "max_mass_drift": drift, "oracle_check_smallest_members": errs}
+
+
+def form_learned(gc, n_train=32, n_eval=4, fine_steps=5000, t_end=200.0, log=None):
+    import gridcalc_b200.learned as L
+    size, batch = 512, 16
+    net = L.new_corrector(size, batch, seed=0)
+    tr = L.train(net, range(1000, 1000 + n_train), size=size, fine_steps=fine_steps, batch=batch, log=log)
+    ev = L.evaluate_heldout(net, range(9000, 9000 + n_eval), size=size, t_end=t_end)
+    net.close()
+    return {"workload": "learned coarse step (dt 0.16 = 16 fine RK4 steps) on 512^2 CH, kappa = M = 1",
+            "budget": f"{n_train} training trajectories x {fine_steps} fine steps, {n_eval} held-out seeds to t = {t_end} "
+                      "(the full configuration uses 512 and 64)",
+            "train": tr, "eval": ev}
+
+
+def run_forms(gc, names, peak):
+    forms = {}
+    table = {"operators": lambda: form_operators(gc, peak), "fvm": lambda: form_fvm(gc, peak),
+             "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc)}
+    for nm in names:
+        t0 = time.perf_counter()
+        try:
+            forms[nm] = table[nm]()
+        except Exception as exc:  # a failing form is reported, the headline stands
+            forms[nm] = {"error": f"{type(exc).__name__}: {exc}"}
+        forms[nm]["wall_s"] = time.perf_counter() - t0
+    return forms
+
+
 def run_ours(args, rank: int, world: int, local: int):
     import numpy as np
     import torch
@@ -240,6 +479,10 @@ def run_ours(args, rank: int, world: int, local: int):
         rate, kind, sample = cpu_sample(1, 2048, 2)
         cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": 1, "kind": kind,
                "sample": f"1 thread, RK4 on 2048x2048, 2 steps ({sample.split(',')[0]})"}
+    forms = None
+    if rank == 0 and world == 1 and args.forms != "headline":
+        names = ["operators", "fvm", "batched", "learned"] if args.forms == "all" else args.forms.split(",")
+        forms = run_forms(gc, [n for n in names if n != "headline"], peaks()[0])
     if rank == 0:
         traffic = None
         if NCU_TRAFFIC_PER_CELL_STEP is not None:
@@ -254,7 +497,8 @@ def run_ours(args, rank: int, world: int, local: int):
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "ch_stage_kernel (4 launches per step, 104 B/cell-step algorithmic)"},
+                         "kernel": "ch_tma_kernel (4 launches per step, 104 B/cell-step algorithmic)",
+                         "traffic_unit": "bytes per launch (average of the 4 stage launches)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": cells * 8 / chunk,
                     "d2h_bytes_per_step": cells * 8 / chunk,
@@ -262,6 +506,8 @@ def run_ours(args, rank: int, world: int, local: int):
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -276,6 +522,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
+    ap.add_argument("--forms", default="all",
+                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -1,0 +1,114 @@
+"""Learned coarse-step workflow for 2-D Cahn-Hilliard (kappa = M = 1).
+
+Trajectories come from the plain GPU solver (FP64 RK4, dt = 0.01); training
+pairs are (c(t), c(t + 16 dt)) taken on the fly along each trajectory, and
+the network is trained by the library's own kernels (Corrector.train_step).
+Evaluation runs held-out seeds to t_end twice -- plain fine RK4 (the
+reference and the "plain form" timing) and learned coarse steps with the
+plain-RK4 fallback -- and reports the relative L2 error, the free-energy
+error (f = (c^2 - 1)^2 / 4 convention: F + V/4), the fallback rate and the
+speedup.  Initial data: c = cbar + U[-0.05, 0.05] with cbar ~ U[-0.3, 0.3],
+one seeded numpy generator per trajectory.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import CahnHilliardRhs, Corrector, Grid, RK4, ch_integrate, corrector_init_params, evaluate
+
+DT_FINE = 0.01
+FINE_PER_COARSE = 16
+
+
+def initial_condition(seed: int, size: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    cbar = rng.uniform(-0.3, 0.3)
+    return cbar + 0.05 * (2.0 * rng.random((size, size)) - 1.0)
+
+
+def train(net: Corrector, seeds, size: int = 512, fine_steps: int = 5000, batch: int = 16,
+          lr: float = 2e-3, lr_final: float = 2e-4, log=None) -> dict:
+    """Trains on trajectories of `fine_steps` fine steps for each seed, `batch`
+    trajectories at a time; one Adam step per coarse interval."""
+    import torch
+    g = Grid(size, size, 1)
+    rhs = CahnHilliardRhs(1.0, 1.0, 2)
+    seeds = list(seeds)
+    groups = [seeds[i:i + batch] for i in range(0, len(seeds), batch)]
+    iters_per_group = fine_steps // FINE_PER_COARSE
+    total = iters_per_group * len(groups)
+    losses, k = [], 0
+    t_data = t_train = 0.0
+    for grp in groups:
+        states = torch.from_numpy(np.stack([initial_condition(s, size) for s in grp])).cuda()
+        for _ in range(iters_per_group):
+            t0 = time.perf_counter()
+            inp = states.float()
+            for b in range(states.shape[0]):
+                ch_integrate(states[b], g, rhs, DT_FINE, FINE_PER_COARSE, RK4)
+            tgt = states.float()
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            frac = k / max(total - 1, 1)
+            rate = lr * (lr_final / lr) ** frac
+            losses.append(net.train_step(inp, tgt, rate))
+            t2 = time.perf_counter()
+            t_data += t1 - t0
+            t_train += t2 - t1
+            k += 1
+            if log and k % 100 == 0:
+                log(f"train iter {k}/{total} loss {losses[-1]:.3e}")
+    return {"iterations": k, "trajectories": len(seeds), "fine_steps": fine_steps, "batch": batch,
+            "loss_first": losses[0], "loss_last": float(np.mean(losses[-10:])),
+            "seconds_data": t_data, "seconds_train": t_train}
+
+
+def _free_energy_baseline(psi, g: Grid) -> float:
+    return evaluate(psi, g, "ch_free_energy", kappa=1.0) + g.size * g.cell_volume / 4.0
+
+
+def evaluate_heldout(net: Corrector, seeds, size: int = 512, t_end: float = 200.0,
+                     residual_tol: float = 0.05, energy_tol: float = 0.0) -> dict:
+    """Fine reference vs learned coarse steps with fallback on each seed."""
+    import torch
+    g = Grid(size, size, 1)
+    rhs = CahnHilliardRhs(1.0, 1.0, 2)
+    n_fine = int(round(t_end / DT_FINE))
+    n_coarse = n_fine // FINE_PER_COARSE
+    l2, ferr, acc, fb = [], [], 0, 0
+    t_fine = t_learned = 0.0
+    for s in seeds:
+        c0 = torch.from_numpy(initial_condition(s, size)).cuda()
+        ref = c0.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ch_integrate(ref, g, rhs, DT_FINE, n_coarse * FINE_PER_COARSE, RK4)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        lrn = c0.clone()
+        st = net.advance(lrn, g, rhs, n_coarse, DT_FINE, FINE_PER_COARSE, residual_tol, energy_tol)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        t_fine += t1 - t0
+        t_learned += t2 - t1
+        acc += st["accepted"]
+        fb += st["fallbacks"]
+        l2.append(float(torch.linalg.norm(lrn - ref) / torch.linalg.norm(ref)))
+        fr, fl = _free_energy_baseline(ref, g), _free_energy_baseline(lrn, g)
+        ferr.append(abs(fl - fr) / abs(fr))
+    cells_steps = len(seeds) * size * size * n_coarse * FINE_PER_COARSE
+    return {"seeds": len(seeds), "t_end": t_end, "coarse_steps": n_coarse * len(seeds),
+            "accepted": acc, "fallbacks": fb, "fallback_rate": fb / max(acc + fb, 1),
+            "l2_err_mean": float(np.mean(l2)), "l2_err_max": float(np.max(l2)),
+            "f_err_mean": float(np.mean(ferr)), "f_err_max": float(np.max(ferr)),
+            "plain_mcell_steps": cells_steps / t_fine / 1e6,
+            "learned_mcell_steps_equiv": cells_steps / t_learned / 1e6,
+            "speedup_vs_plain": t_fine / t_learned}
+
+
+def new_corrector(size: int, batch: int, seed: int = 0) -> Corrector:
+    net = Corrector(size, size, max_batch=batch)
+    net.set_params(corrector_init_params(seed=seed, last_scale=0.1), s_out=0.05)
+    return net
