@@ -1,0 +1,112 @@
+// The C++ drop-in used the way the reference's own tests use gridcalc:
+// the same headers, names and calls, restating known answers of
+// test/fvm_cell_laplacian_test.cpp, test/integrate_test.cpp,
+// test/laplacian_test.cpp, test/diffusion_test.cpp,
+// test/stencil_axis_extent_test.cpp and test/cahn_hilliard_test.cpp.
+// Prints "PASS <name>" per check and exits non-zero on the first failure.
+#include <gridcalc/core/Field.hpp>
+#include <gridcalc/core/Grid.hpp>
+#include <gridcalc/diff/Gradient.hpp>
+#include <gridcalc/diff/Laplacian.hpp>
+#include <gridcalc/func/Functional.hpp>
+#include <gridcalc/func/Integrate.hpp>
+#include <gridcalc/fvm/CellLaplacian.hpp>
+#include <gridcalc/solve/Diffusion.hpp>
+#include <gridcalc/solve/Integrator.hpp>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+
+using gridcalc::core::Field;
+using gridcalc::core::Grid;
+using gridcalc::core::Vec3d;
+
+static void require(bool ok, const char* name) {
+  if (!ok) {
+    std::printf("FAIL %s\n", name);
+    std::exit(1);
+  }
+  std::printf("PASS %s\n", name);
+}
+
+int main() {
+  const double kPi = 3.14159265358979323846;
+  {  // harmonic-mean face coefficient, +-1.6
+    Grid g(4, 1, 1, Vec3d(1.0, 1.0, 1.0));
+    Field<double> psi(g, 0.0), D(g, 0.0);
+    psi(1, 0, 0) = 1.0;
+    psi(2, 0, 0) = 1.0;
+    D(0, 0, 0) = 1.0; D(1, 0, 0) = 4.0; D(2, 0, 0) = 4.0; D(3, 0, 0) = 1.0;
+    auto rhs = gridcalc::fvm::cellLaplacian(psi, D);
+    require(std::abs(rhs(0, 0, 0) - 1.6) < 1e-15 && std::abs(rhs(1, 0, 0) + 1.6) < 1e-15 &&
+                std::abs(rhs(2, 0, 0) + 1.6) < 1e-15 && std::abs(rhs(3, 0, 0) - 1.6) < 1e-15,
+            "fvm harmonic mean face coefficient");
+  }
+  {  // unit field integrates to the domain volume, both tags
+    Grid g(8, 16, 4, Vec3d(0.25, 0.125, 0.5));
+    Field<double> ones(g, 1.0);
+    const double vol = (8 * 0.25) * (16 * 0.125) * (4 * 0.5);
+    require(gridcalc::func::integrate(ones) == vol && gridcalc::func::integrate(ones, gridcalc::func::Kahan{}) == vol,
+            "integrate unit field");
+  }
+  {  // laplacian eigenfunction, relative max error < 1.5e-2 at N = 32
+    const int N = 32;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<double> f(g, [](double x, double y, double z) { return std::sin(x) * std::sin(y) * std::sin(z); });
+    auto lap = gridcalc::diff::laplacian<2>(f);
+    double err = 0, ref = 0;
+    for (size_t i = 0; i < f.size(); ++i) {
+      err = std::max(err, std::abs(lap.data()[i] + 3 * f.data()[i]));
+      ref = std::max(ref, std::abs(3 * f.data()[i]));
+    }
+    require(err / ref < 1.5e-2, "laplacian eigenfunction");
+    auto grad = gridcalc::diff::gradient<4>(f);
+    require(std::abs(grad(3, 5, 7)(0) - std::cos(3 * h) * std::sin(5 * h) * std::sin(7 * h)) < 1e-4, "gradient order 4");
+  }
+  {  // axis-extent error names the axis
+    Grid g(8, 3, 8, Vec3d(1, 1, 1));
+    Field<double> f(g, 0.0);
+    bool threw = false;
+    try {
+      gridcalc::diff::laplacian<4>(f);
+    } catch (const std::invalid_argument& e) {
+      threw = std::string(e.what()).find("axis y") != std::string::npos;
+    }
+    require(threw, "axis extent message");
+  }
+  {  // diffusion decays as exp(-3 D t); CFL violation throws with solve::diffuse
+    const int N = 32;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<double> f(g, [](double x, double y, double z) { return std::sin(x) * std::sin(y) * std::sin(z); });
+    const double m0 = f(8, 8, 8);
+    gridcalc::solve::diffuse(f, 0.5, 0.01, 100, gridcalc::solve::RK4{});
+    require(std::abs(f(8, 8, 8) / m0 - std::exp(-1.5)) < 5e-3, "diffusion decay");
+    bool threw = false;
+    try {
+      gridcalc::solve::diffuse(f, 1.0, 1.0, 1, gridcalc::solve::RK4{});
+    } catch (const std::invalid_argument& e) {
+      threw = std::string(e.what()).find("solve::diffuse") != std::string::npos;
+    }
+    require(threw, "CFL message");
+  }
+  {  // Cahn-Hilliard: mass conserved, free energy decreases (cahn_hilliard_test.cpp)
+    Grid g(64, 64, 1, Vec3d(1, 1, 1));
+    std::srand(42);
+    Field<double> psi(g, [](double, double, double) { return 0.1 * (2.0 * std::rand() / RAND_MAX - 1.0); });
+    double mean = gridcalc::func::integrate(psi) / g.getSize();
+    for (auto& v : psi) v -= mean;
+    const double F0 = gridcalc::func::evaluate(psi, gridcalc::func::FreeEnergy{1.0});
+    const double m0 = gridcalc::func::integrate(psi, gridcalc::func::Kahan{});
+    gridcalc::solve::integrate(psi, gridcalc::solve::CahnHilliardRhs{1.0, 1.0, 2}, 0.01, 3000, gridcalc::solve::RK4{});
+    const double F1 = gridcalc::func::evaluate(psi, gridcalc::func::FreeEnergy{1.0});
+    const double m1 = gridcalc::func::integrate(psi, gridcalc::func::Kahan{});
+    require(F1 < F0 && std::abs(m1 - m0) < 1e-10, "cahn-hilliard energy decay and mass");
+  }
+  std::printf("version %s\n", gridcalc::version());
+  return 0;
+}
