@@ -265,14 +265,17 @@ __global__ void sum_partials(const float* __restrict__ partial, int n_parts, flo
 }
 
 // ---- input, output, loss --------------------------------------------------
+// Channel 0 = c, channel 1 = feature_scale * f (the right-hand side when
+// features are on, else 0), channels 2..31 = 0.
 template <class T>
-__global__ void pack_input(const T* __restrict__ c, size_t n, __nv_bfloat16* __restrict__ x0) {
+__global__ void pack_input(const T* __restrict__ c, const T* __restrict__ f, float feature_scale, size_t n,
+                           __nv_bfloat16* __restrict__ x0) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     uint4* dst = reinterpret_cast<uint4*>(x0 + p * kC);
     uint4 z = make_uint4(0, 0, 0, 0);
-    __nv_bfloat16 v = __float2bfloat16(static_cast<float>(c[p]));
-    z.x = static_cast<uint32_t>(*reinterpret_cast<uint16_t*>(&v));
+    const float fv = f ? feature_scale * static_cast<float>(f[p]) : 0.f;
+    z.x = pack_bf16(static_cast<float>(c[p]), fv);
     dst[0] = z;
     dst[1] = make_uint4(0, 0, 0, 0);
     dst[2] = make_uint4(0, 0, 0, 0);
@@ -303,9 +306,21 @@ __global__ void project_delta(const float* __restrict__ z, const float* __restri
     delta[p] = s_out * (z[p] - mean[p / hw]);
 }
 
-// r = c + delta - target, stored; per-CTA partial sums of r^2 (fixed grid).
+// (target - c)^2, for the per-sample step size of the normalised loss.
+__global__ void step_sq(const float* __restrict__ c, const float* __restrict__ target, size_t n,
+                        float* __restrict__ out) {
+  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float d = target[p] - c[p];
+    out[p] = d * d;
+  }
+}
+
+// r = c + delta - target, stored; per-CTA partial sums of r^2 / den[sample]
+// (den = 1 for the plain loss; fixed grid).
 __global__ void residual_kernel(const float* __restrict__ c, const float* __restrict__ delta,
-                                const float* __restrict__ target, size_t n, float* __restrict__ r,
+                                const float* __restrict__ target, size_t n, int hw,
+                                const float* __restrict__ den, float* __restrict__ r,
                                 double* __restrict__ part) {
   __shared__ double sh[256];
   double acc = 0.0;
@@ -313,7 +328,8 @@ __global__ void residual_kernel(const float* __restrict__ c, const float* __rest
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const float v = c[p] + delta[p] - target[p];
     r[p] = v;
-    acc += static_cast<double>(v) * v;
+    const double w = den ? 1.0 / static_cast<double>(den[p / hw]) : 1.0;
+    acc += static_cast<double>(v) * v * w;
   }
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -324,13 +340,15 @@ __global__ void residual_kernel(const float* __restrict__ c, const float* __rest
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-// dz6 (channel 0) = s_out * 2/N (r - mean_sample(r)); other channels 0.
+// dz6 (channel 0) = s_out * 2/N (r - mean_sample(r)) / den[sample];
+// other channels 0.
 __global__ void last_layer_grad(const float* __restrict__ r, const float* __restrict__ rmean, int hw, size_t n,
-                                float scale, __nv_bfloat16* __restrict__ dz) {
+                                float scale, const float* __restrict__ den, __nv_bfloat16* __restrict__ dz) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     uint4* dst = reinterpret_cast<uint4*>(dz + p * kC);
-    __nv_bfloat16 v = __float2bfloat16(scale * (r[p] - rmean[p / hw]));
+    const float w = den ? 1.0f / den[p / hw] : 1.0f;
+    __nv_bfloat16 v = __float2bfloat16(scale * w * (r[p] - rmean[p / hw]));
     uint4 z = make_uint4(static_cast<uint32_t>(*reinterpret_cast<uint16_t*>(&v)), 0, 0, 0);
     dst[0] = z;
     dst[1] = make_uint4(0, 0, 0, 0);
@@ -436,6 +454,14 @@ struct gc_corrector {
   float* wpart = nullptr;           // per-CTA weight-gradient partials
   int wparts = 0;
   double* adv = nullptr;            // advance scratch: cand, f0, f1 (H x W each)
+  // Right-hand-side input feature: channel 1 = feature_dt * f(c), f the
+  // Cahn-Hilliard RHS with chp (off until gc_corrector_set_physics).
+  bool feature = false;
+  gc_ch_params chp{1.0, 1.0, 2};
+  double feature_dt = 0.0;
+  double* fbuf = nullptr;           // f(c), max_batch x H x W (double-sized)
+  float* den = nullptr;             // per-sample step size (normalised loss)
+  bool normalized = false;
   bool weights_dirty = true;
 };
 
@@ -460,7 +486,18 @@ gc_status corr_forward(gc_corrector* c, int batch, const T* in) {
   const int H = c->H, W = c->W;
   const size_t n = static_cast<size_t>(batch) * H * W;
   cudaStream_t st = c->ctx->stream;
-  pack_input<T><<<c->ctx->num_sms * 8, 256, 0, st>>>(in, n, c->x[0]);
+  const T* feat = nullptr;
+  if (c->feature) {
+    const gc_grid g{W, H, 1, 1.0, 1.0, 1.0};
+    T* fb = reinterpret_cast<T*>(c->fbuf);
+    for (int b = 0; b < batch; ++b) {
+      gc_status fs = gc_ch_rhs(c->ctx, &g, sizeof(T) == 8 ? GC_F64 : GC_F32, &c->chp, in + static_cast<size_t>(b) * H * W,
+                               fb + static_cast<size_t>(b) * H * W);
+      if (fs != GC_OK) return fs;
+    }
+    feat = fb;
+  }
+  pack_input<T><<<c->ctx->num_sms * 8, 256, 0, st>>>(in, feat, static_cast<float>(c->feature_dt), n, c->x[0]);
   GC_CHECK_LAUNCH("pack_input");
   const int tiles_x = div_up(W, kTC), tiles_y = div_up(H, kTR);
   const int tpi = tiles_x * tiles_y;
@@ -489,13 +526,19 @@ gc_status corr_backward(gc_corrector* c, int batch, const float* cin, const floa
   const int H = c->H, W = c->W, hw = H * W;
   const size_t n = static_cast<size_t>(batch) * hw;
   cudaStream_t st = c->ctx->stream;
-  residual_kernel<<<kRedBlocks, 256, 0, st>>>(cin, c->delta, target, n, c->resid, c->part);
+  const float* den = nullptr;
+  if (c->normalized) {
+    step_sq<<<c->ctx->num_sms * 8, 256, 0, st>>>(cin, target, n, c->resid);
+    sample_mean<<<batch, 256, 0, st>>>(c->resid, hw, c->den);
+    den = c->den;
+  }
+  residual_kernel<<<kRedBlocks, 256, 0, st>>>(cin, c->delta, target, n, hw, den, c->resid, c->part);
   GC_CHECK_LAUNCH("residual_kernel");
   sample_mean<<<batch, 256, 0, st>>>(c->resid, hw, c->mean2);
   const float scale = c->s_out * 2.0f / static_cast<float>(n);
   __nv_bfloat16* dz = c->dz_a;
   __nv_bfloat16* dzn = c->dz_b;
-  last_layer_grad<<<c->ctx->num_sms * 8, 256, 0, st>>>(c->resid, c->mean2, hw, n, scale, dz);
+  last_layer_grad<<<c->ctx->num_sms * 8, 256, 0, st>>>(c->resid, c->mean2, hw, n, scale, den, dz);
   GC_CHECK_LAUNCH("last_layer_grad");
   const int tiles_x = div_up(W, kTC), tiles_y = div_up(H, kTR);
   const int tpi = tiles_x * tiles_y;
@@ -564,6 +607,8 @@ GC_API gc_status gc_corrector_create(gc_context* ctx, int32_t height, int32_t wi
   alloc(reinterpret_cast<void**>(&c->mean), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->mean2), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->cbuf), sizeof(float) * n);
+  alloc(reinterpret_cast<void**>(&c->fbuf), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&c->den), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->tbuf), sizeof(float) * n);
   alloc(reinterpret_cast<void**>(&c->part), sizeof(double) * 2 * kRedBlocks);
   c->wparts = ctx->num_sms * 4;
@@ -584,7 +629,8 @@ GC_API gc_status gc_corrector_destroy(gc_corrector* c) {
   cudaSetDevice(c->ctx->device);
   cudaStreamSynchronize(c->ctx->stream);
   void* ptrs[] = {c->params, c->grad, c->adam_m, c->adam_v, c->w_fwd, c->w_bwd, c->dz_a, c->dz_b, c->zlast,
-                  c->delta, c->resid, c->mean, c->mean2, c->cbuf, c->tbuf, c->part, c->wpart, c->adv};
+                  c->delta, c->resid, c->mean, c->mean2, c->cbuf, c->tbuf, c->part, c->wpart, c->adv,
+                  c->fbuf, c->den};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->x)
@@ -596,6 +642,26 @@ GC_API gc_status gc_corrector_destroy(gc_corrector* c) {
 }
 
 GC_API int32_t gc_corrector_num_params(void) { return kParams; }
+
+GC_API gc_status gc_corrector_set_physics(gc_corrector* c, const gc_ch_params* p, double feature_dt) {
+  if (!c) return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_physics: null corrector");
+  if (!p) {
+    c->feature = false;
+    return GC_OK;
+  }
+  if (p->order != 2 && p->order != 4 && p->order != 6)
+    return fail(GC_ERR_UNSUPPORTED, "gc_corrector_set_physics: order must be 2, 4 or 6");
+  c->feature = true;
+  c->chp = *p;
+  c->feature_dt = feature_dt;
+  return GC_OK;
+}
+
+GC_API gc_status gc_corrector_set_loss(gc_corrector* c, int32_t normalized) {
+  if (!c) return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_loss: null corrector");
+  c->normalized = normalized != 0;
+  return GC_OK;
+}
 
 GC_API gc_status gc_corrector_set_params(gc_corrector* c, const float* host, int32_t n, float s_out) {
   if (!c || !host || n != kParams) return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_params: need all parameters");

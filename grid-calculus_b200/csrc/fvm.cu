@@ -46,9 +46,18 @@ struct FvmTile;
 template <> struct FvmTile<false> { static constexpr int TX = 64, TY = 16, TZ = 1; };
 template <> struct FvmTile<true> { static constexpr int TX = 32, TY = 16, TZ = 8; };
 
+// Face coefficient 2ab / (a + b) (reference fvm/CellLaplacian.hpp:48-50).  Double
+// keeps the reference's rounding; float, the precision variant, uses the fast
+// division intrinsic (2 ulp for the positive, normal-range coefficients the
+// positivity check admits): six IEEE divisions per cell would otherwise
+// dominate the kernel's issue slots.
 template <class T>
 __device__ __forceinline__ T hmean(T a, T b) {
   return Ar<T>::div(Ar<T>::mul(Ar<T>::mul(T(2), a), b), Ar<T>::add(a, b));
+}
+template <>
+__device__ __forceinline__ float hmean<float>(float a, float b) {
+  return __fdividef(2.0f * a * b, a + b);
 }
 
 template <class T, int KIND, bool Z3, int MODE>
@@ -137,8 +146,165 @@ gc_status launch_fvm(gc_context* ctx, const FvmParams<T>& p) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// 3-D z-march stage kernel.  A 32 x 8 CTA owns a column of cells and
+// marches up a chunk of z planes.  Each thread keeps its own column's psi,
+// k_prev, y = psi + a k_prev and D at planes z-1, z, z+1 in registers; the
+// current plane of y and D goes to shared memory with a one-cell x/y halo
+// (strips loaded by a few threads).  Every global load of plane z+1 is
+// issued while plane z is computed.  Same arithmetic as fvm_stage_kernel.
+constexpr int FZ_X = 32, FZ_Y = 8;
+
+template <class T, int KIND, int MODE>
+__global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_kernel(const FvmParams<T> p, int zc) {
+  constexpr bool FVM = KIND == KIND_FVM;
+  __shared__ T sy[FZ_Y + 2][FZ_X + 2];
+  __shared__ T sd[FVM ? FZ_Y + 2 : 1][FVM ? FZ_X + 2 : 1];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * FZ_X, y0 = blockIdx.y * FZ_Y;
+  const int z0 = blockIdx.z * zc;
+  const int z1 = min(z0 + zc, nz);
+  const size_t plane = static_cast<size_t>(nx) * ny;
+  const int gx = wrap(x0 + tx, nx), gy = wrap(y0 + ty, ny);
+  const size_t col = static_cast<size_t>(gy) * nx + gx;
+  const bool active = x0 + tx < nx && y0 + ty < ny;
+  const bool hx = tx < 2;
+  const size_t hx_off = static_cast<size_t>(gy) * nx + wrap(tx == 0 ? x0 - 1 : x0 + FZ_X, nx);
+  const int hx_slot = tx == 0 ? 0 : FZ_X + 1;
+  const bool hy = ty < 2;
+  const size_t hy_off = static_cast<size_t>(wrap(ty == 0 ? y0 - 1 : y0 + FZ_Y, ny)) * nx + gx;
+  const int hy_slot = ty == 0 ? 0 : FZ_Y + 1;
+  const bool has_kin = p.kin != nullptr;
+
+  auto yval = [&](size_t gi) -> T {
+    T v = __ldg(p.psi + gi);
+    if (has_kin) v = Ar<T>::add(v, Ar<T>::mul(p.a, __ldg(p.kin + gi)));
+    return v;
+  };
+  auto dval = [&](size_t gi) -> T { return FVM ? __ldg(p.D + gi) : T(0); };
+
+  // Queues: index 0 = plane z-1, 1 = z, 2 = z+1.
+  T qy[3], qd[3], qp[3], qk[3];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const size_t gi = static_cast<size_t>(wrap(z0 - 1 + k, nz)) * plane + col;
+    qp[k + 1] = __ldg(p.psi + gi);
+    qk[k + 1] = has_kin ? __ldg(p.kin + gi) : T(0);
+    qy[k + 1] = has_kin ? Ar<T>::add(qp[k + 1], Ar<T>::mul(p.a, qk[k + 1])) : qp[k + 1];
+    qd[k + 1] = dval(gi);
+  }
+  // Prefetch registers for plane z0: queue entry (z0 + 1), halos of z0, k1/k2 of z0.
+  auto qaddr = [&](int z) { return static_cast<size_t>(wrap(z, nz)) * plane + col; };
+  T n_p = __ldg(p.psi + qaddr(z0 + 1));
+  T n_k = has_kin ? __ldg(p.kin + qaddr(z0 + 1)) : T(0);
+  T n_d = dval(qaddr(z0 + 1));
+  T n_hxy = hx ? yval(static_cast<size_t>(z0) * plane + hx_off) : T(0);
+  T n_hxd = hx ? dval(static_cast<size_t>(z0) * plane + hx_off) : T(0);
+  T n_hyy = hy ? yval(static_cast<size_t>(z0) * plane + hy_off) : T(0);
+  T n_hyd = hy ? dval(static_cast<size_t>(z0) * plane + hy_off) : T(0);
+  T n_k1 = T(0), n_k2 = T(0);
+  if (MODE == MODE_RK4_FINAL && active) {
+    n_k1 = __ldg(p.k1 + static_cast<size_t>(z0) * plane + col);
+    n_k2 = __ldg(p.k2 + static_cast<size_t>(z0) * plane + col);
+  }
+
+  for (int z = z0; z < z1; ++z) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      qy[k] = qy[k + 1];
+      qd[k] = qd[k + 1];
+      qp[k] = qp[k + 1];
+      qk[k] = qk[k + 1];
+    }
+    qp[2] = n_p;
+    qk[2] = n_k;
+    qy[2] = has_kin ? Ar<T>::add(n_p, Ar<T>::mul(p.a, n_k)) : n_p;
+    qd[2] = n_d;
+    const T hxy = n_hxy, hxd = n_hxd, hyy = n_hyy, hyd = n_hyd, k1c = n_k1, k2c = n_k2;
+    if (z + 1 < z1) {
+      const size_t zo = static_cast<size_t>(z + 1) * plane;
+      n_p = __ldg(p.psi + qaddr(z + 2));
+      if (has_kin) n_k = __ldg(p.kin + qaddr(z + 2));
+      n_d = dval(qaddr(z + 2));
+      if (hx) {
+        n_hxy = yval(zo + hx_off);
+        n_hxd = dval(zo + hx_off);
+      }
+      if (hy) {
+        n_hyy = yval(zo + hy_off);
+        n_hyd = dval(zo + hy_off);
+      }
+      if (MODE == MODE_RK4_FINAL && active) {
+        n_k1 = __ldg(p.k1 + zo + col);
+        n_k2 = __ldg(p.k2 + zo + col);
+      }
+    }
+    sy[ty + 1][tx + 1] = qy[1];
+    if (FVM) sd[ty + 1][tx + 1] = qd[1];
+    if (hx) {
+      sy[ty + 1][hx_slot] = hxy;
+      if (FVM) sd[ty + 1][hx_slot] = hxd;
+    }
+    if (hy) {
+      sy[hy_slot][tx + 1] = hyy;
+      if (FVM) sd[hy_slot][tx + 1] = hyd;
+    }
+    __syncthreads();
+    if (active) {
+      const T pc = qy[1];
+      T rhs;
+      if constexpr (FVM) {
+        const T dc = qd[1];
+        const T dxp = hmean(dc, sd[ty + 1][tx + 2]), dxm = hmean(sd[ty + 1][tx], dc);
+        const T dyp = hmean(dc, sd[ty + 2][tx + 1]), dym = hmean(sd[ty][tx + 1], dc);
+        const T dzp = hmean(dc, qd[2]), dzm = hmean(qd[0], dc);
+        const T rx = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dxp, Ar<T>::sub(sy[ty + 1][tx + 2], pc)),
+                                           Ar<T>::mul(dxm, Ar<T>::sub(pc, sy[ty + 1][tx]))), p.ihx2);
+        const T ry = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dyp, Ar<T>::sub(sy[ty + 2][tx + 1], pc)),
+                                           Ar<T>::mul(dym, Ar<T>::sub(pc, sy[ty][tx + 1]))), p.ihy2);
+        const T rz = Ar<T>::mul(Ar<T>::sub(Ar<T>::mul(dzp, Ar<T>::sub(qy[2], pc)),
+                                           Ar<T>::mul(dzm, Ar<T>::sub(pc, qy[0]))), p.ihz2);
+        rhs = Ar<T>::add(Ar<T>::add(rx, ry), rz);
+      } else {
+        const T ax = tap_sum<T, 2, 2>([&](int o) { return sy[ty + 1][tx + 1 + o]; });
+        const T ay = tap_sum<T, 2, 2>([&](int o) { return sy[ty + 1 + o][tx + 1]; });
+        const T az = tap_sum<T, 2, 2>([&](int o) { return qy[1 + o]; });
+        rhs = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+      }
+      const size_t gi = static_cast<size_t>(z) * plane + static_cast<size_t>(y0 + ty) * nx + (x0 + tx);
+      if constexpr (MODE == MODE_RHS) {
+        p.out[gi] = rhs;
+      } else if constexpr (MODE == MODE_RK4_FINAL) {
+        const T s14 = Ar<T>::add(k1c, rhs);
+        const T s23 = Ar<T>::add(k2c, qk[1]);
+        p.out[gi] = Ar<T>::add(qp[1], Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+      } else {
+        p.out[gi] = Ar<T>::add(pc, Ar<T>::mul(p.c6, rhs));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class T, int KIND, int MODE>
+gc_status launch_fvm_zmarch(gc_context* ctx, const FvmParams<T>& p) {
+  const int tiles_x = div_up(p.nx, FZ_X), tiles_y = div_up(p.ny, FZ_Y);
+  const long long tiles = static_cast<long long>(tiles_x) * tiles_y;
+  const long long want = 16LL * ctx->num_sms;
+  int chunks = static_cast<int>(std::min<long long>((want + tiles - 1) / tiles, std::max(1, p.nz / 16)));
+  chunks = std::max(chunks, 1);
+  const int zc = div_up(p.nz, chunks);
+  chunks = div_up(p.nz, zc);
+  dim3 grid(tiles_x, tiles_y, chunks), block(FZ_X, FZ_Y);
+  fvm_zmarch_kernel<T, KIND, MODE><<<grid, block, 0, ctx->stream>>>(p, zc);
+  GC_CHECK_LAUNCH("fvm_zmarch_kernel");
+  return GC_OK;
+}
+
 template <class T, int KIND, int MODE>
 gc_status launch_kind(gc_context* ctx, const FvmParams<T>& p) {
+  if (p.nz > 2) return launch_fvm_zmarch<T, KIND, MODE>(ctx, p);
   return p.nz > 1 ? launch_fvm<T, KIND, true, MODE>(ctx, p) : launch_fvm<T, KIND, false, MODE>(ctx, p);
 }
 

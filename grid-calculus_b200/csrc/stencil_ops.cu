@@ -66,17 +66,22 @@ __global__ void __launch_bounds__(NT) stencil_kernel(const OpParams<T> p) {
   const int z1 = min(z0 + p.zc, p.nz);
   const int nx = p.nx, ny = p.ny, nz = p.nz;
 
+  // Plane loads map threads onto rows and columns directly (no division):
+  // column wraps are formed once per thread, row wraps once per row.
+  const int gxa = wrap(x0 - R + tx, nx);
+  const bool has_b = tx < PW - BX;
+  const int gxb = wrap(x0 - R + BX + tx, nx);
+  (void)tid;
   auto load_plane = [&](int z, int slot) {
     const int zw = wrap(z, nz);
     const size_t zoff = static_cast<size_t>(zw) * nx * ny;
-    for (int e = tid; e < PS; e += NT) {
-      const int sy = e / PW;
-      const int sx = e - sy * PW;
-      const int gx = wrap(x0 - R + sx, nx);
-      const int gy = wrap(y0 - R + sy, ny);
-      const size_t gi = zoff + static_cast<size_t>(gy) * nx + gx;
+    for (int r = ty; r < PH; r += BY) {
+      const size_t rowo = zoff + static_cast<size_t>(wrap(y0 - R + r, ny)) * nx;
 #pragma unroll
-      for (int f = 0; f < NF; ++f) ring[(f * NP + slot) * PS + e] = __ldg(p.in[f] + gi);
+      for (int f = 0; f < NF; ++f) {
+        ring[(f * NP + slot) * PS + r * PW + tx] = __ldg(p.in[f] + rowo + gxa);
+        if (has_b) ring[(f * NP + slot) * PS + r * PW + BX + tx] = __ldg(p.in[f] + rowo + gxb);
+      }
     }
   };
 
@@ -158,6 +163,129 @@ __global__ void __launch_bounds__(NT) stencil_kernel(const OpParams<T> p) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// z-march kernel for the axis-separable operators (laplacian, gradient,
+// divergence) on 3-D grids.  A 32 x 8 CTA owns a column of cells and
+// marches up a chunk of z planes; each thread keeps its own column's z taps
+// in a register queue, so only the current plane goes through shared memory
+// (its interior taken from the queue, its x/y halo strips loaded by a few
+// threads).  The next plane's value and halo are loaded one iteration
+// ahead into registers, so global latency overlaps the current plane.
+// Divergence stages the x component with an x halo and the y component
+// with a y halo; the z component only needs the queue.
+constexpr int ZM_X = 32, ZM_Y = 8;
+
+template <class T, int OP, int ORDER>
+__global__ void __launch_bounds__(ZM_X * ZM_Y) zmarch_kernel(const OpParams<T> p) {
+  constexpr int R = OpShape<OP, ORDER>::R;
+  constexpr int NQ = 2 * R + 1;
+  constexpr int PW = ZM_X + 2 * R, PH = ZM_Y + 2 * R;
+  constexpr int K = OP == OP_LAP ? 2 : 1;
+  // plane of the field (LAP, GRAD) or of the x component (DIV), and for DIV
+  // the y component's plane.
+  __shared__ T sp[PH][PW];
+  __shared__ T sy[OP == OP_DIV ? PH : 1][OP == OP_DIV ? ZM_X : 1];
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * ZM_X, y0 = blockIdx.y * ZM_Y;
+  const int z0 = blockIdx.z * p.zc;
+  const int z1 = min(z0 + p.zc, nz);
+  const size_t plane = static_cast<size_t>(nx) * ny;
+  const int gx = wrap(x0 + tx, nx), gy = wrap(y0 + ty, ny);
+  const size_t col = static_cast<size_t>(gy) * nx + gx;
+  const bool active = x0 + tx < nx && y0 + ty < ny;
+  // Halo duties: x halo (threads tx < 2R: left for tx < R, right otherwise)
+  // for row ty; y halo (threads ty < 2R) for column tx.
+  const bool hx = tx < 2 * R;
+  const int hx_col = tx < R ? x0 - R + tx : x0 + ZM_X + (tx - R);
+  const size_t hx_off = static_cast<size_t>(gy) * nx + wrap(hx_col, nx);
+  const int hx_slot = tx < R ? tx : ZM_X + R + (tx - R);
+  const bool hy = ty < 2 * R;
+  const int hy_row = ty < R ? y0 - R + ty : y0 + ZM_Y + (ty - R);
+  const size_t hy_off = static_cast<size_t>(wrap(hy_row, ny)) * nx + gx;
+  const int hy_slot = ty < R ? ty : ZM_Y + R + (ty - R);
+
+  const T* fx = p.in[0];                         // LAP/GRAD field, DIV x component
+  const T* fy = p.in[1];                         // DIV y component
+  const T* fz = OP == OP_DIV ? p.in[2] : p.in[0];  // field whose z taps are queued
+
+  T q[NQ];
+#pragma unroll
+  for (int k = 0; k < NQ - 1; ++k) q[k + 1] = __ldg(fz + static_cast<size_t>(wrap(z0 - R + k, nz)) * plane + col);
+  // Prefetch of plane z0: its queue value (z0 + R), centre and halos.
+  T n_q = __ldg(fz + static_cast<size_t>(wrap(z0 + R, nz)) * plane + col);
+  size_t zoff = static_cast<size_t>(z0) * plane;
+  T n_c = (OP == OP_DIV) ? __ldg(fx + zoff + col) : T(0);
+  T n_cy = (OP == OP_DIV) ? __ldg(fy + zoff + col) : T(0);
+  T n_hx = hx ? __ldg(fx + zoff + hx_off) : T(0);
+  T n_hy = hy ? __ldg((OP == OP_DIV ? fy : fx) + zoff + hy_off) : T(0);
+
+  for (int z = z0; z < z1; ++z) {
+#pragma unroll
+    for (int k = 0; k + 1 < NQ; ++k) q[k] = q[k + 1];
+    q[NQ - 1] = n_q;
+    const T c_x = OP == OP_DIV ? n_c : q[R];
+    const T c_y = n_cy;
+    const T h_x = n_hx, h_y = n_hy;
+    if (z + 1 < z1) {  // prefetch plane z + 1
+      const size_t zo = static_cast<size_t>(z + 1) * plane;
+      n_q = __ldg(fz + static_cast<size_t>(wrap(z + 1 + R, nz)) * plane + col);
+      if (OP == OP_DIV) {
+        n_c = __ldg(fx + zo + col);
+        n_cy = __ldg(fy + zo + col);
+      }
+      if (hx) n_hx = __ldg(fx + zo + hx_off);
+      if (hy) n_hy = __ldg((OP == OP_DIV ? fy : fx) + zo + hy_off);
+    }
+    sp[ty + R][tx + R] = c_x;
+    if (hx) sp[ty + R][hx_slot] = h_x;
+    if (OP == OP_DIV) {
+      sy[ty + R][tx] = c_y;
+      if (hy) sy[hy_slot][tx] = h_y;
+    } else {
+      if (hy) sp[hy_slot][tx + R] = h_y;
+    }
+    __syncthreads();
+    if (active) {
+      const size_t c = static_cast<size_t>(z) * plane + static_cast<size_t>(y0 + ty) * nx + (x0 + tx);
+      const T ax = tap_sum<T, K, ORDER>([&](int o) { return sp[ty + R][tx + R + o]; });
+      const T az = tap_sum<T, K, ORDER>([&](int o) { return q[R + o]; });
+      if constexpr (OP == OP_DIV) {
+        const T ay = tap_sum<T, 1, ORDER>([&](int o) { return sy[ty + R + o][tx]; });
+        p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx), Ar<T>::mul(ay, p.ihy)), Ar<T>::mul(az, p.ihz));
+      } else {
+        const T ay = tap_sum<T, K, ORDER>([&](int o) { return sp[ty + R + o][tx + R]; });
+        if constexpr (OP == OP_LAP) {
+          p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)), Ar<T>::mul(az, p.ihz2));
+        } else {
+          p.out[c] = Ar<T>::mul(ax, p.ihx);
+          p.out[p.n + c] = Ar<T>::mul(ay, p.ihy);
+          p.out[2 * p.n + c] = Ar<T>::mul(az, p.ihz);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <class T, int OP, int ORDER>
+gc_status launch_zmarch(gc_context* ctx, const OpParams<T>& p0) {
+  OpParams<T> p = p0;
+  const int tiles_x = div_up(p.nx, ZM_X), tiles_y = div_up(p.ny, ZM_Y);
+  const long long tiles = static_cast<long long>(tiles_x) * tiles_y;
+  // Enough CTAs to fill the GPU several times, chunks of at least 16 planes.
+  const long long want = 16LL * ctx->num_sms;
+  int chunks = static_cast<int>(std::min<long long>((want + tiles - 1) / tiles, std::max(1, p.nz / 16)));
+  chunks = std::max(chunks, 1);
+  p.zc = div_up(p.nz, chunks);
+  chunks = div_up(p.nz, p.zc);
+  dim3 grid(tiles_x, tiles_y, chunks), block(ZM_X, ZM_Y);
+  zmarch_kernel<T, OP, ORDER><<<grid, block, 0, ctx->stream>>>(p);
+  GC_CHECK_LAUNCH("zmarch_kernel");
+  return GC_OK;
+}
+
 template <class T, int OP, int ORDER, bool Z3>
 gc_status launch_one(gc_context* ctx, const OpParams<T>& p0) {
   constexpr int R = OpShape<OP, ORDER>::R;
@@ -189,6 +317,18 @@ gc_status launch_one(gc_context* ctx, const OpParams<T>& p0) {
 template <class T, int OP>
 gc_status dispatch_order(gc_context* ctx, int order, const OpParams<T>& p) {
   const bool z3 = p.nz > 1;
+  if constexpr (OP != OP_BIH) {
+    // 3-D axis-separable operators: z-march with a register queue.  The
+    // queue and the halo strips need the z extent and the tile to exceed
+    // the radius (degenerate and tiny axes keep the plane-ring kernel).
+    if (z3 && p.nz > 2 * OpShape<OP, 6>::R) {
+      switch (order) {
+        case 2: return launch_zmarch<T, OP, 2>(ctx, p);
+        case 4: return launch_zmarch<T, OP, 4>(ctx, p);
+        case 6: return launch_zmarch<T, OP, 6>(ctx, p);
+      }
+    }
+  }
   switch (order) {
     case 2: return z3 ? launch_one<T, OP, 2, true>(ctx, p) : launch_one<T, OP, 2, false>(ctx, p);
     case 4: return z3 ? launch_one<T, OP, 4, true>(ctx, p) : launch_one<T, OP, 4, false>(ctx, p);

@@ -473,6 +473,8 @@ for _name, _args in {
     "gc_corrector_destroy": [_vp],
     "gc_corrector_set_params": [_vp, C.POINTER(C.c_float), C.c_int32, C.c_float],
     "gc_corrector_get_params": [_vp, C.POINTER(C.c_float), C.c_int32],
+    "gc_corrector_set_physics": [_vp, C.c_void_p, C.c_double],
+    "gc_corrector_set_loss": [_vp, C.c_int32],
     "gc_corrector_forward": [_vp, C.c_int32, _i32, _vp, _vp],
     "gc_corrector_gradient": [_vp, C.c_int32, _vp, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)],
     "gc_corrector_train_step": [_vp, C.c_int32, _vp, _vp, C.c_float, C.POINTER(C.c_double)],
@@ -488,18 +490,19 @@ lib.gc_corrector_num_params.argtypes = []
 CORRECTOR_LAYERS, CORRECTOR_CHANNELS = 6, 32
 
 
-def corrector_init_params(seed: int = 0, last_scale: float = 0.1):
+def corrector_init_params(seed: int = 0, last_scale: float = 0.1, inputs: int = 1):
     """He-normal initial parameters (FP32) for the corrector: per layer
-    W[9][32 in][32 out] then b[32]; the first layer sees one input channel."""
+    W[9][32 in][32 out] then b[32]; the first layer sees `inputs` input
+    channels (1: c; 2: c and the right-hand-side feature)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     n_c = CORRECTOR_CHANNELS
     out = []
     for layer in range(CORRECTOR_LAYERS):
-        fan_in = 9 * (1 if layer == 0 else n_c)
+        fan_in = 9 * (inputs if layer == 0 else n_c)
         w = rng.standard_normal((9, n_c, n_c)) * np.sqrt(2.0 / fan_in)
         if layer == 0:
-            w[:, 1:, :] = 0.0
+            w[:, inputs:, :] = 0.0
         if layer == CORRECTOR_LAYERS - 1:
             w *= last_scale
             w[:, :, 1:] = 0.0
@@ -533,6 +536,16 @@ class Corrector:
         p = np.empty(self.n_params, dtype=np.float32)
         _check(lib.gc_corrector_get_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
         return p
+
+    def set_physics(self, rhs: "CahnHilliardRhs | None", feature_dt: float = 0.16) -> None:
+        """Feeds feature_dt * f(c) (f the Cahn-Hilliard RHS) as the second
+        input channel; None turns the feature off."""
+        _check(lib.gc_corrector_set_physics(self.handle, C.byref(rhs.c()) if rhs is not None else None,
+                                            feature_dt))
+
+    def set_loss(self, normalized: bool) -> None:
+        """normalized: weight each training sample by 1 / mean((target - c)^2)."""
+        _check(lib.gc_corrector_set_loss(self.handle, 1 if normalized else 0))
 
     def forward(self, c):
         """Zero-mean correction for a (B, H, W) float32/float64 CUDA tensor."""

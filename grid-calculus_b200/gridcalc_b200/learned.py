@@ -16,7 +16,7 @@ import time
 
 import numpy as np
 
-from . import CahnHilliardRhs, Corrector, Grid, RK4, ch_integrate, corrector_init_params, evaluate
+from . import CahnHilliardRhs, Corrector, Grid, RK4, ch_integrate, ch_rhs, corrector_init_params, evaluate
 
 DT_FINE = 0.01
 FINE_PER_COARSE = 16
@@ -65,6 +65,40 @@ def train(net: Corrector, seeds, size: int = 512, fine_steps: int = 5000, batch:
             "seconds_data": t_data, "seconds_train": t_train}
 
 
+def trapezoid_residual(c0, c1, g: Grid, rhs: CahnHilliardRhs, dt: float) -> float:
+    """|(c1 - c0)/dt - (f(c0) + f(c1))/2| / |(f(c0) + f(c1))/2| with f the
+    Cahn-Hilliard RHS: the acceptance test of gc_corrector_advance."""
+    import torch
+    fm = 0.5 * (ch_rhs(c0, g, rhs) + ch_rhs(c1, g, rhs))
+    return float(torch.linalg.norm((c1 - c0) / dt - fm) / torch.linalg.norm(fm))
+
+
+def residual_profile(net: Corrector, seeds, size: int = 512, times=(2.0, 10.0, 50.0, 100.0, 200.0)) -> dict:
+    """Residual of the true coarse pair (c(t), c(t + 16 dt)) and of the
+    network's step from c(t), and their one-step errors, at several times."""
+    import torch
+    g = Grid(size, size, 1)
+    rhs = CahnHilliardRhs(1.0, 1.0, 2)
+    dtc = DT_FINE * FINE_PER_COARSE
+    rows = []
+    for s in seeds:
+        c = torch.from_numpy(initial_condition(s, size)).cuda()
+        t_now = 0.0
+        for t in times:
+            n = int(round((t - t_now) / DT_FINE))
+            ch_integrate(c, g, rhs, DT_FINE, n, RK4)
+            t_now = t
+            nxt = c.clone()
+            ch_integrate(nxt, g, rhs, DT_FINE, FINE_PER_COARSE, RK4)
+            cand = c + net.forward(c[None]).double()[0]
+            rows.append({"seed": s, "t": t,
+                         "residual_true": trapezoid_residual(c, nxt, g, rhs, dtc),
+                         "residual_net": trapezoid_residual(c, cand, g, rhs, dtc),
+                         "step_err_net": float(torch.linalg.norm(cand - nxt) / torch.linalg.norm(nxt - c)),
+                         "step_err_without_net": 1.0})
+    return {"rows": rows}
+
+
 def _free_energy_baseline(psi, g: Grid) -> float:
     return evaluate(psi, g, "ch_free_energy", kappa=1.0) + g.size * g.cell_volume / 4.0
 
@@ -108,7 +142,13 @@ def evaluate_heldout(net: Corrector, seeds, size: int = 512, t_end: float = 200.
             "speedup_vs_plain": t_fine / t_learned}
 
 
-def new_corrector(size: int, batch: int, seed: int = 0) -> Corrector:
+def new_corrector(size: int, batch: int, seed: int = 0, features: bool = True) -> Corrector:
+    """features: feed dt_coarse * f(c) as a second input channel and train
+    on the per-sample normalised loss (late-time steps are small, and without
+    it they barely count)."""
     net = Corrector(size, size, max_batch=batch)
-    net.set_params(corrector_init_params(seed=seed, last_scale=0.1), s_out=0.05)
+    net.set_params(corrector_init_params(seed=seed, last_scale=0.1, inputs=2 if features else 1), s_out=0.05)
+    if features:
+        net.set_physics(CahnHilliardRhs(1.0, 1.0, 2), DT_FINE * FINE_PER_COARSE)
+        net.set_loss(True)
     return net

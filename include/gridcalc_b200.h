@@ -240,7 +240,8 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
 /* ---- learned coarse-step corrector ---------------------------------------
  * No reference counterpart.  A 6-layer periodic 3x3 CNN (32 channels, GELU,
  * BF16 weights and activations, FP32 accumulation on the tensor cores)
- * maps a 2-D Cahn-Hilliard field c to a zero-mean correction delta so that
+ * maps a 2-D Cahn-Hilliard field c (and optionally its right-hand side, see
+ * gc_corrector_set_physics) to a zero-mean correction delta so that
  * c + delta approximates fine_per_coarse plain RK4 steps.  Parameters are
  * FP32 masters, per layer W[9 taps][32 in][32 out] then b[32], tap t at
  * offset (t / 3 - 1, t % 3 - 1) in (y, x); delta = s_out (z6 - mean z6)
@@ -265,6 +266,12 @@ GC_API gc_status gc_corrector_create(gc_context* ctx, int32_t height, int32_t wi
 GC_API gc_status gc_corrector_destroy(gc_corrector* c);
 GC_API int32_t gc_corrector_num_params(void);
 GC_API gc_status gc_corrector_set_params(gc_corrector* c, const float* host, int32_t n, float s_out);
+/* Second input channel feature_dt * f(c), f the Cahn-Hilliard RHS with p
+ * (computed by gc_ch_rhs); NULL p turns it off (channel 1 = 0). */
+GC_API gc_status gc_corrector_set_physics(gc_corrector* c, const gc_ch_params* p, double feature_dt);
+/* normalized != 0: the training loss weights each sample by 1 / mean((target
+ * - c)^2), so that small (late-time) steps count as much as large ones. */
+GC_API gc_status gc_corrector_set_loss(gc_corrector* c, int32_t normalized);
 GC_API gc_status gc_corrector_get_params(gc_corrector* c, float* host, int32_t n);
 /* delta for `batch` fields (batch x height x width, dtype F32 or F64) into
  * delta_out (device, float). */

@@ -69,6 +69,39 @@ def test_gradient_matches_cpu_network(gc):
     net.close()
 
 
+def test_rhs_feature_and_normalized_loss_match_cpu_network(gc):
+    """Second input channel feature_dt * f(c) (f from the library's CH RHS)
+    and the per-sample normalised loss, against the float64 network fed the
+    same feature."""
+    import torch
+    params = gc.corrector_init_params(seed=6, last_scale=1.0, inputs=2)
+    rng = np.random.default_rng(8)
+    h, w, fdt = 32, 40, 0.16
+    c = rng.uniform(-1, 1, (2, h, w)).astype(np.float32)
+    target = (c + np.array([0.05, 0.005])[:, None, None] * rng.standard_normal(c.shape)).astype(np.float32)
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
+    ct = torch.from_numpy(c).cuda()
+    feat = torch.stack([gc.ch_rhs(ct[b], gc.Grid(w, h, 1), rhs) for b in range(2)]).reshape(2, h, w).double().cpu().numpy() * fdt
+    net = gc.Corrector(h, w, max_batch=2)
+    net.set_params(params, s_out=0.05)
+    net.set_physics(rhs, fdt)
+    got = net.forward(ct).double().cpu().numpy()
+    want = corrector_ref.delta(params, c, 0.05, feat)
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < 3e-2
+    without = corrector_ref.delta(params, c, 0.05)
+    assert np.linalg.norm(without - want) > 0.1 * np.linalg.norm(want)   # the feature matters
+    net.set_loss(True)
+    g_gpu, loss_gpu = net.gradient(ct, torch.from_numpy(target).cuda())
+    loss_cpu, g_cpu = corrector_ref.loss_and_grad(params, c, target, 0.05, feat, normalized=True)
+    assert abs(loss_gpu - loss_cpu) / loss_cpu < 1e-2, (loss_gpu, loss_cpu)
+    cos = float(g_gpu @ g_cpu / (np.linalg.norm(g_gpu) * np.linalg.norm(g_cpu)))
+    assert np.linalg.norm(g_gpu - g_cpu) / np.linalg.norm(g_cpu) < 6e-2 and cos > 0.995, cos
+    net.set_physics(None)
+    got_off = net.forward(ct).double().cpu().numpy()
+    assert np.linalg.norm(got_off - without) / np.linalg.norm(without) < 3e-2
+    net.close()
+
+
 def test_training_gains_over_the_scheme_without_network(gc):
     """Trained on solver pairs at 64 x 64, the network's coarse step c + delta
     is closer to 16 fine RK4 steps than the coarse step without it (c), on
