@@ -111,6 +111,14 @@ __global__ void __launch_bounds__(kThreads) ch_stage_kernel(const StageParams<T>
       const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
       const T s23 = Ar<T>::add(__ldg(p.k2 + gi), __ldg(p.k3 + gi));
       p.out[gi] = Ar<T>::add(__ldg(p.psi + gi), Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+    } else if constexpr (MODE == MODE_RKC_FIRST || MODE == MODE_RKC) {
+      const int cy = ((ez + 2 * RZ) * YY + (ey + 2 * R)) * YX + (ex + 2 * R);
+      if constexpr (MODE == MODE_RKC_FIRST) {
+        p.out[gi] = rhs;
+        p.out2[gi] = Ar<T>::add(ys[cy], Ar<T>::mul(p.r[0], rhs));
+      } else {
+        p.out[gi] = rkc_combine(p, p.k1[gi], ys[cy], p.k2[gi], rhs, p.k3[gi]);
+      }
     } else {
       const int cy = ((ez + 2 * RZ) * YY + (ey + 2 * R)) * YX + (ex + 2 * R);
       p.out[gi] = Ar<T>::add(ys[cy], Ar<T>::mul(p.c6, rhs));
@@ -440,7 +448,7 @@ gc_status launch_pipe(gc_context* ctx, const StageParams<T>& p) {
 // cp.async-pipelined persistent loop otherwise.
 template <class T, int ORDER, int MODE>
 gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
-  if constexpr (sizeof(T) == 8) {
+  if constexpr (sizeof(T) == 8 && MODE != MODE_RKC_FIRST && MODE != MODE_RKC) {
     gc_status s;
     if constexpr (MODE == MODE_RHS) {
       s = p.kin ? launch_tma<T, ORDER, MODE, true>(ctx, p) : launch_tma<T, ORDER, MODE, false>(ctx, p);
@@ -538,6 +546,138 @@ gc_status integrate_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp,
   });
 }
 
+// ---------------------------------------------------------------------------
+// RKC2: the damped second-order Runge-Kutta-Chebyshev method (Sommeijer,
+// Shampine & Verwer, "RKC: an explicit solver for parabolic PDEs", 1998;
+// Hundsdorfer & Verwer, 2003, ch. V.1), damping eps = 2/13.  With
+// w0 = 1 + eps/s^2 and Chebyshev polynomials T_j (and derivatives) at w0:
+//   w1 = T_s'/T_s'', b_j = T_j''/T_j'^2 (j >= 2), b_0 = b_1 = b_2,
+//   a_j = 1 - b_j T_j;
+//   Y1 = Y0 + mu~1 dt F0,                                   mu~1 = b1 w1
+//   Yj = (1 - mu_j - nu_j) Y0 + mu_j Y_{j-1} + nu_j Y_{j-2}
+//        + mu~_j dt F(Y_{j-1}) + gamma~_j dt F0,
+//   mu_j = 2 b_j w0 / b_{j-1}, nu_j = -b_j / b_{j-2},
+//   mu~_j = 2 b_j w1 / b_{j-1}, gamma~_j = -a_{j-1} mu~_j;   y' = Y_s.
+// All coefficients come from three-term recurrences (no transcendental
+// calls).  Real stability interval [-beta, 0], beta = (w0 + 1) T_s''/T_s'
+// (about 0.65 s^2): s stages reach s^2 / 4 times the RK4 step limit.
+struct RkcCoeffs {
+  int s = 0;
+  double mt1 = 0.0;                       // mu~_1
+  double mu[65], nu[65], mt[65], gt[65];  // j = 2..s
+  double beta = 0.0;
+};
+
+RkcCoeffs rkc_coeffs(int s) {
+  RkcCoeffs c;
+  c.s = s;
+  const double eps = 2.0 / 13.0;
+  const double w0 = 1.0 + eps / (static_cast<double>(s) * s);
+  double T[65], d1[65], d2[65];
+  T[0] = 1.0; T[1] = w0;
+  d1[0] = 0.0; d1[1] = 1.0;
+  d2[0] = 0.0; d2[1] = 0.0;
+  for (int j = 2; j <= s; ++j) {
+    T[j] = 2.0 * w0 * T[j - 1] - T[j - 2];
+    d1[j] = 2.0 * T[j - 1] + 2.0 * w0 * d1[j - 1] - d1[j - 2];
+    d2[j] = 4.0 * d1[j - 1] + 2.0 * w0 * d2[j - 1] - d2[j - 2];
+  }
+  const double w1 = d1[s] / d2[s];
+  double b[65], a[65];
+  for (int j = 2; j <= s; ++j) b[j] = d2[j] / (d1[j] * d1[j]);
+  b[0] = b[1] = b[2];
+  for (int j = 0; j <= s; ++j) a[j] = 1.0 - b[j] * T[j];
+  c.mt1 = b[1] * w1;
+  for (int j = 2; j <= s; ++j) {
+    c.mu[j] = 2.0 * b[j] * w0 / b[j - 1];
+    c.nu[j] = -b[j] / b[j - 2];
+    c.mt[j] = 2.0 * b[j] * w1 / b[j - 1];
+    c.gt[j] = -a[j - 1] * c.mt[j];
+  }
+  c.beta = (w0 + 1.0) * d2[s] / d1[s];
+  return c;
+}
+
+// One RKC2 step of psi in place.  Scratch: F0 and three rotating stage
+// buffers; the last stage writes psi (it reads Y0 only at its own cell).
+template <class T>
+gc_status rkc_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, T* psi, double dt, const RkcCoeffs& c,
+                   T* f0, T* const (&yb)[3]) {
+  StageParams<T> p = base_params<T>(g, cp);
+  const int order = cp->order;
+  p.psi = psi;
+  p.kin = nullptr;
+  p.out = f0;
+  p.out2 = yb[0];
+  p.r[0] = static_cast<T>(c.mt1 * dt);
+  GC_TRY((launch_mode<T, MODE_RKC_FIRST>(ctx, order, p)));
+  const T* ym2 = psi;    // Y_{j-2}
+  const T* ym1 = yb[0];  // Y_{j-1}
+  for (int j = 2; j <= c.s; ++j) {
+    T* out = j == c.s ? psi : yb[(j - 1) % 3];
+    p.psi = ym1;
+    p.out = out;
+    p.k1 = psi;
+    p.k2 = ym2;
+    p.k3 = f0;
+    p.r[0] = static_cast<T>(1.0 - c.mu[j] - c.nu[j]);
+    p.r[1] = static_cast<T>(c.mu[j]);
+    p.r[2] = static_cast<T>(c.nu[j]);
+    p.r[3] = static_cast<T>(c.mt[j] * dt);
+    p.r[4] = static_cast<T>(c.gt[j] * dt);
+    GC_TRY((launch_mode<T, MODE_RKC>(ctx, order, p)));
+    ym2 = ym1;
+    ym1 = out;
+  }
+  return GC_OK;
+}
+
+template <class T>
+gc_status rhs_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const T* psi, T* out) {
+  StageParams<T> p = base_params<T>(g, cp);
+  p.psi = psi;
+  p.out = out;
+  return launch_mode<T, MODE_RHS>(ctx, cp->order, p);
+}
+
+template <class T>
+gc_status rkc_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, T* psi, double dt, int n_steps,
+                int stages) {
+  const size_t bytes = cells(g) * sizeof(T);
+  void *vf = nullptr, *va = nullptr, *vb = nullptr, *vc = nullptr;
+  GC_TRY(scratch_get(ctx, kSlotK1, bytes, &vf));
+  GC_TRY(scratch_get(ctx, kSlotK2, bytes, &va));
+  GC_TRY(scratch_get(ctx, kSlotK3, bytes, &vb));
+  GC_TRY(scratch_get(ctx, kSlotPsiB, bytes, &vc));
+  T* const yb[3] = {static_cast<T*>(va), static_cast<T*>(vb), static_cast<T*>(vc)};
+  const RkcCoeffs c = rkc_coeffs(stages);
+  for (int k = 0; k < n_steps; ++k) GC_TRY(rkc_step<T>(ctx, g, cp, psi, dt, c, static_cast<T*>(vf), yb));
+  return GC_OK;
+}
+
+}  // namespace
+
+gc_status ch_rhs_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, const void* psi,
+                         void* out) {
+  if (dt == GC_F64) return rhs_t<double>(ctx, g, cp, static_cast<const double*>(psi), static_cast<double*>(out));
+  return rhs_t<float>(ctx, g, cp, static_cast<const float*>(psi), static_cast<float*>(out));
+}
+
+gc_status ch_rkc_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
+                         double dt_step, int stages, void* const (&scratch)[4]) {
+  const RkcCoeffs c = rkc_coeffs(stages);
+  if (dt == GC_F64) {
+    double* const yb[3] = {static_cast<double*>(scratch[1]), static_cast<double*>(scratch[2]),
+                           static_cast<double*>(scratch[3])};
+    return rkc_step<double>(ctx, g, cp, static_cast<double*>(psi), dt_step, c, static_cast<double*>(scratch[0]), yb);
+  }
+  float* const yb[3] = {static_cast<float*>(scratch[1]), static_cast<float*>(scratch[2]),
+                        static_cast<float*>(scratch[3])};
+  return rkc_step<float>(ctx, g, cp, static_cast<float*>(psi), dt_step, c, static_cast<float*>(scratch[0]), yb);
+}
+
+namespace {
+
 gc_status check_ch(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp) {
   Call call(ctx);
   gc_status s = call.st;
@@ -566,16 +706,7 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt, const
   if (s != GC_OK) return s;
   if ((s = require_axes(g, cp->order / 2)) != GC_OK) return s;
   if (!psi || !out) return fail(GC_ERR_INVALID_ARG, "gc_ch_rhs: null field pointer");
-  if (dt == GC_F64) {
-    StageParams<double> p = base_params<double>(g, cp);
-    p.psi = static_cast<const double*>(psi);
-    p.out = static_cast<double*>(out);
-    return launch_mode<double, MODE_RHS>(ctx, cp->order, p);
-  }
-  StageParams<float> p = base_params<float>(g, cp);
-  p.psi = static_cast<const float*>(psi);
-  p.out = static_cast<float*>(out);
-  return launch_mode<float, MODE_RHS>(ctx, cp->order, p);
+  return ch_rhs_enqueue(ctx, g, dt, cp, psi, out);
 }
 
 GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
@@ -598,6 +729,27 @@ GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
   if (dt == GC_F64)
     return integrate_t<double>(ctx, g, cp, static_cast<double*>(psi), dt_step, n_steps, integ);
   return integrate_t<float>(ctx, g, cp, static_cast<float*>(psi), dt_step, n_steps, integ);
+}
+
+GC_API gc_status gc_ch_rkc(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
+                           double dt_step, int32_t n_steps, int32_t stages) {
+  Call call(ctx);
+  if (call.st != GC_OK) return call.st;
+  gc_status s = check_ch(ctx, g, dt, cp);
+  if (s != GC_OK) return s;
+  if (n_steps < 0 || !(dt_step >= 0.0))
+    return fail(GC_ERR_INVALID_ARG, "gc_ch_rkc: n_steps and dt must be >= 0");
+  if (stages < 2 || stages > 64) return fail(GC_ERR_INVALID_ARG, "gc_ch_rkc: stages must be in [2, 64]");
+  if (n_steps == 0) return GC_OK;
+  if ((s = require_axes(g, cp->order / 2)) != GC_OK) return s;
+  if (!psi) return fail(GC_ERR_INVALID_ARG, "gc_ch_rkc: null psi");
+  if (dt == GC_F64) return rkc_t<double>(ctx, g, cp, static_cast<double*>(psi), dt_step, n_steps, stages);
+  return rkc_t<float>(ctx, g, cp, static_cast<float*>(psi), dt_step, n_steps, stages);
+}
+
+GC_API double gc_rkc_stability_bound(int32_t stages) {
+  if (stages < 2 || stages > 64) return 0.0;
+  return rkc_coeffs(stages).beta;
 }
 
 }  // extern "C"

@@ -9,7 +9,10 @@
 namespace gcb {
 namespace {
 
-enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2 };
+// MODE_RKC_FIRST: out = f(psi), out2 = psi + r[0] f(psi)    (stage 1 of RKC2)
+// MODE_RKC:       out = r[0] Y0 + r[1] y + r[2] Yjm2 + r[3] f(y) + r[4] F0
+//                 with Y0 = k1, Yjm2 = k2, F0 = k3, summed left to right
+enum StageMode { MODE_RHS = 0, MODE_RK4_FINAL = 1, MODE_EULER_FINAL = 2, MODE_RKC_FIRST = 3, MODE_RKC = 4 };
 
 template <class T>
 struct StageParams {
@@ -21,6 +24,8 @@ struct StageParams {
   const T* k2;
   const T* k3;
   T c6, c3;        // dt/6, dt/3 (RK4 final) ; c6 = dt (Euler final)
+  T* out2;         // MODE_RKC_FIRST second output
+  T r[5];          // RKC stage coefficients
   T mob, kappa;
   T ihx2, ihy2, ihz2;
   int nx, ny, nz;
@@ -46,6 +51,17 @@ __device__ __forceinline__ T chem_pot(const StageParams<T>& p, T y, T lap) {
 template <class T>
 __device__ __forceinline__ T mobility(const StageParams<T>& p, T lap) {
   return p.unit_m ? lap : Ar<T>::mul(lap, p.mob);
+}
+
+// r0 Y0 + r1 y + r2 Yjm2 + r3 f + r4 F0, products rounded and summed left to
+// right (the order the RKC restatement in the tests uses).
+template <class T>
+__device__ __forceinline__ T rkc_combine(const StageParams<T>& p, T y0, T y, T yjm2, T f, T f0) {
+  T acc = Ar<T>::mul(p.r[0], y0);
+  acc = Ar<T>::add(acc, Ar<T>::mul(p.r[1], y));
+  acc = Ar<T>::add(acc, Ar<T>::mul(p.r[2], yjm2));
+  acc = Ar<T>::add(acc, Ar<T>::mul(p.r[3], f));
+  return Ar<T>::add(acc, Ar<T>::mul(p.r[4], f0));
 }
 
 // ---------------------------------------------------------------------------
@@ -222,6 +238,11 @@ __device__ __forceinline__ void pipelined_tiles(const Source& src, unsigned char
           const T s14 = Ar<T>::add(__ldg(p.k1 + gi), rhs);
           const T s23 = Ar<T>::add(__ldg(p.k2 + gi), rk[yc_idx]);
           p.out[gi] = Ar<T>::add(rp[yc_idx], Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
+        } else if constexpr (MODE == MODE_RKC_FIRST) {
+          p.out[gi] = rhs;
+          p.out2[gi] = Ar<T>::add(ys[yc_idx], Ar<T>::mul(p.r[0], rhs));
+        } else if constexpr (MODE == MODE_RKC) {
+          p.out[gi] = rkc_combine(p, p.k1[gi], ys[yc_idx], p.k2[gi], rhs, p.k3[gi]);
         } else {
           p.out[gi] = Ar<T>::add(rp[yc_idx], Ar<T>::mul(p.c6, rhs));
         }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 
 #include "gridcalc_b200.h"
@@ -26,6 +27,12 @@ gc_status cuda_fail(cudaError_t e, const char* what);
   do {                                                           \
     cudaError_t gc_e_ = cudaGetLastError();                      \
     if (gc_e_ != cudaSuccess) return ::gcb::cuda_fail(gc_e_, what); \
+  } while (0)
+
+#define GC_TRY(expr)                                             \
+  do {                                                           \
+    gc_status gc_s_ = (expr);                                    \
+    if (gc_s_ != GC_OK) return gc_s_;                            \
   } while (0)
 
 // ---------------------------------------------------------------------------
@@ -82,6 +89,17 @@ gc_status check_grid(const gc_grid* g);
 gc_status require_axes(const gc_grid* g, int radius);
 gc_status check_ctx(gc_context* ctx);
 
+// Stream-ordered building blocks for other parts of the library (no
+// validation, no Call scope, no allocation): enqueue on ctx->stream only, so
+// they can be captured into a CUDA graph.
+// f(psi) of the Cahn-Hilliard RHS into out.
+gc_status ch_rhs_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, const void* psi,
+                         void* out);
+// One RKC2 step of psi in place; scratch = four fields of the grid's size
+// (F0 and three stage buffers).
+gc_status ch_rkc_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
+                         double dt_step, int stages, void* const (&scratch)[4]);
+
 // Scope of one API call: validates the context, orders the context stream
 // after the caller's stream on entry and the caller's stream after the
 // context stream on exit.
@@ -91,6 +109,11 @@ struct Call {
   explicit Call(gc_context* c);
   ~Call();
 };
+inline uint64_t bits_of(double d) {
+  uint64_t b;
+  std::memcpy(&b, &d, sizeof b);
+  return b;
+}
 inline size_t cells(const gc_grid* g) {
   return static_cast<size_t>(g->nx) * static_cast<size_t>(g->ny) * static_cast<size_t>(g->nz);
 }

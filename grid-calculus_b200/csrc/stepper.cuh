@@ -75,10 +75,4 @@ gc_status run_steps(gc_context* ctx, T* psi, T* other, size_t bytes, int n_steps
   return GC_OK;
 }
 
-inline uint64_t bits_of(double d) {
-  uint64_t b;
-  std::memcpy(&b, &d, sizeof b);
-  return b;
-}
-
 }  // namespace gcb

@@ -23,7 +23,8 @@ __all__ = [
     "Pairwise", "Kahan", "RK4", "ExplicitEuler", "CahnHilliardRhs",
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
-    "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params",
+    "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
+    "rkc_stability_bound",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -79,6 +80,7 @@ _SIGS = {
     "gc_diffuse": [_vp, _gp, _i32, _vp, _dbl, _dbl, _i32, _i32],
     "gc_diffuse_fvm": [_vp, _gp, _i32, _vp, _vp, _dbl, _i32, _i32, C.POINTER(C.c_int64)],
     "gc_d_max_face": [_vp, _gp, _i32, _vp, C.POINTER(C.c_double)],
+    "gc_ch_rkc": [_vp, _gp, _i32, C.POINTER(gc_ch_params), _vp, _dbl, C.c_int32, C.c_int32],
 }
 
 
@@ -103,6 +105,8 @@ for _name, _args in _SIGS.items():
 lib.gc_last_error.restype = C.c_char_p
 lib.gc_last_error.argtypes = []
 lib.gc_version.restype = C.c_char_p
+lib.gc_rkc_stability_bound.restype = C.c_double
+lib.gc_rkc_stability_bound.argtypes = [C.c_int32]
 lib.gc_status_string.restype = C.c_char_p
 lib.gc_status_string.argtypes = [C.c_int]
 
@@ -344,6 +348,20 @@ def ch_rhs(psi, grid: Grid, rhs: CahnHilliardRhs, out=None, ctx=None):
     _check(lib.gc_ch_rhs(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), C.byref(rhs.c()),
                          psi.data_ptr(), out.data_ptr()))
     return out
+
+
+def ch_rkc(psi, grid: Grid, rhs: CahnHilliardRhs, dt: float, n_steps: int, stages: int, ctx=None):
+    """n_steps damped RKC2 steps of dt with `stages` stages, psi in place (no
+    reference counterpart: the base step of the learned coarse step)."""
+    _require(psi, grid)
+    _check(lib.gc_ch_rkc(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), C.byref(rhs.c()),
+                         psi.data_ptr(), dt, n_steps, stages))
+    return psi
+
+
+def rkc_stability_bound(stages: int) -> float:
+    """beta(s): RKC2 is stable for dt * lambda_max <= beta(s)."""
+    return lib.gc_rkc_stability_bound(stages)
 
 
 def ch_integrate(psi, grid: Grid, rhs: CahnHilliardRhs, dt: float, n_steps: int, tag=RK4, ctx=None):

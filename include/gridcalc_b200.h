@@ -186,6 +186,16 @@ GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
                                  const gc_ch_params* p, void* psi, double dt_step,
                                  int n_steps, gc_integrator integrator);
 
+/* RKC2 (damped second-order Runge-Kutta-Chebyshev, eps = 2/13) with
+ * `stages` stages (2..64): n_steps steps of dt_step, psi in place, same RHS
+ * as gc_ch_integrate.  No reference counterpart (the reference offers
+ * Euler and RK4); it is the base step of the learned coarse step.  Stable
+ * for dt_step * lambda_max <= gc_rkc_stability_bound(stages) (~0.65 s^2),
+ * lambda_max the spectral radius of the linearised RHS. */
+GC_API gc_status gc_ch_rkc(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* p, void* psi,
+                           double dt_step, int32_t n_steps, int32_t stages);
+GC_API double gc_rkc_stability_bound(int32_t stages);
+
 /* solve::diffuse(psi, double D, dt, n_steps, tag) (solve/Diffusion.hpp:89-112):
  * constant-D heat equation with the order-2 Laplacian and the tag's CFL check. */
 GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi,
