@@ -1,12 +1,22 @@
 // Learned coarse-step corrector for 2-D Cahn-Hilliard: a 6-layer periodic
-// 3x3 CNN (32 channels, GELU), BF16 weights and activations, FP32
+// 3x3 CNN (32 channels, GELU in tanh form), BF16 weights and activations, FP32
 // accumulation on the tensor cores (mma.sync m16n8k16 bf16), trained and run
 // by the kernels in this file.
 //
-// Network: x0 = [c, 0, ..., 0] (32 channels, NHWC), for l = 1..6:
+// Network: x0 = [c, u, e, 0, ..., 0] (32 channels, NHWC), for l = 1..6:
 //   z_l = conv3x3_periodic(x_{l-1}, W_l) + b_l,  x_l = gelu(z_l) (l < 6);
-// the correction is delta = s_out * (z_6[ch 0] - mean(z_6[ch 0])) per sample
-// (zero mean, so the coarse step c + delta conserves mass).  Every layer is
+// the correction is delta = s_out * rho * (z_6[ch 0] - mean(z_6[ch 0]))
+// per sample (zero mean, so the coarse step conserves mass).
+// Without a base step: u = e = 0, rho = 1 and the coarse step is c + delta.
+// With a base step B (one RKC2 step of the coarse dt Dt, gc_ch_rkc) the
+// coarse step is B(c) + delta, and the network sees the base step's
+// increment and its error indicator, each scaled to unit RMS per sample:
+//   u = (B(c) - c) / rms(B(c) - c),
+//   e = est / rms(est),  est = (B(c) - c) / Dt - (f(c) + f(B(c))) / 2
+// (the trapezoid residual of the base step, f the Cahn-Hilliard RHS), with
+// rho = Dt rms(est): the correction is learned in units of the base step's
+// own error indicator, so small late-time errors are corrected as precisely
+// as large early ones.  Every layer is
 // computed as a 32 -> 32 convolution (the first layer's input channels
 // 1..31 are zero and the last layer's outputs 1..31 are unused), so one
 // implicit-GEMM kernel serves all layers: M = pixels, N = 32 output
@@ -33,13 +43,38 @@ constexpr int kTaps = 9;
 constexpr int kLayerParams = kTaps * kC * kC + kC;
 constexpr int kParams = kLayers * kLayerParams;
 constexpr int kPixStride = 40;               // bf16 per pixel in shared memory (80 B: conflict-free)
-constexpr int kTR = 8, kTC = 16;             // conv tile: 8 rows x 16 columns of pixels
-constexpr int kConvThreads = 128;            // 4 warps, 2 rows (2 m16 tiles) each
+// Weight-gradient tiles: 8 rows x 16 columns of pixels.
+constexpr int kTR = 8, kTC = 16;
 constexpr int kHaloR = kTR + 2, kHaloC = kTC + 2;
+// Forward / backward-data tiles: 4 rows x 64 columns (256 pixels), 8 warps;
+// warp w owns row w / 2, columns (w % 2) * 32 .. + 31 (two m16 tiles).
+constexpr int kCR = 4, kCC = 64;
+constexpr int kConvThreads = 256;
+constexpr int kInR = kCR + 2, kInC = kCC + 2, kInPix = kInR * kInC;
+constexpr int kConvSmemW = kTaps * kC * kPixStride * 2;     // 23,040 B
+constexpr int kConvSmemIn = kInPix * kPixStride * 2;         // 31,680 B per buffer
+constexpr int kConvSmem = kConvSmemW + 2 * kConvSmemIn;      // 86,400 B: two CTAs per SM
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016):
+//   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
+//   gelu'(z) = (1 + tanh(u))/2 + z/2 (1 - tanh(u)^2) sqrt(2/pi) (1 + 3 0.044715 z^2),
+// with the hardware tanh (tanh.approx.f32, relative error ~2^-11, below the
+// bf16 rounding of the activations it feeds).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluA = 0.7978845608028654f;   // sqrt(2/pi)
+constexpr float kGeluB = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(kGeluA * fmaf(kGeluB * z * z, z, z));
+  return 0.5f * z * (1.0f + t);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float z2 = z * z;
+  const float t = tanh_hw(kGeluA * fmaf(kGeluB * z2, z, z));
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluA * fmaf(3.0f * kGeluB, z2, 1.0f);
 }
 
 __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
@@ -55,109 +90,157 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t (&r)[2], const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void cp_async16(void* s, const void* g) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(s)), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---- forward / backward-data convolution ----------------------------------
 // out[p][n] = sum_t sum_k in[p + off_t][k] * Bw[t][n][k]  (+ epilogue)
 // Epilogue kinds:
-//   EPI_FWD    z = acc + bias; store z (bf16) and gelu(z) (bf16)
+//   EPI_FWD    z = acc + bias; store gelu(z) (bf16) and, for training, z (bf16)
 //   EPI_LAST   z0 = acc + bias (channel 0 only); store z0 (fp32)
 //   EPI_BWD    dz_prev = acc * gelu'(z_prev); store (bf16)
+// Persistent CTAs: the layer's weights are staged once; pixel tiles (with a
+// one-pixel periodic halo) are double-buffered with cp.async so the next
+// tile's loads overlap this tile's tensor-core work.  Operands reach the
+// tensor cores through ldmatrix from 80-byte pixel rows (conflict-free).
 enum Epi { EPI_FWD = 0, EPI_LAST = 1, EPI_BWD = 2 };
 
-template <int EPI, int NT>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(
+template <int EPI, int NT, bool STORE_Z>
+__global__ void __launch_bounds__(kConvThreads, 2) conv3x3_kernel(
     const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ bw, const float* __restrict__ bias,
     __nv_bfloat16* __restrict__ out_z, __nv_bfloat16* __restrict__ out_y, float* __restrict__ out_f,
-    const __nv_bfloat16* __restrict__ z_prev, int H, int W, int tiles_x, int tiles_per_img) {
-  __shared__ __align__(16) __nv_bfloat16 s_in[kHaloR * kHaloC * kPixStride];
-  __shared__ __align__(16) __nv_bfloat16 s_w[kTaps * kC * kPixStride];
+    const __nv_bfloat16* __restrict__ z_prev, int H, int W, int tiles_x, int tiles_per_img, int n_tiles) {
+  extern __shared__ __align__(16) unsigned char conv_smem[];
+  __nv_bfloat16* s_w = reinterpret_cast<__nv_bfloat16*>(conv_smem);
+  __nv_bfloat16* s_in = reinterpret_cast<__nv_bfloat16*>(conv_smem + kConvSmemW);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tig = lane & 3;
-  const int img = blockIdx.x / tiles_per_img;
-  const int tile = blockIdx.x - img * tiles_per_img;
-  const int y0 = (tile / tiles_x) * kTR, x0 = (tile % tiles_x) * kTC;
-  const size_t img_off = static_cast<size_t>(img) * H * W;
+  const int wr = warp >> 1, wc = (warp & 1) * 32;
 
-  // Weights: [t][n][k] dense 32 -> padded rows of 40.
-  for (int v = tid; v < kTaps * kC * (kC / 8); v += kConvThreads) {
-    const int row = v >> 2, q = v & 3;  // row = t * 32 + n
-    *reinterpret_cast<uint4*>(&s_w[row * kPixStride + q * 8]) = reinterpret_cast<const uint4*>(bw)[v];
-  }
-  // Input tile with a one-pixel periodic halo.
-  for (int v = tid; v < kHaloR * kHaloC * (kC / 8); v += kConvThreads) {
-    const int pix = v >> 2, q = v & 3;
-    const int r = pix / kHaloC, c = pix - r * kHaloC;
-    const int gy = wrap(y0 - 1 + r, H), gx = wrap(x0 - 1 + c, W);
-    const size_t gp = img_off + static_cast<size_t>(gy) * W + gx;
-    *reinterpret_cast<uint4*>(&s_in[pix * kPixStride + q * 8]) =
-        reinterpret_cast<const uint4*>(in + gp * kC)[q];
-  }
-  __syncthreads();
+  // Weights [t][n][k] (dense 32 x 32 per tap) -> rows of 40.
+  for (int v = tid; v < kTaps * kC * (kC / 8); v += kConvThreads)
+    cp_async16(&s_w[(v >> 2) * kPixStride + (v & 3) * 8], bw + static_cast<size_t>(v) * 8);
 
-  float acc[2][NT][4];
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.f;
-
-#pragma unroll
-  for (int t = 0; t < kTaps; ++t) {
-    const int dy = t / 3 - 1, dx = t % 3 - 1;
-#pragma unroll
-    for (int kh = 0; kh < 2; ++kh) {
-      uint32_t b[NT][2];
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt) {
-        const __nv_bfloat16* wp = &s_w[(t * kC + nt * 8 + g) * kPixStride + kh * 16 + tig * 2];
-        b[nt][0] = *reinterpret_cast<const uint32_t*>(wp);
-        b[nt][1] = *reinterpret_cast<const uint32_t*>(wp + 8);
-      }
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        const int r = warp * 2 + mt + 1 + dy;
-        const __nv_bfloat16* p0 = &s_in[(r * kHaloC + g + 1 + dx) * kPixStride + kh * 16 + tig * 2];
-        const __nv_bfloat16* p1 = p0 + 8 * kPixStride;
-        uint32_t a[4];
-        a[0] = *reinterpret_cast<const uint32_t*>(p0);
-        a[1] = *reinterpret_cast<const uint32_t*>(p1);
-        a[2] = *reinterpret_cast<const uint32_t*>(p0 + 8);
-        a[3] = *reinterpret_cast<const uint32_t*>(p1 + 8);
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], a, b[nt]);
-      }
+  auto issue = [&](int tl, int buf) {
+    const int img = tl / tiles_per_img;
+    const int tile = tl - img * tiles_per_img;
+    const int y0 = (tile / tiles_x) * kCR, x0 = (tile % tiles_x) * kCC;
+    const size_t img_off = static_cast<size_t>(img) * H * W;
+    __nv_bfloat16* dst = s_in + buf * (kInPix * kPixStride);
+    for (int v = tid; v < kInPix * (kC / 8); v += kConvThreads) {
+      const int pix = v >> 2, q = v & 3;
+      const int r = pix / kInC, c = pix - r * kInC;
+      const size_t gp = img_off + static_cast<size_t>(wrap(y0 - 1 + r, H)) * W + wrap(x0 - 1 + c, W);
+      cp_async16(dst + pix * kPixStride + q * 8, in + gp * kC + q * 8);
     }
-  }
+  };
 
-  // Epilogue: C fragment rows are pixels g and g + 8, columns 2 tig, 2 tig + 1.
+  issue(blockIdx.x, 0);  // the grid never exceeds n_tiles
+  cp_commit();
+  int it = 0;
+  for (int tl = blockIdx.x; tl < n_tiles; tl += gridDim.x, ++it) {
+    const int buf = it & 1;
+    if (tl + static_cast<int>(gridDim.x) < n_tiles) issue(tl + gridDim.x, buf ^ 1);
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();
+    const __nv_bfloat16* sb = s_in + buf * (kInPix * kPixStride);
+
+    float acc[2][NT][4];
 #pragma unroll
-  for (int mt = 0; mt < 2; ++mt) {
-    const int oy = y0 + warp * 2 + mt;
-    if (oy >= H) continue;
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int ox = x0 + g + half * 8;
-      if (ox >= W) continue;
-      const size_t gp = img_off + static_cast<size_t>(oy) * W + ox;
+      for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-      for (int nt = 0; nt < NT; ++nt) {
-        const int n = nt * 8 + tig * 2;
-        float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
-        if constexpr (EPI == EPI_FWD) {
-          v0 += bias[n];
-          v1 += bias[n + 1];
-          *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) = pack_bf16(v0, v1);
-          *reinterpret_cast<uint32_t*>(out_y + gp * kC + n) = pack_bf16(gelu(v0), gelu(v1));
-        } else if constexpr (EPI == EPI_LAST) {
-          if (n == 0) out_f[gp] = v0 + bias[0];
+        for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.f;
+
+#pragma unroll
+    for (int t = 0; t < kTaps; ++t) {
+      const int dy = t / 3 - 1, dx = t % 3 - 1;
+#pragma unroll
+      for (int kh = 0; kh < 2; ++kh) {
+        uint32_t b[NT][2];
+        if constexpr (NT == 4) {
+#pragma unroll
+          for (int pr = 0; pr < 2; ++pr) {
+            uint32_t r[4];
+            const int n = t * kC + pr * 16 + (lane & 7) + ((lane >> 4) << 3);
+            ldsm_x4(r, &s_w[n * kPixStride + kh * 16 + ((lane >> 3) & 1) * 8]);
+            b[2 * pr][0] = r[0];
+            b[2 * pr][1] = r[1];
+            b[2 * pr + 1][0] = r[2];
+            b[2 * pr + 1][1] = r[3];
+          }
         } else {
-          const __nv_bfloat162 zp = *reinterpret_cast<const __nv_bfloat162*>(z_prev + gp * kC + n);
-          const float2 zf = __bfloat1622float2(zp);
-          *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) = pack_bf16(v0 * gelu_grad(zf.x), v1 * gelu_grad(zf.y));
+          uint32_t r[2];
+          ldsm_x2(r, &s_w[(t * kC + (lane & 7)) * kPixStride + kh * 16 + ((lane >> 3) & 1) * 8]);
+          b[0][0] = r[0];
+          b[0][1] = r[1];
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const int pix = (wr + 1 + dy) * kInC + (wc + mt * 16 + (lane & 15) + 1 + dx);
+          uint32_t a[4];
+          ldsm_x4(a, &sb[pix * kPixStride + kh * 16 + (lane >> 4) * 8]);
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], a, b[nt]);
         }
       }
     }
+
+    // Epilogue: C fragment rows are pixels g and g + 8 of the m16 tile,
+    // columns (channels) 2 tig, 2 tig + 1 of each n8 tile.
+    const int img = tl / tiles_per_img;
+    const int tile = tl - img * tiles_per_img;
+    const int oy = (tile / tiles_x) * kCR + wr, x0 = (tile % tiles_x) * kCC;
+    const size_t img_off = static_cast<size_t>(img) * H * W;
+    if (oy < H) {
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+          const int ox = x0 + wc + mt * 16 + g + half * 8;
+          if (ox >= W) continue;
+          const size_t gp = img_off + static_cast<size_t>(oy) * W + ox;
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) {
+            const int n = nt * 8 + tig * 2;
+            float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
+            if constexpr (EPI == EPI_FWD) {
+              v0 += bias[n];
+              v1 += bias[n + 1];
+              if constexpr (STORE_Z) *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) = pack_bf16(v0, v1);
+              *reinterpret_cast<uint32_t*>(out_y + gp * kC + n) = pack_bf16(gelu(v0), gelu(v1));
+            } else if constexpr (EPI == EPI_LAST) {
+              if (n == 0) out_f[gp] = v0 + bias[0];
+            } else {
+              const __nv_bfloat162 zp = *reinterpret_cast<const __nv_bfloat162*>(z_prev + gp * kC + n);
+              const float2 zf = __bfloat1622float2(zp);
+              *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) =
+                  pack_bf16(v0 * gelu_grad(zf.x), v1 * gelu_grad(zf.y));
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // every warp is done with buf before it is refilled
   }
+  cp_wait<0>();
 }
 
 // ---- weight gradient ------------------------------------------------------
@@ -265,17 +348,43 @@ __global__ void sum_partials(const float* __restrict__ partial, int n_parts, flo
 }
 
 // ---- input, output, loss --------------------------------------------------
-// Channel 0 = c, channel 1 = feature_scale * f (the right-hand side when
-// features are on, else 0), channels 2..31 = 0.
+__device__ __forceinline__ float inv_rms(const float* ms, size_t b) {
+  const float v = ms[b];
+  return v > 0.f ? rsqrtf(v) : 0.f;
+}
+
+// incr = B(c) - c and est = incr / Dt - (f(c) + f(B(c))) / 2, formed in T
+// and rounded to float, with their squares.
 template <class T>
-__global__ void pack_input(const T* __restrict__ c, const T* __restrict__ f, float feature_scale, size_t n,
+__global__ void base_features(const T* __restrict__ c, const T* __restrict__ base, const T* __restrict__ f0,
+                              const T* __restrict__ fb, T inv_dt, size_t n, float* __restrict__ incr,
+                              float* __restrict__ est, float* __restrict__ sq_incr, float* __restrict__ sq_est) {
+  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const T d = base[p] - c[p];
+    const float u = static_cast<float>(d);
+    const float e = static_cast<float>(d * inv_dt - T(0.5) * (f0[p] + fb[p]));
+    incr[p] = u;
+    est[p] = e;
+    sq_incr[p] = u * u;
+    sq_est[p] = e * e;
+  }
+}
+
+// Channel 0 = c, channels 1, 2 = incr and est at unit RMS per sample (0
+// without a base step), channels 3..31 = 0.
+template <class T>
+__global__ void pack_input(const T* __restrict__ c, const float* __restrict__ incr, const float* __restrict__ ms,
+                           const float* __restrict__ est, const float* __restrict__ ms_est, int hw, size_t n,
                            __nv_bfloat16* __restrict__ x0) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     uint4* dst = reinterpret_cast<uint4*>(x0 + p * kC);
     uint4 z = make_uint4(0, 0, 0, 0);
-    const float fv = f ? feature_scale * static_cast<float>(f[p]) : 0.f;
-    z.x = pack_bf16(static_cast<float>(c[p]), fv);
+    const float u = incr ? incr[p] * inv_rms(ms, p / hw) : 0.f;
+    const float e = est ? est[p] * inv_rms(ms_est, p / hw) : 0.f;
+    z.x = pack_bf16(static_cast<float>(c[p]), u);
+    z.y = pack_bf16(e, 0.f);
     dst[0] = z;
     dst[1] = make_uint4(0, 0, 0, 0);
     dst[2] = make_uint4(0, 0, 0, 0);
@@ -283,50 +392,80 @@ __global__ void pack_input(const T* __restrict__ c, const T* __restrict__ f, flo
   }
 }
 
-// Per-sample mean of f over H*W pixels (one CTA per sample, fixed order).
-__global__ void sample_mean(const float* __restrict__ f, int hw, float* __restrict__ mean) {
+// Per-sample mean of f over H*W pixels in two fixed-order passes: kMeanParts
+// CTAs per sample sum contiguous chunks in double, then one warp per sample
+// adds the partials in order.
+constexpr int kMeanParts = 32;
+
+__global__ void sample_sum_parts(const float* __restrict__ f, int hw, double* __restrict__ part) {
   __shared__ double sh[256];
-  const float* s = f + static_cast<size_t>(blockIdx.x) * hw;
+  const int b = blockIdx.y, k = blockIdx.x;
+  const int len = (hw + kMeanParts - 1) / kMeanParts;
+  const int lo = k * len, hi = min(hw, lo + len);
+  const float* s = f + static_cast<size_t>(b) * hw;
   double acc = 0.0;
-  for (int i = threadIdx.x; i < hw; i += 256) acc += s[i];
+  for (int i = lo + threadIdx.x; i < hi; i += 256) acc += s[i];
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int w = 128; w >= 1; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) mean[blockIdx.x] = static_cast<float>(sh[0] / hw);
+  if (threadIdx.x == 0) part[b * kMeanParts + k] = sh[0];
 }
 
-// delta = s_out (z - mean_z)
-__global__ void project_delta(const float* __restrict__ z, const float* __restrict__ mean, int hw, size_t n,
-                              float s_out, float* __restrict__ delta) {
-  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
-       p += static_cast<size_t>(gridDim.x) * blockDim.x)
-    delta[p] = s_out * (z[p] - mean[p / hw]);
+__global__ void sample_mean_final(const double* __restrict__ part, int hw, int batch, float* __restrict__ mean) {
+  const int b = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (b >= batch) return;
+  double v = lane < kMeanParts ? part[b * kMeanParts + lane] : 0.0;
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) mean[b] = static_cast<float>(v / hw);
 }
 
-// (target - c)^2, for the per-sample step size of the normalised loss.
-__global__ void step_sq(const float* __restrict__ c, const float* __restrict__ target, size_t n,
-                        float* __restrict__ out) {
+
+// delta = scale rho_b (z - mean_z), rho_b = sqrt(ms[b]) (1 without ms).
+__global__ void project_delta(const float* __restrict__ z, const float* __restrict__ mean,
+                              const float* __restrict__ ms, int hw, size_t n, float scale,
+                              float* __restrict__ delta) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float d = target[p] - c[p];
+    const float rho = ms ? sqrtf(ms[p / hw]) : 1.f;
+    delta[p] = scale * rho * (z[p] - mean[p / hw]);
+  }
+}
+
+// out = incr + delta: the whole coarse-step increment.
+__global__ void add_increment(const float* __restrict__ incr, const float* __restrict__ delta, size_t n,
+                              float* __restrict__ out) {
+  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<size_t>(gridDim.x) * blockDim.x)
+    out[p] = incr[p] + delta[p];
+}
+
+// (target - start)^2, for the per-sample scale of the normalised loss.
+template <class T>
+__global__ void step_sq(const T* __restrict__ c, const T* __restrict__ target, size_t n, float* __restrict__ out) {
+  for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
+       p += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const float d = static_cast<float>(target[p] - c[p]);
     out[p] = d * d;
   }
 }
 
-// r = c + delta - target, stored; per-CTA partial sums of r^2 / den[sample]
+// r = start + delta - target (start = B(c) with a base step, else c),
+// formed in T and stored as float; per-CTA partial sums of r^2 / den[sample]
 // (den = 1 for the plain loss; fixed grid).
-__global__ void residual_kernel(const float* __restrict__ c, const float* __restrict__ delta,
-                                const float* __restrict__ target, size_t n, int hw,
+template <class T>
+__global__ void residual_kernel(const T* __restrict__ start, const float* __restrict__ delta,
+                                const T* __restrict__ target, size_t n, int hw,
                                 const float* __restrict__ den, float* __restrict__ r,
                                 double* __restrict__ part) {
   __shared__ double sh[256];
   double acc = 0.0;
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const float v = c[p] + delta[p] - target[p];
+    const float v = static_cast<float>((start[p] - target[p]) + static_cast<T>(delta[p]));
     r[p] = v;
     const double w = den ? 1.0 / static_cast<double>(den[p / hw]) : 1.0;
     acc += static_cast<double>(v) * v * w;
@@ -340,14 +479,16 @@ __global__ void residual_kernel(const float* __restrict__ c, const float* __rest
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-// dz6 (channel 0) = s_out * 2/N (r - mean_sample(r)) / den[sample];
-// other channels 0.
+// dz6 (channel 0) = scale rho_b 2/N (r - mean_sample(r)) / den[sample]
+// (scale = s_out Dt with a base step, else s_out; `scale` here already
+// includes 2/N); other channels 0.
 __global__ void last_layer_grad(const float* __restrict__ r, const float* __restrict__ rmean, int hw, size_t n,
-                                float scale, const float* __restrict__ den, __nv_bfloat16* __restrict__ dz) {
+                                float scale, const float* __restrict__ den, const float* __restrict__ ms,
+                                __nv_bfloat16* __restrict__ dz) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
     uint4* dst = reinterpret_cast<uint4*>(dz + p * kC);
-    const float w = den ? 1.0f / den[p / hw] : 1.0f;
+    const float w = (den ? 1.0f / den[p / hw] : 1.0f) * (ms ? sqrtf(ms[p / hw]) : 1.f);
     __nv_bfloat16 v = __float2bfloat16(scale * w * (r[p] - rmean[p / hw]));
     uint4 z = make_uint4(static_cast<uint32_t>(*reinterpret_cast<uint16_t*>(&v)), 0, 0, 0);
     dst[0] = z;
@@ -385,7 +526,7 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
   w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// cand = psi + delta
+// cand = start + delta (start = B(psi) with a base step, else psi)
 __global__ void apply_delta(const double* __restrict__ psi, const float* __restrict__ delta, size_t n,
                             double* __restrict__ cand) {
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
@@ -393,33 +534,52 @@ __global__ void apply_delta(const double* __restrict__ psi, const float* __restr
     cand[p] = psi[p] + static_cast<double>(delta[p]);
 }
 
-// Trapezoid residual of a coarse step: sums of ((c1 - c0)/dt - (f0 + f1)/2)^2
-// and ((f0 + f1)/2)^2, per CTA (fixed grid).
-__global__ void trapezoid_residual(const double* __restrict__ c0, const double* __restrict__ c1,
-                                   const double* __restrict__ f0, const double* __restrict__ f1, size_t n,
-                                   double inv_dt, double* __restrict__ part) {
-  __shared__ double sr[256], sf[256];
-  double ar = 0.0, af = 0.0;
+// Acceptance statistics of a coarse step, per CTA (fixed grid, double):
+//   [0] sum of the free-energy density of c1, -c^2/2 + c^4/4 + kappa/2 |grad c|^2
+//       (order-2 central gradient, the reference's density), times the cell area;
+//   [1] sum of ((c1 - c0)/Dt - (f0 + f1)/2)^2 and [2] of ((f0 + f1)/2)^2
+//       (the trapezoid residual; skipped when c0 is null).
+// 2-D periodic grid; part holds 3 x gridDim.x doubles.
+__global__ void accept_stats(const double* __restrict__ c0, const double* __restrict__ c1,
+                             const double* __restrict__ f0, const double* __restrict__ f1, int nx, int ny,
+                             double inv_2hx, double inv_2hy, double area, double kappa, double inv_dt,
+                             double* __restrict__ part) {
+  __shared__ double se[256], sr[256], sf[256];
+  double ae = 0.0, ar = 0.0, af = 0.0;
+  const size_t n = static_cast<size_t>(nx) * ny;
   for (size_t p = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; p < n;
        p += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const double fm = 0.5 * (f0[p] + f1[p]);
-    const double r = (c1[p] - c0[p]) * inv_dt - fm;
-    ar += r * r;
-    af += fm * fm;
+    const int j = static_cast<int>(p / nx), i = static_cast<int>(p - static_cast<size_t>(j) * nx);
+    const double c = c1[p];
+    const double gx = (c1[static_cast<size_t>(j) * nx + wrap(i + 1, nx)] -
+                       c1[static_cast<size_t>(j) * nx + wrap(i - 1, nx)]) * inv_2hx;
+    const double gy = (c1[static_cast<size_t>(wrap(j + 1, ny)) * nx + i] -
+                       c1[static_cast<size_t>(wrap(j - 1, ny)) * nx + i]) * inv_2hy;
+    const double c2 = c * c;
+    ae += -0.5 * c2 + 0.25 * c2 * c2 + 0.5 * kappa * (gx * gx + gy * gy);
+    if (c0) {
+      const double fm = 0.5 * (f0[p] + f1[p]);
+      const double r = (c - c0[p]) * inv_dt - fm;
+      ar += r * r;
+      af += fm * fm;
+    }
   }
+  se[threadIdx.x] = ae;
   sr[threadIdx.x] = ar;
   sf[threadIdx.x] = af;
   __syncthreads();
   for (int w = 128; w >= 1; w >>= 1) {
     if (threadIdx.x < w) {
+      se[threadIdx.x] += se[threadIdx.x + w];
       sr[threadIdx.x] += sr[threadIdx.x + w];
       sf[threadIdx.x] += sf[threadIdx.x + w];
     }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    part[2 * blockIdx.x] = sr[0];
-    part[2 * blockIdx.x + 1] = sf[0];
+    part[3 * blockIdx.x] = se[0] * area;
+    part[3 * blockIdx.x + 1] = sr[0];
+    part[3 * blockIdx.x + 2] = sf[0];
   }
 }
 
@@ -450,17 +610,31 @@ struct gc_corrector {
   float* mean2 = nullptr;
   float* cbuf = nullptr;            // fp32 copies of inputs / targets
   float* tbuf = nullptr;
-  double* part = nullptr;
+  double* part = nullptr;           // per-CTA partial sums (3 x kRedBlocks)
   float* wpart = nullptr;           // per-CTA weight-gradient partials
   int wparts = 0;
-  double* adv = nullptr;            // advance scratch: cand, f0, f1 (H x W each)
-  // Right-hand-side input feature: channel 1 = feature_dt * f(c), f the
-  // Cahn-Hilliard RHS with chp (off until gc_corrector_set_physics).
-  bool feature = false;
+  double* mpart = nullptr;          // per-sample partial sums (kMeanParts per sample)
+  double* adv = nullptr;            // advance scratch: cand, f1 (H x W each)
+  double* rkc = nullptr;            // base-step scratch: 4 fields of H x W doubles
+  double* host_part = nullptr;      // pinned copy of the acceptance partials
+  // Captured graph of one proposed coarse step (forward, candidate,
+  // acceptance statistics), rebuilt when anything it bakes in changes.
+  cudaGraphExec_t prop_exec = nullptr;
+  uint64_t prop_key[8] = {};
+  // Base step B = one RKC2 step of dt_coarse with `stages` stages and the
+  // Cahn-Hilliard RHS chp (off until gc_corrector_set_base).
+  bool base = false;
   gc_ch_params chp{1.0, 1.0, 2};
-  double feature_dt = 0.0;
-  double* fbuf = nullptr;           // f(c), max_batch x H x W (double-sized)
-  float* den = nullptr;             // per-sample step size (normalised loss)
+  double dt_coarse = 0.0;
+  int stages = 0;
+  double* bbuf = nullptr;           // B(c), max_batch x H x W (double-sized)
+  double* f0buf = nullptr;          // f(c)
+  double* fbbuf = nullptr;          // f(B(c))
+  float* incr = nullptr;            // B(c) - c
+  float* est = nullptr;             // trapezoid residual of the base step
+  float* ms = nullptr;              // per-sample mean squares of incr, est
+  float* ms_est = nullptr;
+  float* den = nullptr;             // per-sample scale of the normalised loss
   bool normalized = false;
   bool weights_dirty = true;
 };
@@ -479,66 +653,117 @@ gc_status corr_layout(gc_corrector* c) {
   return GC_OK;
 }
 
+gc_status sample_mean(gc_corrector* c, int batch, const float* f, int hw, float* mean) {
+  cudaStream_t st = c->ctx->stream;
+  sample_sum_parts<<<dim3(kMeanParts, batch), 256, 0, st>>>(f, hw, c->mpart);
+  GC_CHECK_LAUNCH("sample_sum_parts");
+  sample_mean_final<<<div_up(batch, 8), 256, 0, st>>>(c->mpart, hw, batch, mean);
+  GC_CHECK_LAUNCH("sample_mean_final");
+  return GC_OK;
+}
+
+template <int EPI, int NT, bool STORE_Z>
+gc_status launch_conv(gc_corrector* c, int batch, const __nv_bfloat16* in, const __nv_bfloat16* w,
+                      const float* bias, __nv_bfloat16* oz, __nv_bfloat16* oy, float* of, const __nv_bfloat16* zp) {
+  auto kern = conv3x3_kernel<EPI, NT, STORE_Z>;
+  static bool attr = false;  // one flag per instantiation
+  if (!attr) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+    attr = true;
+  }
+  const int tiles_x = div_up(c->W, kCC), tiles_y = div_up(c->H, kCR);
+  const int tpi = tiles_x * tiles_y;
+  const int n_tiles = batch * tpi;
+  const int grid = std::min(n_tiles, 2 * c->ctx->num_sms);
+  kern<<<grid, kConvThreads, kConvSmem, c->ctx->stream>>>(in, w, bias, oz, oy, of, zp, c->H, c->W, tiles_x, tpi,
+                                                          n_tiles);
+  GC_CHECK_LAUNCH("conv3x3_kernel");
+  return GC_OK;
+}
+
+// Output scale of the network: s_out Dt with a base step (times rho_b =
+// rms(est) per sample), else s_out.
+float out_scale(const gc_corrector* c) {
+  return c->base ? c->s_out * static_cast<float>(c->dt_coarse) : c->s_out;
+}
+
 template <class T>
-gc_status corr_forward(gc_corrector* c, int batch, const T* in) {
-  gc_status s = corr_layout(c);
-  if (s != GC_OK) return s;
+gc_status corr_forward(gc_corrector* c, int batch, const T* in, bool train) {
+  GC_TRY(corr_layout(c));
   const int H = c->H, W = c->W;
   const size_t n = static_cast<size_t>(batch) * H * W;
   cudaStream_t st = c->ctx->stream;
-  const T* feat = nullptr;
-  if (c->feature) {
+  const int grid_ew = c->ctx->num_sms * 8;
+  if (c->base) {
     const gc_grid g{W, H, 1, 1.0, 1.0, 1.0};
-    T* fb = reinterpret_cast<T*>(c->fbuf);
+    const gc_dtype dt = sizeof(T) == 8 ? GC_F64 : GC_F32;
+    T* bb = reinterpret_cast<T*>(c->bbuf);
+    T* f0 = reinterpret_cast<T*>(c->f0buf);
+    T* fb = reinterpret_cast<T*>(c->fbbuf);
+    GC_CUDA(cudaMemcpyAsync(bb, in, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+    const size_t hw = static_cast<size_t>(H) * W;
+    void* const scratch[4] = {c->rkc, c->rkc + hw, c->rkc + 2 * hw, c->rkc + 3 * hw};
     for (int b = 0; b < batch; ++b) {
-      gc_status fs = gc_ch_rhs(c->ctx, &g, sizeof(T) == 8 ? GC_F64 : GC_F32, &c->chp, in + static_cast<size_t>(b) * H * W,
-                               fb + static_cast<size_t>(b) * H * W);
-      if (fs != GC_OK) return fs;
+      const size_t o = b * hw;
+      GC_TRY(ch_rkc_enqueue(c->ctx, &g, dt, &c->chp, bb + o, c->dt_coarse, c->stages, scratch));
+      GC_TRY(ch_rhs_enqueue(c->ctx, &g, dt, &c->chp, in + o, f0 + o));
+      GC_TRY(ch_rhs_enqueue(c->ctx, &g, dt, &c->chp, bb + o, fb + o));
     }
-    feat = fb;
+    // squares of incr into resid, of est into delta (both overwritten below)
+    base_features<T><<<grid_ew, 256, 0, st>>>(in, bb, f0, fb, static_cast<T>(1.0 / c->dt_coarse), n, c->incr,
+                                               c->est, c->resid, c->delta);
+    GC_CHECK_LAUNCH("base_features");
+    GC_TRY(sample_mean(c, batch, c->resid, H * W, c->ms));
+    GC_TRY(sample_mean(c, batch, c->delta, H * W, c->ms_est));
   }
-  pack_input<T><<<c->ctx->num_sms * 8, 256, 0, st>>>(in, feat, static_cast<float>(c->feature_dt), n, c->x[0]);
+  pack_input<T><<<grid_ew, 256, 0, st>>>(in, c->base ? c->incr : nullptr, c->ms, c->base ? c->est : nullptr,
+                                         c->ms_est, H * W, n, c->x[0]);
   GC_CHECK_LAUNCH("pack_input");
-  const int tiles_x = div_up(W, kTC), tiles_y = div_up(H, kTR);
-  const int tpi = tiles_x * tiles_y;
   for (int l = 0; l < kLayers; ++l) {
     const __nv_bfloat16* wl = c->w_fwd + static_cast<size_t>(l) * kTaps * kC * kC;
     const float* bl = c->params + static_cast<size_t>(l) * kLayerParams + kTaps * kC * kC;
+    gc_status s;
     if (l + 1 < kLayers) {
-      conv3x3_kernel<EPI_FWD, 4><<<batch * tpi, kConvThreads, 0, st>>>(c->x[l], wl, bl, c->z[l], c->x[l + 1],
-                                                                      nullptr, nullptr, H, W, tiles_x, tpi);
+      s = train ? launch_conv<EPI_FWD, 4, true>(c, batch, c->x[l], wl, bl, c->z[l], c->x[l + 1], nullptr, nullptr)
+                : launch_conv<EPI_FWD, 4, false>(c, batch, c->x[l], wl, bl, nullptr, c->x[l + 1], nullptr, nullptr);
     } else {
-      conv3x3_kernel<EPI_LAST, 1><<<batch * tpi, kConvThreads, 0, st>>>(c->x[l], wl, bl, nullptr, nullptr,
-                                                                       c->zlast, nullptr, H, W, tiles_x, tpi);
+      s = launch_conv<EPI_LAST, 1, false>(c, batch, c->x[l], wl, bl, nullptr, nullptr, c->zlast, nullptr);
     }
-    GC_CHECK_LAUNCH("conv3x3_kernel (forward)");
+    if (s != GC_OK) return s;
   }
-  sample_mean<<<batch, 256, 0, st>>>(c->zlast, H * W, c->mean);
-  project_delta<<<c->ctx->num_sms * 8, 256, 0, st>>>(c->zlast, c->mean, H * W, n, c->s_out, c->delta);
+  GC_TRY(sample_mean(c, batch, c->zlast, H * W, c->mean));
+  project_delta<<<grid_ew, 256, 0, st>>>(c->zlast, c->mean, c->base ? c->ms_est : nullptr, H * W, n, out_scale(c),
+                                         c->delta);
   GC_CHECK_LAUNCH("project_delta");
   return GC_OK;
 }
 
-// Forward + loss + backward into c->grad (no update). loss = mean((c + delta - target)^2).
-gc_status corr_backward(gc_corrector* c, int batch, const float* cin, const float* target, double* loss) {
-  gc_status s = corr_forward<float>(c, batch, cin);
-  if (s != GC_OK) return s;
+// Forward + loss + backward into c->grad (no update).
+// loss = sum_b sum_p (start + delta - target)^2 / (N den_b), N = batch H W,
+// start = B(c) with a base step else c, den_b = mean((target - start)^2)
+// of sample b with the normalised loss else 1 (so with a base step the loss
+// is the squared error left relative to the base step's own error).
+template <class T>
+gc_status corr_backward(gc_corrector* c, int batch, const T* cin, const T* target, double* loss) {
+  GC_TRY(corr_forward<T>(c, batch, cin, true));
   const int H = c->H, W = c->W, hw = H * W;
   const size_t n = static_cast<size_t>(batch) * hw;
   cudaStream_t st = c->ctx->stream;
+  const int grid_ew = c->ctx->num_sms * 8;
+  const T* start = c->base ? reinterpret_cast<const T*>(c->bbuf) : cin;
   const float* den = nullptr;
   if (c->normalized) {
-    step_sq<<<c->ctx->num_sms * 8, 256, 0, st>>>(cin, target, n, c->resid);
-    sample_mean<<<batch, 256, 0, st>>>(c->resid, hw, c->den);
+    step_sq<T><<<grid_ew, 256, 0, st>>>(start, target, n, c->resid);
+    GC_TRY(sample_mean(c, batch, c->resid, hw, c->den));
     den = c->den;
   }
-  residual_kernel<<<kRedBlocks, 256, 0, st>>>(cin, c->delta, target, n, hw, den, c->resid, c->part);
+  residual_kernel<T><<<kRedBlocks, 256, 0, st>>>(start, c->delta, target, n, hw, den, c->resid, c->part);
   GC_CHECK_LAUNCH("residual_kernel");
-  sample_mean<<<batch, 256, 0, st>>>(c->resid, hw, c->mean2);
-  const float scale = c->s_out * 2.0f / static_cast<float>(n);
+  GC_TRY(sample_mean(c, batch, c->resid, hw, c->mean2));
+  const float scale = out_scale(c) * 2.0f / static_cast<float>(n);
   __nv_bfloat16* dz = c->dz_a;
   __nv_bfloat16* dzn = c->dz_b;
-  last_layer_grad<<<c->ctx->num_sms * 8, 256, 0, st>>>(c->resid, c->mean2, hw, n, scale, den, dz);
+  last_layer_grad<<<grid_ew, 256, 0, st>>>(c->resid, c->mean2, hw, n, scale, den, c->base ? c->ms_est : nullptr, dz);
   GC_CHECK_LAUNCH("last_layer_grad");
   const int tiles_x = div_up(W, kTC), tiles_y = div_up(H, kTR);
   const int tpi = tiles_x * tiles_y;
@@ -552,9 +777,7 @@ gc_status corr_backward(gc_corrector* c, int batch, const float* cin, const floa
     GC_CHECK_LAUNCH("sum_partials");
     if (l > 0) {
       const __nv_bfloat16* wl = c->w_bwd + static_cast<size_t>(l) * kTaps * kC * kC;
-      conv3x3_kernel<EPI_BWD, 4><<<n_tiles, kConvThreads, 0, st>>>(dz, wl, nullptr, dzn, nullptr, nullptr,
-                                                                   c->z[l - 1], H, W, tiles_x, tpi);
-      GC_CHECK_LAUNCH("conv3x3_kernel (backward)");
+      GC_TRY((launch_conv<EPI_BWD, 4, true>(c, batch, dz, wl, nullptr, dzn, nullptr, nullptr, c->z[l - 1])));
       std::swap(dz, dzn);
     }
   }
@@ -567,6 +790,13 @@ gc_status corr_backward(gc_corrector* c, int batch, const float* cin, const floa
     *loss = sum / static_cast<double>(n);
   }
   return GC_OK;
+}
+
+gc_status corr_backward_any(gc_corrector* c, int batch, gc_dtype dt, const void* cin, const void* target,
+                            double* loss) {
+  if (dt == GC_F64)
+    return corr_backward<double>(c, batch, static_cast<const double*>(cin), static_cast<const double*>(target), loss);
+  return corr_backward<float>(c, batch, static_cast<const float*>(cin), static_cast<const float*>(target), loss);
 }
 
 }  // namespace
@@ -607,10 +837,20 @@ GC_API gc_status gc_corrector_create(gc_context* ctx, int32_t height, int32_t wi
   alloc(reinterpret_cast<void**>(&c->mean), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->mean2), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->cbuf), sizeof(float) * n);
-  alloc(reinterpret_cast<void**>(&c->fbuf), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&c->bbuf), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&c->f0buf), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&c->fbbuf), sizeof(double) * n);
+  alloc(reinterpret_cast<void**>(&c->incr), sizeof(float) * n);
+  alloc(reinterpret_cast<void**>(&c->est), sizeof(float) * n);
+  alloc(reinterpret_cast<void**>(&c->ms), sizeof(float) * max_batch);
+  alloc(reinterpret_cast<void**>(&c->ms_est), sizeof(float) * max_batch);
   alloc(reinterpret_cast<void**>(&c->den), sizeof(float) * max_batch);
+  alloc(reinterpret_cast<void**>(&c->mpart), sizeof(double) * kMeanParts * max_batch);
+  alloc(reinterpret_cast<void**>(&c->rkc), sizeof(double) * 4 * height * width);
+  alloc(reinterpret_cast<void**>(&c->adv), sizeof(double) * 2 * height * width);
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&c->host_part), sizeof(double) * 3 * kRedBlocks);
   alloc(reinterpret_cast<void**>(&c->tbuf), sizeof(float) * n);
-  alloc(reinterpret_cast<void**>(&c->part), sizeof(double) * 2 * kRedBlocks);
+  alloc(reinterpret_cast<void**>(&c->part), sizeof(double) * 3 * kRedBlocks);
   c->wparts = ctx->num_sms * 4;
   alloc(reinterpret_cast<void**>(&c->wpart), sizeof(float) * kLayerParams * c->wparts);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->params, 0, sizeof(float) * kParams, ctx->stream);
@@ -630,30 +870,38 @@ GC_API gc_status gc_corrector_destroy(gc_corrector* c) {
   cudaStreamSynchronize(c->ctx->stream);
   void* ptrs[] = {c->params, c->grad, c->adam_m, c->adam_v, c->w_fwd, c->w_bwd, c->dz_a, c->dz_b, c->zlast,
                   c->delta, c->resid, c->mean, c->mean2, c->cbuf, c->tbuf, c->part, c->wpart, c->adv,
-                  c->fbuf, c->den};
+                  c->bbuf, c->f0buf, c->fbbuf, c->incr, c->est, c->ms, c->ms_est, c->den, c->mpart, c->rkc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto* p : c->x)
     if (p) cudaFree(p);
   for (auto* p : c->z)
     if (p) cudaFree(p);
+  if (c->host_part) cudaFreeHost(c->host_part);
+  if (c->prop_exec) cudaGraphExecDestroy(c->prop_exec);
   delete c;
   return GC_OK;
 }
 
 GC_API int32_t gc_corrector_num_params(void) { return kParams; }
 
-GC_API gc_status gc_corrector_set_physics(gc_corrector* c, const gc_ch_params* p, double feature_dt) {
-  if (!c) return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_physics: null corrector");
+GC_API gc_status gc_corrector_set_base(gc_corrector* c, const gc_ch_params* p, double dt_coarse, int32_t stages) {
+  if (!c) return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_base: null corrector");
   if (!p) {
-    c->feature = false;
+    c->base = false;
     return GC_OK;
   }
   if (p->order != 2 && p->order != 4 && p->order != 6)
-    return fail(GC_ERR_UNSUPPORTED, "gc_corrector_set_physics: order must be 2, 4 or 6");
-  c->feature = true;
+    return fail(GC_ERR_UNSUPPORTED, "gc_corrector_set_base: order must be 2, 4 or 6");
+  if (stages < 2 || stages > 64 || !(dt_coarse > 0.0))
+    return fail(GC_ERR_INVALID_ARG, "gc_corrector_set_base: need dt_coarse > 0 and 2 <= stages <= 64");
+  const gc_grid g{c->W, c->H, 1, 1.0, 1.0, 1.0};
+  gc_status s = require_axes(&g, p->order / 2);
+  if (s != GC_OK) return s;
+  c->base = true;
   c->chp = *p;
-  c->feature_dt = feature_dt;
+  c->dt_coarse = dt_coarse;
+  c->stages = stages;
   return GC_OK;
 }
 
@@ -686,30 +934,36 @@ GC_API gc_status gc_corrector_get_params(gc_corrector* c, float* host, int32_t n
   return GC_OK;
 }
 
-// delta_out = zero-mean correction for each of `batch` fields c (fp32 or fp64, batch x H x W).
+// delta_out = the coarse-step increment for each of `batch` fields c (fp32
+// or fp64, batch x H x W): B(c) - c + delta with a base step, else delta.
 GC_API gc_status gc_corrector_forward(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
                                       float* delta_out) {
   if (!c || !cin || !delta_out) return fail(GC_ERR_INVALID_ARG, "gc_corrector_forward: null pointer");
   Call call(c->ctx);
   if (call.st != GC_OK) return call.st;
   if (batch < 1 || batch > c->max_batch) return fail(GC_ERR_INVALID_ARG, "gc_corrector_forward: batch out of range");
-  gc_status s = dt == GC_F64 ? corr_forward<double>(c, batch, static_cast<const double*>(cin))
-                             : corr_forward<float>(c, batch, static_cast<const float*>(cin));
+  gc_status s = dt == GC_F64 ? corr_forward<double>(c, batch, static_cast<const double*>(cin), false)
+                             : corr_forward<float>(c, batch, static_cast<const float*>(cin), false);
   if (s != GC_OK) return s;
-  GC_CUDA(cudaMemcpyAsync(delta_out, c->delta, sizeof(float) * batch * c->H * c->W, cudaMemcpyDeviceToDevice,
-                          c->ctx->stream));
+  const size_t n = static_cast<size_t>(batch) * c->H * c->W;
+  if (c->base) {
+    add_increment<<<c->ctx->num_sms * 8, 256, 0, c->ctx->stream>>>(c->incr, c->delta, n, delta_out);
+    GC_CHECK_LAUNCH("add_increment");
+  } else {
+    GC_CUDA(cudaMemcpyAsync(delta_out, c->delta, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->ctx->stream));
+  }
   return GC_OK;
 }
 
-// Gradient of the loss mean((c + delta(c) - target)^2) into grad_host
-// (kParams floats), without updating the parameters.
-GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, const float* cin, const float* target,
-                                       float* grad_host, double* loss) {
+// Gradient of the training loss (corr_backward) into grad_host (kParams
+// floats), without updating the parameters.
+GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
+                                       const void* target, float* grad_host, double* loss) {
   if (!c || !cin || !target) return fail(GC_ERR_INVALID_ARG, "gc_corrector_gradient: null pointer");
   Call call(c->ctx);
   if (call.st != GC_OK) return call.st;
   if (batch < 1 || batch > c->max_batch) return fail(GC_ERR_INVALID_ARG, "gc_corrector_gradient: batch out of range");
-  gc_status s = corr_backward(c, batch, cin, target, loss);
+  gc_status s = corr_backward_any(c, batch, dt, cin, target, loss);
   if (s != GC_OK) return s;
   if (grad_host) {
     GC_CUDA(cudaMemcpyAsync(grad_host, c->grad, sizeof(float) * kParams, cudaMemcpyDeviceToHost, c->ctx->stream));
@@ -718,14 +972,14 @@ GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, const flo
   return GC_OK;
 }
 
-// One Adam step on the loss above (fp32 inputs and targets on the device).
-GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, const float* cin, const float* target,
-                                         float lr, double* loss) {
+// One Adam step on the training loss (inputs and targets on the device).
+GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
+                                         const void* target, float lr, double* loss) {
   if (!c || !cin || !target) return fail(GC_ERR_INVALID_ARG, "gc_corrector_train_step: null pointer");
   Call call(c->ctx);
   if (call.st != GC_OK) return call.st;
   if (batch < 1 || batch > c->max_batch) return fail(GC_ERR_INVALID_ARG, "gc_corrector_train_step: batch out of range");
-  gc_status s = corr_backward(c, batch, cin, target, loss);
+  gc_status s = corr_backward_any(c, batch, dt, cin, target, loss);
   if (s != GC_OK) return s;
   ++c->adam_t;
   const float b1 = 0.9f, b2 = 0.999f;
@@ -739,11 +993,14 @@ GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, const f
 }
 
 // Advances one 2-D double field by n_coarse coarse steps of
-// dt_fine * fine_per_coarse.  Each coarse step proposes c + delta(c) and
-// accepts it when the free energy does not rise by more than energy_tol and
-// the trapezoid residual |(c1 - c0)/Dt - (f(c0) + f(c1))/2| / |(f(c0) + f(c1))/2|
-// is at most residual_tol; otherwise the step is taken by fine_per_coarse
-// plain RK4 steps.
+// dt_fine * fine_per_coarse.  Each coarse step proposes B(c) + delta(c)
+// (c + delta(c) without a base step) and accepts it when the free energy
+// does not rise by more than energy_tol and the trapezoid residual
+// |(c1 - c0)/Dt - (f(c0) + f(c1))/2| / |(f(c0) + f(c1))/2| is at most
+// residual_tol; otherwise the step is taken by fine_per_coarse plain RK4
+// steps.  The proposal (base step, network, candidate, acceptance
+// statistics) is one captured CUDA graph; the host reads the statistics
+// back once per coarse step to decide.
 GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const gc_ch_params* cp, double* psi,
                                       int32_t n_coarse, const gc_corrector_policy* pol,
                                       gc_corrector_stats* stats) {
@@ -754,64 +1011,114 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
     return fail(GC_ERR_GRID_MISMATCH, "gc_corrector_advance: grid must be 2-D and match the corrector's size");
   if (n_coarse < 0 || pol->fine_per_coarse < 1 || !(pol->dt_fine > 0.0))
     return fail(GC_ERR_INVALID_ARG, "gc_corrector_advance: bad policy or step count");
-  gc_context* ctx = c->ctx;
-  const size_t n = static_cast<size_t>(c->H) * c->W;
-  if (!c->adv) GC_CUDA(cudaMalloc(&c->adv, sizeof(double) * 3 * n));
-  double* cand = c->adv;
-  double* f0 = c->adv + n;
-  double* f1 = c->adv + 2 * n;
-  const double dt_coarse = pol->dt_fine * pol->fine_per_coarse;
-  gc_integrand fe{GC_INTEGRAND_CH_FREE_ENERGY, cp->kappa};
-  double F0 = 0.0;
-  gc_status s = gc_evaluate(ctx, g, GC_F64, psi, &fe, GC_SUM_PAIRWISE, &F0);
+  if (cp->order != 2 && cp->order != 4 && cp->order != 6)
+    return fail(GC_ERR_UNSUPPORTED, "gc_corrector_advance: order must be 2, 4 or 6");
+  gc_status s = require_axes(g, cp->order / 2);
   if (s != GC_OK) return s;
-  bool f0_valid = false;
-  gc_corrector_stats st{};
-  std::vector<double> part(2 * kRedBlocks);
-  for (int k = 0; k < n_coarse; ++k) {
-    if ((s = corr_forward<double>(c, 1, psi)) != GC_OK) return s;
-    apply_delta<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(psi, c->delta, n, cand);
+  if (c->base && (g->hx != 1.0 || g->hy != 1.0))
+    return fail(GC_ERR_INVALID_ARG, "gc_corrector_advance: the base step works on unit cell spacing");
+  gc_context* ctx = c->ctx;
+  cudaStream_t st = ctx->stream;
+  const size_t n = static_cast<size_t>(c->H) * c->W;
+  double* cand = c->adv;
+  double* f1 = c->adv + n;
+  const double dt_coarse = pol->dt_fine * pol->fine_per_coarse;
+  const double inv_2hx = 0.5 / g->hx, inv_2hy = 0.5 / g->hy, area = g->hx * g->hy;
+
+  // Acceptance statistics of c1 (and of the step c0 -> c1 when c0 != null)
+  // into c->part.
+  auto stats_enqueue = [&](const double* c0, const double* c1) -> gc_status {
+    accept_stats<<<kRedBlocks, 256, 0, st>>>(c0, c1, c->f0buf, f1, c->W, c->H, inv_2hx, inv_2hy, area, cp->kappa,
+                                              1.0 / dt_coarse, c->part);
+    GC_CHECK_LAUNCH("accept_stats");
+    return GC_OK;
+  };
+  double sums[3];
+  auto read_stats = [&]() -> gc_status {
+    GC_CUDA(cudaMemcpyAsync(c->host_part, c->part, sizeof(double) * 3 * kRedBlocks, cudaMemcpyDeviceToHost, st));
+    GC_CUDA(cudaStreamSynchronize(st));
+    sums[0] = sums[1] = sums[2] = 0.0;
+    for (int b = 0; b < kRedBlocks; ++b)
+      for (int q = 0; q < 3; ++q) sums[q] += c->host_part[3 * b + q];
+    return GC_OK;
+  };
+  // One proposal: cand = B(psi) + delta(psi), f1 = f(cand), statistics.
+  // The forward pass with a base step leaves f(psi) in f0buf (with chp;
+  // it is recomputed with cp when the two differ or without a base step).
+  const bool same_rhs = c->base && c->chp.order == cp->order && c->chp.mobility == cp->mobility &&
+                        c->chp.kappa == cp->kappa;
+  auto propose = [&]() -> gc_status {
+    GC_TRY(corr_forward<double>(c, 1, psi, false));
+    apply_delta<<<ctx->num_sms * 8, 256, 0, st>>>(c->base ? c->bbuf : psi, c->delta, n, cand);
     GC_CHECK_LAUNCH("apply_delta");
-    double F1 = 0.0;
-    if ((s = gc_evaluate(ctx, g, GC_F64, cand, &fe, GC_SUM_PAIRWISE, &F1)) != GC_OK) return s;
-    bool accept = F1 <= F0 + pol->energy_tol;
-    double res = 0.0;
-    if (accept) {
-      if (!f0_valid && (s = gc_ch_rhs(ctx, g, GC_F64, cp, psi, f0)) != GC_OK) return s;
-      if ((s = gc_ch_rhs(ctx, g, GC_F64, cp, cand, f1)) != GC_OK) return s;
-      trapezoid_residual<<<kRedBlocks, 256, 0, ctx->stream>>>(psi, cand, f0, f1, n, 1.0 / dt_coarse,
-                                                              reinterpret_cast<double*>(c->part));
-      GC_CHECK_LAUNCH("trapezoid_residual");
-      GC_CUDA(cudaMemcpyAsync(part.data(), c->part, sizeof(double) * 2 * kRedBlocks, cudaMemcpyDeviceToHost,
-                              ctx->stream));
-      GC_CUDA(cudaStreamSynchronize(ctx->stream));
-      double sr = 0.0, sf = 0.0;
-      for (int b = 0; b < kRedBlocks; ++b) {
-        sr += part[2 * b];
-        sf += part[2 * b + 1];
+    if (!same_rhs) GC_TRY(ch_rhs_enqueue(ctx, g, GC_F64, cp, psi, c->f0buf));
+    GC_TRY(ch_rhs_enqueue(ctx, g, GC_F64, cp, cand, f1));
+    return stats_enqueue(psi, cand);
+  };
+  const uint64_t key[8] = {reinterpret_cast<uint64_t>(psi), bits_of(dt_coarse), bits_of(cp->mobility),
+                           bits_of(cp->kappa),
+                           (static_cast<uint64_t>(cp->order) << 32) ^ static_cast<uint64_t>(c->stages) ^
+                               (c->base ? 1ULL << 40 : 0),
+                           bits_of(c->dt_coarse) ^ bits_of(c->chp.kappa) * 3 ^ bits_of(c->chp.mobility) * 5 ^
+                               static_cast<uint64_t>(c->chp.order) << 56,
+                           bits_of(static_cast<double>(c->s_out)) ^ bits_of(g->hx) * 7, bits_of(g->hy)};
+
+  GC_TRY(stats_enqueue(nullptr, psi));
+  GC_TRY(read_stats());
+  double F0 = sums[0];
+  gc_corrector_stats sres{};
+  for (int k = 0; k < n_coarse; ++k) {
+    GC_TRY(corr_layout(c));
+    if (c->prop_exec && std::memcmp(key, c->prop_key, sizeof(key)) == 0) {
+      GC_CUDA(cudaGraphLaunch(c->prop_exec, st));
+    } else {
+      // Run this proposal directly (which also sets up every lazily
+      // initialised kernel attribute), then capture the sequence for the
+      // following steps.
+      GC_TRY(propose());
+      if (c->prop_exec) {
+        cudaGraphExecDestroy(c->prop_exec);
+        c->prop_exec = nullptr;
       }
-      res = sf > 0.0 ? std::sqrt(sr / sf) : 0.0;
-      accept = res <= pol->residual_tol;
+      cudaGraph_t graph = nullptr;
+      GC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      const gc_status cs = propose();
+      const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+      if (cs != GC_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return cs;
+      }
+      if (ce != cudaSuccess) return cuda_fail(ce, "gc_corrector_advance: capture");
+      const cudaError_t ie = cudaGraphInstantiate(&c->prop_exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        c->prop_exec = nullptr;
+        return cuda_fail(ie, "gc_corrector_advance: graph instantiation");
+      }
+      std::memcpy(c->prop_key, key, sizeof(key));
     }
-    st.last_residual = res;
+    GC_TRY(read_stats());
+    const double F1 = sums[0];
+    const double res = sums[2] > 0.0 ? std::sqrt(sums[1] / sums[2]) : 0.0;
+    const bool accept = F1 <= F0 + pol->energy_tol && res <= pol->residual_tol;
+    sres.last_residual = res;
     if (accept) {
-      GC_CUDA(cudaMemcpyAsync(psi, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-      std::swap(f0, f1);  // f(psi) of the new state is known
-      f0_valid = true;
+      GC_CUDA(cudaMemcpyAsync(psi, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       F0 = F1;
-      ++st.accepted;
+      ++sres.accepted;
     } else {
       if ((s = gc_ch_integrate(ctx, g, GC_F64, cp, psi, pol->dt_fine, pol->fine_per_coarse, GC_RK4)) != GC_OK)
         return s;
-      if ((s = gc_evaluate(ctx, g, GC_F64, psi, &fe, GC_SUM_PAIRWISE, &F0)) != GC_OK) return s;
-      f0_valid = false;
-      ++st.fallbacks;
+      GC_TRY(stats_enqueue(nullptr, psi));
+      GC_TRY(read_stats());
+      F0 = sums[0];
+      ++sres.fallbacks;
     }
   }
   if (stats) {
-    stats->accepted += st.accepted;
-    stats->fallbacks += st.fallbacks;
-    stats->last_residual = st.last_residual;
+    stats->accepted += sres.accepted;
+    stats->fallbacks += sres.fallbacks;
+    stats->last_residual = sres.last_residual;
   }
   return GC_OK;
 }

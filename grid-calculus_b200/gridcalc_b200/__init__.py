@@ -491,11 +491,11 @@ for _name, _args in {
     "gc_corrector_destroy": [_vp],
     "gc_corrector_set_params": [_vp, C.POINTER(C.c_float), C.c_int32, C.c_float],
     "gc_corrector_get_params": [_vp, C.POINTER(C.c_float), C.c_int32],
-    "gc_corrector_set_physics": [_vp, C.c_void_p, C.c_double],
+    "gc_corrector_set_base": [_vp, C.c_void_p, C.c_double, C.c_int32],
     "gc_corrector_set_loss": [_vp, C.c_int32],
     "gc_corrector_forward": [_vp, C.c_int32, _i32, _vp, _vp],
-    "gc_corrector_gradient": [_vp, C.c_int32, _vp, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)],
-    "gc_corrector_train_step": [_vp, C.c_int32, _vp, _vp, C.c_float, C.POINTER(C.c_double)],
+    "gc_corrector_gradient": [_vp, C.c_int32, _i32, _vp, _vp, C.POINTER(C.c_float), C.POINTER(C.c_double)],
+    "gc_corrector_train_step": [_vp, C.c_int32, _i32, _vp, _vp, C.c_float, C.POINTER(C.c_double)],
     "gc_corrector_advance": [_vp, _gp, C.POINTER(gc_ch_params), _vp, C.c_int32,
                              C.POINTER(gc_corrector_policy), C.POINTER(gc_corrector_stats)],
 }.items():
@@ -511,7 +511,7 @@ CORRECTOR_LAYERS, CORRECTOR_CHANNELS = 6, 32
 def corrector_init_params(seed: int = 0, last_scale: float = 0.1, inputs: int = 1):
     """He-normal initial parameters (FP32) for the corrector: per layer
     W[9][32 in][32 out] then b[32]; the first layer sees `inputs` input
-    channels (1: c; 2: c and the right-hand-side feature)."""
+    channels (1: c alone; 3: c and the two base-step features)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     n_c = CORRECTOR_CHANNELS
@@ -555,18 +555,21 @@ class Corrector:
         _check(lib.gc_corrector_get_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
         return p
 
-    def set_physics(self, rhs: "CahnHilliardRhs | None", feature_dt: float = 0.16) -> None:
-        """Feeds feature_dt * f(c) (f the Cahn-Hilliard RHS) as the second
-        input channel; None turns the feature off."""
-        _check(lib.gc_corrector_set_physics(self.handle, C.byref(rhs.c()) if rhs is not None else None,
-                                            feature_dt))
+    def set_base(self, rhs: "CahnHilliardRhs | None", dt_coarse: float = 0.16, stages: int = 6) -> None:
+        """Coarse step B(c) + delta over one RKC2 step B of dt_coarse with
+        `stages` stages (the network sees B's increment and error indicator);
+        None turns the base step off (coarse step c + delta)."""
+        _check(lib.gc_corrector_set_base(self.handle, C.byref(rhs.c()) if rhs is not None else None,
+                                         dt_coarse, stages))
 
     def set_loss(self, normalized: bool) -> None:
-        """normalized: weight each training sample by 1 / mean((target - c)^2)."""
+        """normalized: weight each training sample by 1 / mean((target - s)^2),
+        s = B(c) with a base step else c."""
         _check(lib.gc_corrector_set_loss(self.handle, 1 if normalized else 0))
 
     def forward(self, c):
-        """Zero-mean correction for a (B, H, W) float32/float64 CUDA tensor."""
+        """Coarse-step increment (B(c) - c + delta with a base step, else the
+        zero-mean correction delta) for a (B, H, W) float32/float64 CUDA tensor."""
         import torch
         c = c.contiguous()
         out = torch.empty(c.shape, dtype=torch.float32, device=c.device)
@@ -574,17 +577,22 @@ class Corrector:
         return out
 
     def gradient(self, c, target):
+        """(gradient, loss) for (B, H, W) CUDA tensors c, target of one dtype."""
         import numpy as np
+        if c.dtype != target.dtype:
+            raise ValueError("gridcalc_b200: c and target must share a dtype")
         g = np.empty(self.n_params, dtype=np.float32)
         loss = C.c_double()
-        _check(lib.gc_corrector_gradient(self.handle, c.shape[0], c.contiguous().data_ptr(),
+        _check(lib.gc_corrector_gradient(self.handle, c.shape[0], _dtype_code(c), c.contiguous().data_ptr(),
                                          target.contiguous().data_ptr(),
                                          g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
         return g, loss.value
 
     def train_step(self, c, target, lr: float) -> float:
+        if c.dtype != target.dtype:
+            raise ValueError("gridcalc_b200: c and target must share a dtype")
         loss = C.c_double()
-        _check(lib.gc_corrector_train_step(self.handle, c.shape[0], c.contiguous().data_ptr(),
+        _check(lib.gc_corrector_train_step(self.handle, c.shape[0], _dtype_code(c), c.contiguous().data_ptr(),
                                            target.contiguous().data_ptr(), lr, C.byref(loss)))
         return loss.value
 

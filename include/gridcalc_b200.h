@@ -248,14 +248,17 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
                                       char* report, size_t report_len);
 
 /* ---- learned coarse-step corrector ---------------------------------------
- * No reference counterpart.  A 6-layer periodic 3x3 CNN (32 channels, GELU,
- * BF16 weights and activations, FP32 accumulation on the tensor cores)
- * maps a 2-D Cahn-Hilliard field c (and optionally its right-hand side, see
- * gc_corrector_set_physics) to a zero-mean correction delta so that
- * c + delta approximates fine_per_coarse plain RK4 steps.  Parameters are
- * FP32 masters, per layer W[9 taps][32 in][32 out] then b[32], tap t at
- * offset (t / 3 - 1, t % 3 - 1) in (y, x); delta = s_out (z6 - mean z6)
- * with z6 the last layer's channel 0. */
+ * No reference counterpart.  A 6-layer periodic 3x3 CNN (32 channels, GELU
+ * in tanh form, BF16 weights and activations, FP32 accumulation on the
+ * tensor cores) maps a 2-D Cahn-Hilliard field c to a zero-mean correction
+ * delta so that the coarse step -- c + delta, or B(c) + delta over a base
+ * step B (see gc_corrector_set_base) -- approximates fine_per_coarse plain
+ * RK4 steps.  Parameters are FP32 masters, per layer W[9 taps][32 in][32 out]
+ * then b[32], tap t at offset (t / 3 - 1, t % 3 - 1) in (y, x).  Input
+ * channels: c, u = (B(c) - c) / rms and e = est / rms with est = (B(c) - c)
+ * / Dt - (f(c) + f(B(c))) / 2 (u = e = 0 without a base step);
+ * delta = s_out rho (z6 - mean z6), z6 the last layer's channel 0, rho =
+ * Dt rms(est) per sample (1 without a base step). */
 typedef struct gc_corrector gc_corrector;
 
 typedef struct gc_corrector_policy {
@@ -276,24 +279,31 @@ GC_API gc_status gc_corrector_create(gc_context* ctx, int32_t height, int32_t wi
 GC_API gc_status gc_corrector_destroy(gc_corrector* c);
 GC_API int32_t gc_corrector_num_params(void);
 GC_API gc_status gc_corrector_set_params(gc_corrector* c, const float* host, int32_t n, float s_out);
-/* Second input channel feature_dt * f(c), f the Cahn-Hilliard RHS with p
- * (computed by gc_ch_rhs); NULL p turns it off (channel 1 = 0). */
-GC_API gc_status gc_corrector_set_physics(gc_corrector* c, const gc_ch_params* p, double feature_dt);
+/* Base step: one gc_ch_rkc step of dt_coarse with `stages` stages and the
+ * RHS p on unit cell spacing.  With it, the coarse step is B(c) + delta and
+ * the network also sees the base step's increment and error indicator;
+ * NULL p turns it off (coarse step c + delta). */
+GC_API gc_status gc_corrector_set_base(gc_corrector* c, const gc_ch_params* p, double dt_coarse, int32_t stages);
 /* normalized != 0: the training loss weights each sample by 1 / mean((target
- * - c)^2), so that small (late-time) steps count as much as large ones. */
+ * - s)^2), s = B(c) with a base step else c, so that small (late-time) steps
+ * count as much as large ones. */
 GC_API gc_status gc_corrector_set_loss(gc_corrector* c, int32_t normalized);
 GC_API gc_status gc_corrector_get_params(gc_corrector* c, float* host, int32_t n);
-/* delta for `batch` fields (batch x height x width, dtype F32 or F64) into
+/* The coarse-step increment (B(c) - c + delta, or delta without a base
+ * step) for `batch` fields (batch x height x width, dtype F32 or F64) into
  * delta_out (device, float). */
 GC_API gc_status gc_corrector_forward(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
                                       float* delta_out);
-/* Gradient of mean((c + delta(c) - target)^2) w.r.t. all parameters
- * (host, num_params floats); parameters unchanged. */
-GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, const float* cin, const float* target,
-                                       float* grad_host, double* loss);
+/* Gradient w.r.t. all parameters (host, num_params floats; parameters
+ * unchanged) of the loss sum_b sum_p (s_b + delta_b - target_b)^2 / (N den_b):
+ * s = B(c) with a base step else c, N = batch x height x width, den_b =
+ * mean((target_b - s_b)^2) with the normalised loss else 1.  cin and target
+ * are device fields of dtype dt. */
+GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
+                                       const void* target, float* grad_host, double* loss);
 /* One Adam step (beta 0.9 / 0.999) on that loss. */
-GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, const float* cin, const float* target,
-                                         float lr, double* loss);
+GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
+                                         const void* target, float lr, double* loss);
 /* Learned coarse steps on one double field with the plain-RK4 fallback. */
 GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const gc_ch_params* cp, double* psi,
                                       int32_t n_coarse, const gc_corrector_policy* pol,

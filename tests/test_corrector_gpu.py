@@ -69,35 +69,61 @@ def test_gradient_matches_cpu_network(gc):
     net.close()
 
 
-def test_rhs_feature_and_normalized_loss_match_cpu_network(gc):
-    """Second input channel feature_dt * f(c) (f from the library's CH RHS)
-    and the per-sample normalised loss, against the float64 network fed the
-    same feature."""
+def _base_features(gc, c, dt, stages=6):
+    """B(c), [u, e] and rho: u = (B - c)/rms, e = est/rms, rho = rms(est),
+    est = (B - c)/dt - (f(c) + f(B))/2, from the library's own RKC2 step and
+    RHS (FP64)."""
     import torch
-    params = gc.corrector_init_params(seed=6, last_scale=1.0, inputs=2)
-    rng = np.random.default_rng(8)
-    h, w, fdt = 32, 40, 0.16
-    c = rng.uniform(-1, 1, (2, h, w)).astype(np.float32)
-    target = (c + np.array([0.05, 0.005])[:, None, None] * rng.standard_normal(c.shape)).astype(np.float32)
+    h, w = c.shape[1:]
+    g = gc.Grid(w, h, 1)
     rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
     ct = torch.from_numpy(c).cuda()
-    feat = torch.stack([gc.ch_rhs(ct[b], gc.Grid(w, h, 1), rhs) for b in range(2)]).reshape(2, h, w).double().cpu().numpy() * fdt
+    base = ct.clone()
+    est = torch.empty_like(ct)
+    for b in range(c.shape[0]):
+        gc.ch_rkc(base[b], g, rhs, dt, 1, stages)
+        est[b] = (base[b] - ct[b]) / dt - 0.5 * (gc.ch_rhs(ct[b], g, rhs)[0] + gc.ch_rhs(base[b], g, rhs)[0])
+    base, est = base.cpu().numpy(), est.cpu().numpy()
+    incr = base - c
+    sigma = np.sqrt((incr ** 2).mean(axis=(1, 2)))
+    rho = np.sqrt((est ** 2).mean(axis=(1, 2)))
+    return base, [incr / sigma[:, None, None], est / rho[:, None, None]], rho
+
+
+def test_base_step_and_normalized_loss_match_cpu_network(gc):
+    """With an RKC2 base step B: input channels (B(c) - c) and the base step's
+    trapezoid residual est, each at unit RMS; output scaled by Dt rms(est);
+    coarse step B(c) + delta; loss normalised by the base step's error.
+    Against the float64 network fed the same features (B and f from the
+    library's gc_ch_rkc and gc_ch_rhs, bit-identical to their CPU
+    restatements)."""
+    import torch
+    params = gc.corrector_init_params(seed=6, last_scale=1.0, inputs=3)
+    rng = np.random.default_rng(8)
+    h, w, dtc = 32, 40, 0.16
+    c = rng.uniform(-1, 1, (2, h, w))
+    base, feats, rho = _base_features(gc, c, dtc)
     net = gc.Corrector(h, w, max_batch=2)
-    net.set_params(params, s_out=0.05)
-    net.set_physics(rhs, fdt)
-    got = net.forward(ct).double().cpu().numpy()
-    want = corrector_ref.delta(params, c, 0.05, feat)
+    net.set_params(params, s_out=0.5)
+    net.set_base(gc.CahnHilliardRhs(1.0, 1.0, 2), dtc, 6)
+    ct = torch.from_numpy(c).cuda()
+    got = net.forward(ct).double().cpu().numpy() - (base - c)          # the network's part
+    want = corrector_ref.delta(params, c, 0.5, feats, dtc * rho)
     assert np.linalg.norm(got - want) / np.linalg.norm(want) < 3e-2
-    without = corrector_ref.delta(params, c, 0.05)
-    assert np.linalg.norm(without - want) > 0.1 * np.linalg.norm(want)   # the feature matters
+    assert np.abs(got.mean(axis=(1, 2))).max() < 1e-5 * np.abs(want).max()
+    no_feat = corrector_ref.delta(params, c, 0.5, (), dtc * rho)
+    assert np.linalg.norm(no_feat - want) > 0.1 * np.linalg.norm(want)   # the features matter
+    target = base + 0.3 * dtc * rho[:, None, None] * rng.standard_normal(c.shape)
     net.set_loss(True)
     g_gpu, loss_gpu = net.gradient(ct, torch.from_numpy(target).cuda())
-    loss_cpu, g_cpu = corrector_ref.loss_and_grad(params, c, target, 0.05, feat, normalized=True)
+    loss_cpu, g_cpu = corrector_ref.loss_and_grad(params, c, target, 0.5, feats, dtc * rho, start=base,
+                                                  normalized=True)
     assert abs(loss_gpu - loss_cpu) / loss_cpu < 1e-2, (loss_gpu, loss_cpu)
     cos = float(g_gpu @ g_cpu / (np.linalg.norm(g_gpu) * np.linalg.norm(g_cpu)))
     assert np.linalg.norm(g_gpu - g_cpu) / np.linalg.norm(g_cpu) < 6e-2 and cos > 0.995, cos
-    net.set_physics(None)
+    net.set_base(None)
     got_off = net.forward(ct).double().cpu().numpy()
+    without = corrector_ref.delta(params, c, 0.5)
     assert np.linalg.norm(got_off - without) / np.linalg.norm(without) < 3e-2
     net.close()
 
