@@ -174,6 +174,33 @@ GC_API gc_status gc_context_destroy(gc_context* ctx) {
   return GC_OK;
 }
 
+namespace {
+// Waits on a device flag that nothing sets, for at most `budget` clock
+// cycles, then records GC_ERR_TIMEOUT in the status word and returns: the
+// same bounded-wait path the TMA pipeline takes when a tile never arrives.
+__global__ void bounded_wait_selftest(const volatile int* flag, long long budget, int* status) {
+  const long long t0 = clock64();
+  while (*flag == 0) {
+    if (clock64() - t0 > budget) {
+      atomicExch(status, static_cast<int>(GC_ERR_TIMEOUT));
+      return;
+    }
+  }
+}
+}  // namespace
+
+GC_API gc_status gc_selftest_bounded_wait(gc_context* ctx, int64_t budget_cycles) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if (budget_cycles < 0 || budget_cycles > 4000000000LL)
+    return fail(GC_ERR_INVALID_ARG, "gc_selftest_bounded_wait: budget must be in [0, 4e9] cycles");
+  // ints 32..63 of the 256-byte status block are never written after creation
+  bounded_wait_selftest<<<1, 1, 0, ctx->stream>>>(ctx->device_status + 32, budget_cycles, ctx->device_status);
+  GC_CHECK_LAUNCH("bounded_wait_selftest");
+  return GC_OK;
+}
+
 GC_API gc_status gc_synchronize(gc_context* ctx) {
   Call call(ctx);
   gc_status s = call.st;

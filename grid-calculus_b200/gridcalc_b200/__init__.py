@@ -64,6 +64,7 @@ _SIGS = {
     "gc_context_create": [C.POINTER(C.c_void_p), _i32, _vp],
     "gc_context_destroy": [_vp],
     "gc_synchronize": [_vp],
+    "gc_selftest_bounded_wait": [_vp, C.c_int64],
     "gc_malloc": [_vp, C.c_size_t, C.POINTER(C.c_void_p)],
     "gc_free": [_vp, _vp],
     "gc_memcpy_h2d": [_vp, _vp, _vp, C.c_size_t],

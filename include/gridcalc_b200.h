@@ -87,6 +87,12 @@ typedef struct gc_context gc_context;
 GC_API gc_status gc_context_create(gc_context** out, int device, void* stream);
 GC_API gc_status gc_context_destroy(gc_context* ctx);
 GC_API gc_status gc_synchronize(gc_context* ctx);
+/* Failure-detection self-test (no reference counterpart): launches one
+ * thread that waits on a device flag nothing sets, gives up after
+ * budget_cycles (at most 4e9, about 2 s) and records GC_ERR_TIMEOUT exactly
+ * as a bounded TMA wait does; the next gc_synchronize reports it and clears
+ * it, and the context stays usable. */
+GC_API gc_status gc_selftest_bounded_wait(gc_context* ctx, int64_t budget_cycles);
 GC_API const char* gc_last_error(void);
 GC_API const char* gc_status_string(gc_status s);
 /* gridcalc::version() (include/gridcalc/version.hpp.in:16-18). */
