@@ -174,7 +174,7 @@ GC_API gc_status gc_context_destroy(gc_context* ctx) {
   return GC_OK;
 }
 
-namespace {
+namespace gcb {
 // Waits on a device flag that nothing sets, for at most `budget` clock
 // cycles, then records GC_ERR_TIMEOUT in the status word and returns: the
 // same bounded-wait path the TMA pipeline takes when a tile never arrives.
@@ -187,7 +187,7 @@ __global__ void bounded_wait_selftest(const volatile int* flag, long long budget
     }
   }
 }
-}  // namespace
+}  // namespace gcb
 
 GC_API gc_status gc_selftest_bounded_wait(gc_context* ctx, int64_t budget_cycles) {
   Call call(ctx);
@@ -196,7 +196,7 @@ GC_API gc_status gc_selftest_bounded_wait(gc_context* ctx, int64_t budget_cycles
   if (budget_cycles < 0 || budget_cycles > 4000000000LL)
     return fail(GC_ERR_INVALID_ARG, "gc_selftest_bounded_wait: budget must be in [0, 4e9] cycles");
   // ints 32..63 of the 256-byte status block are never written after creation
-  bounded_wait_selftest<<<1, 1, 0, ctx->stream>>>(ctx->device_status + 32, budget_cycles, ctx->device_status);
+  gcb::bounded_wait_selftest<<<1, 1, 0, ctx->stream>>>(ctx->device_status + 32, budget_cycles, ctx->device_status);
   GC_CHECK_LAUNCH("bounded_wait_selftest");
   return GC_OK;
 }
