@@ -444,8 +444,41 @@ gc_status launch_pipe(gc_context* ctx, const StageParams<T>& p) {
   return GC_OK;
 }
 
+// Two-column float variant (even grid widths): 64 x 4 threads over a
+// 128-column mu region.
+constexpr int kX2T = 64;
+
+template <int ORDER, int MODE>
+__global__ void __launch_bounds__(kX2T * kT2TY) ch_pipe_x2_kernel(const StageParams<float> p, int tiles_x,
+                                                                  int n_tiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int TX = 2 * kX2T - 2 * W<2, ORDER>::R;
+  const GridSource<float> src{p, tiles_x, n_tiles, TX, kT2Y};
+  pipelined_tiles_x2<ORDER, MODE, kX2T, kT2Y, kT2TY>(src, smem_raw);
+}
+
+template <int ORDER, int MODE>
+gc_status launch_pipe_x2(gc_context* ctx, const StageParams<float>& p) {
+  constexpr int TX = 2 * kX2T - 2 * W<2, ORDER>::R;
+  constexpr size_t smem = pipe_smem_x2<ORDER, kX2T, kT2Y>();
+  auto kern = ch_pipe_x2_kernel<ORDER, MODE>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kX2T * kT2TY, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int tiles_x = div_up(p.nx, TX), tiles_y = div_up(p.ny, kT2Y);
+  const int n_tiles = tiles_x * tiles_y;
+  const int grid = std::max(1, std::min(n_tiles, per_sm * ctx->num_sms));
+  kern<<<grid, dim3(kX2T, kT2TY), smem, ctx->stream>>>(p, tiles_x, n_tiles);
+  GC_CHECK_LAUNCH("ch_pipe_x2_kernel");
+  return GC_OK;
+}
+
 // 2-D dispatch: TMA pipeline for double when its rules hold, the
-// cp.async-pipelined persistent loop otherwise.
+// cp.async-pipelined persistent loop otherwise (two columns per thread for
+// float on even widths).
 template <class T, int ORDER, int MODE>
 gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
   if constexpr (sizeof(T) == 8 && MODE != MODE_RKC_FIRST && MODE != MODE_RKC) {
@@ -458,6 +491,9 @@ gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
       s = launch_tma<T, ORDER, MODE, false>(ctx, p);
     }
     if (s != GC_ERR_UNSUPPORTED) return s;
+  }
+  if constexpr (sizeof(T) == 4) {
+    if (p.nx % 2 == 0) return launch_pipe_x2<ORDER, MODE>(ctx, p);
   }
   return launch_pipe<T, ORDER, MODE>(ctx, p);
 }

@@ -45,8 +45,8 @@ struct BatchBuffers {
   T* k3;
 };
 
-// Tile-shape candidates: mu-region width (threads in x), output rows,
-// thread rows.
+// Tile-shape candidates: threads in x (the mu-region width, doubled for the
+// two-column float tiles), output rows, thread rows.
 struct TileShape {
   int tw, ty, nty;
 };
@@ -116,6 +116,17 @@ __global__ void __launch_bounds__(TW * NTY) ch_batch_kernel(const Member<T>* __r
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const BatchSource<T> src{members, items, n_items, buf, stage};
   pipelined_tiles<T, ORDER, MODE, TW, TY, NTY>(src, smem_raw);
+}
+
+// Float ensembles whose members all have even widths: two columns per
+// thread (TW threads cover 2 TW columns).
+template <int ORDER, int MODE, int TW, int TY, int NTY>
+__global__ void __launch_bounds__(TW * NTY) ch_batch_x2_kernel(const Member<float>* __restrict__ members,
+                                                               const int4* __restrict__ items, int n_items,
+                                                               const BatchBuffers<float> buf, int stage) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const BatchSource<float> src{members, items, n_items, buf, stage};
+  pipelined_tiles_x2<ORDER, MODE, TW, TY, NTY>(src, smem_raw);
 }
 
 // ---- per-member FP64 diagnostics -----------------------------------------
@@ -224,6 +235,7 @@ struct gc_ch_batch {
   void* items = nullptr;           // int4 work list for the current shape
   int n_items = 0;
   int shape = 2;                   // index into kShapes
+  bool x2 = false;                 // float with all widths even: two-column tiles
   int items_shape = -1;
   void* diag_items = nullptr;
   int n_diag_items = 0;
@@ -236,8 +248,28 @@ struct gc_ch_batch {
 namespace gcb {
 namespace {
 
+template <int ORDER, int MODE, int TW, int TY, int NTY>
+gc_status launch_batch_shape_x2(gc_ch_batch* b, const BatchBuffers<float>& buf, int stage) {
+  constexpr size_t smem = pipe_smem_x2<ORDER, TW, TY>();
+  auto kern = ch_batch_x2_kernel<ORDER, MODE, TW, TY, NTY>;
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TW * NTY, smem));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int grid = std::max(1, std::min(b->n_items, per_sm * b->ctx->num_sms));
+  kern<<<grid, dim3(TW, NTY), smem, b->ctx->stream>>>(static_cast<const Member<float>*>(b->member_table),
+                                                     static_cast<const int4*>(b->items), b->n_items, buf, stage);
+  GC_CHECK_LAUNCH("ch_batch_x2_kernel");
+  return GC_OK;
+}
+
 template <class T, int ORDER, int MODE, int TW, int TY, int NTY>
 gc_status launch_batch_shape(gc_ch_batch* b, const BatchBuffers<T>& buf, int stage) {
+  if constexpr (sizeof(T) == 4) {
+    if (b->x2) return launch_batch_shape_x2<ORDER, MODE, TW, TY, NTY>(b, buf, stage);
+  }
   constexpr size_t smem = pipe_smem<T, ORDER, TW, TY>();
   auto kern = ch_batch_kernel<T, ORDER, MODE, TW, TY, NTY>;
   static int per_sm = 0;
@@ -287,7 +319,7 @@ gc_status build_items(gc_ch_batch* b) {
   if (b->items_shape == b->shape) return GC_OK;
   const TileShape sh = kShapes[b->shape];
   const int R = b->order / 2;
-  const int tx = sh.tw - 2 * R;
+  const int tx = (b->x2 ? 2 * sh.tw : sh.tw) - 2 * R;
   std::vector<int4> items;
   for (int m = 0; m < b->n; ++m) {
     const int nx = b->members[m].nx, ny = b->members[m].ny;
@@ -386,6 +418,7 @@ std::string signature(const gc_ch_batch* b) {
   mix(static_cast<unsigned long long>(b->n));
   mix(static_cast<unsigned long long>(b->order));
   mix(static_cast<unsigned long long>(b->dtype));
+  mix(b->x2 ? 2ULL : 1ULL);
   for (const auto& m : b->members) {
     mix(static_cast<unsigned long long>(m.nx));
     mix(static_cast<unsigned long long>(m.ny));
@@ -423,6 +456,8 @@ GC_API gc_status gc_ch_batch_create(gc_context* ctx, int32_t n, const gc_ch_memb
   b->order = order;
   b->dtype = dt;
   b->members.assign(members, members + n);
+  b->x2 = dt == GC_F32;
+  for (int m = 0; m < n; ++m) b->x2 = b->x2 && members[m].nx % 2 == 0;
   b->offsets.resize(n + 1);
   long long off = 0;
   for (int m = 0; m < n; ++m) {

@@ -71,6 +71,23 @@ def test_f32_ensemble_error_and_diagnostics(gc, oracle):
     b.close()
 
 
+def test_f32_ensemble_with_odd_width_member(gc, oracle):
+    """One odd-width member sends the float ensemble down the one-column
+    tiles; every member still within 1e-4 of the FP64 oracle."""
+    import torch
+    members = [(nx, ny, 1.0, kap, stable_dt(kap)) for nx, ny, kap in [(64, 48, 0.7), (33, 40, 1.1), (96, 17, 1.5)]]
+    b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    init = [c.astype(np.float32).astype(np.float64) for c in ics(members, seed=5)]
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    b.run(150)
+    for i, (nx, ny, mob, kap, dt) in enumerate(members):
+        want = oracle.ch_integrate(4, mob, kap, init[i].reshape(1, ny, nx), dt, 150)
+        l2 = np.linalg.norm(b.get_member(i).reshape(1, ny, nx) - want) / np.linalg.norm(want)
+        assert l2 < 1e-4, (i, l2)
+    b.close()
+
+
 def test_diagnostics_match_oracle_f64(gc, oracle):
     import torch
     b = gc.ChBatch(MEMBERS[:5], order=4, dtype=torch.float64)

@@ -147,6 +147,40 @@ def test_float32_error_vs_double_oracle(gc, oracle):
     assert abs((f_gpu + v4) - (f_ref + v4)) / abs(f_ref + v4) < 1e-3
 
 
+@pytest.mark.parametrize("shape,order", [((1, 96, 130), 2), ((1, 96, 130), 4), ((1, 40, 134), 6),
+                                         ((1, 40, 127), 2), ((1, 33, 71), 4), ((1, 24, 10), 2), ((1, 20, 16), 4)])
+def test_float32_tile_paths_vs_double_oracle(gc, oracle, shape, order):
+    """Float runs two columns per thread on even widths and one otherwise;
+    both, with edge and partial tiles and grids narrower than a tile, stay
+    within 1e-4 relative L2 of the FP64 oracle over 200 RK4 steps."""
+    import torch
+    psi0 = uniform_ic(shape, 7).astype(np.float32).astype(np.float64)
+    t = dev(psi0, torch.float32)
+    dt = {2: 0.01, 4: 0.006, 6: 0.005}[order]
+    gc.ch_integrate(t, grid_of(gc, shape), gc.CahnHilliardRhs(0.9, 1.1, order), dt, 200, gc.RK4)
+    want = oracle.ch_integrate(order, 0.9, 1.1, psi0, dt, 200)
+    err = np.linalg.norm(host(t) - want) / np.linalg.norm(want)
+    assert err < 1e-4, err
+
+
+@pytest.mark.parametrize("width", [130, 127])
+def test_float32_rkc_and_euler_vs_double(gc, width):
+    """The RKC2 stages and the Euler step in float (two-column and one-column
+    tiles) against the same library steps in double."""
+    import torch
+    shape = (1, 48, width)
+    psi0 = uniform_ic(shape, 9).astype(np.float32).astype(np.float64)
+    g = grid_of(gc, shape)
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
+    for run in (lambda x: gc.ch_rkc(x, g, rhs, 0.16, 10, 6),
+                lambda x: gc.ch_integrate(x, g, rhs, 0.01, 50, gc.ExplicitEuler)):
+        a, b = dev(psi0, torch.float32), dev(psi0)
+        run(a)
+        run(b)
+        err = float(torch.linalg.norm(a.double() - b) / torch.linalg.norm(b))
+        assert err < 1e-5, err
+
+
 def test_acceptance_3d_coarsening(gc, oracle):
     """test/cahn_hilliard_test.cpp:95-184 restated: 24^3, dt = 0.02,
     kappa = 0.5, amplitude 0.1 (mean removed), snapshots after 0, 500, 1000,
