@@ -1,14 +1,15 @@
 // Periodic finite-difference operators: laplacian, gradient, divergence,
 // biharmonic at orders 2, 4, 6, in double (reference-exact) and float.
 //
-// Kernel shape (3-D): a CTA owns a BX x BY column of cells and marches up a
-// chunk of z planes.  Each plane is staged once in shared memory with its
-// periodic x/y halo (wrapped indices, coalesced rows), into a ring of
-// 2*RZ+1 planes, so the z taps, the in-plane taps and the mixed taps of the
+// Kernel shape: a CTA owns a BX x BY column of cells.  Planes are staged in
+// shared memory with their periodic x/y halo (wrapped indices, coalesced
+// rows), so the z taps, the in-plane taps and the mixed taps of the
 // biharmonic all come from shared memory and each input value is read from
-// HBM once.  2-D grids (Nz == 1) use the same kernel with a single plane;
-// the degenerate z axis then sums the centre value with the z weights, as
-// the reference's wrapped access does.
+// HBM once.  3-D grids march up a chunk of z planes, either with a register
+// queue of z taps (zmarch_kernel) or through a ring of whole planes filled
+// asynchronously several planes ahead (zring_kernel); 2-D grids (Nz == 1)
+// use one staged plane (stencil_kernel), and the degenerate z axis then sums
+// the centre value with the z weights, as the reference's wrapped access does.
 #include <algorithm>
 
 #include "common.cuh"
@@ -47,6 +48,69 @@ struct OpParams {
   T ihx2, ihy2, ihz2;  // 1/h^2
   T ihx4, ihy4, ihz4;  // 1/h^4
 };
+
+// Output of one cell from the staged values: at(f, dx, dy, dz) is field f
+// at that offset from the cell.  The arithmetic follows the reference's
+// tap order (diff/Laplacian.hpp:63-69, Gradient.hpp, Divergence.hpp,
+// Biharmonic.hpp:70-99), so double results are bit-identical to it.
+template <class T, int OP, int ORDER, bool Z3, class At>
+__device__ __forceinline__ void cell_op(const OpParams<T>& p, size_t c, const At& at) {
+  if constexpr (OP == OP_LAP || OP == OP_GRAD) {
+    constexpr int K = OP == OP_LAP ? 2 : 1;
+    const T ax = tap_sum<T, K, ORDER>([&](int o) { return at(0, o, 0, 0); });
+    const T ay = tap_sum<T, K, ORDER>([&](int o) { return at(0, 0, o, 0); });
+    const T az = tap_sum<T, K, ORDER>([&](int o) { return at(0, 0, 0, Z3 ? o : 0); });
+    if constexpr (OP == OP_LAP) {
+      p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)),
+                            Ar<T>::mul(az, p.ihz2));
+    } else {
+      p.out[c] = Ar<T>::mul(ax, p.ihx);
+      p.out[p.n + c] = Ar<T>::mul(ay, p.ihy);
+      p.out[2 * p.n + c] = Ar<T>::mul(az, p.ihz);
+    }
+  } else if constexpr (OP == OP_DIV) {
+    const T ax = tap_sum<T, 1, ORDER>([&](int o) { return at(0, o, 0, 0); });
+    const T ay = tap_sum<T, 1, ORDER>([&](int o) { return at(1, 0, o, 0); });
+    const T az = tap_sum<T, 1, ORDER>([&](int o) { return at(2, 0, 0, Z3 ? o : 0); });
+    p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx), Ar<T>::mul(ay, p.ihy)),
+                          Ar<T>::mul(az, p.ihz));
+  } else {
+    // diff/Biharmonic.hpp:70-99: axial fourth derivatives, then the three
+    // mixed second-derivative products, outer loop over the second axis.
+    const T d4x = tap_sum<T, 4, ORDER>([&](int o) { return at(0, o, 0, 0); });
+    const T d4y = tap_sum<T, 4, ORDER>([&](int o) { return at(0, 0, o, 0); });
+    const T d4z = tap_sum<T, 4, ORDER>([&](int o) { return at(0, 0, 0, Z3 ? o : 0); });
+    constexpr int R2 = W<2, ORDER>::R;
+    T xy = T(0), xz = T(0), yz = T(0);
+#pragma unroll
+    for (int mb = 0; mb <= 2 * R2; ++mb) {
+#pragma unroll
+      for (int ma = 0; ma <= 2 * R2; ++ma) {
+        const double wab_d = W<2, ORDER>::w(ma) * W<2, ORDER>::w(mb);
+        const T wab = static_cast<T>(wab_d);
+        const int oa = ma - R2, ob = mb - R2;
+        const T vxy = at(0, oa, ob, 0);
+        const T vxz = at(0, oa, 0, Z3 ? ob : 0);
+        const T vyz = at(0, 0, oa, Z3 ? ob : 0);
+        if (wab_d == 1.0) {
+          xy = Ar<T>::add(xy, vxy);
+          xz = Ar<T>::add(xz, vxz);
+          yz = Ar<T>::add(yz, vyz);
+        } else {
+          xy = Ar<T>::mac(xy, wab, vxy);
+          xz = Ar<T>::mac(xz, wab, vxz);
+          yz = Ar<T>::mac(yz, wab, vyz);
+        }
+      }
+    }
+    const T axial = Ar<T>::add(Ar<T>::add(Ar<T>::mul(d4x, p.ihx4), Ar<T>::mul(d4y, p.ihy4)),
+                               Ar<T>::mul(d4z, p.ihz4));
+    const T c1 = Ar<T>::mul(Ar<T>::mul(xy, p.ihx2), p.ihy2);
+    const T c2 = Ar<T>::mul(Ar<T>::mul(xz, p.ihx2), p.ihz2);
+    const T c3 = Ar<T>::mul(Ar<T>::mul(yz, p.ihy2), p.ihz2);
+    p.out[c] = Ar<T>::add(axial, Ar<T>::mul(T(2), Ar<T>::add(Ar<T>::add(c1, c2), c3)));
+  }
+}
 
 template <class T, int OP, int ORDER, bool Z3>
 __global__ void __launch_bounds__(NT) stencil_kernel(const OpParams<T> p) {
@@ -103,61 +167,7 @@ __global__ void __launch_bounds__(NT) stencil_kernel(const OpParams<T> p) {
     };
     if (active) {
       const size_t c = static_cast<size_t>(z) * nx * ny + static_cast<size_t>(gy) * nx + gx;
-      if constexpr (OP == OP_LAP || OP == OP_GRAD) {
-        constexpr int K = OP == OP_LAP ? 2 : 1;
-        const T ax = tap_sum<T, K, ORDER>([&](int o) { return at(0, o, 0, 0); });
-        const T ay = tap_sum<T, K, ORDER>([&](int o) { return at(0, 0, o, 0); });
-        const T az = tap_sum<T, K, ORDER>([&](int o) { return at(0, 0, 0, Z3 ? o : 0); });
-        if constexpr (OP == OP_LAP) {
-          p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx2), Ar<T>::mul(ay, p.ihy2)),
-                                Ar<T>::mul(az, p.ihz2));
-        } else {
-          p.out[c] = Ar<T>::mul(ax, p.ihx);
-          p.out[p.n + c] = Ar<T>::mul(ay, p.ihy);
-          p.out[2 * p.n + c] = Ar<T>::mul(az, p.ihz);
-        }
-      } else if constexpr (OP == OP_DIV) {
-        const T ax = tap_sum<T, 1, ORDER>([&](int o) { return at(0, o, 0, 0); });
-        const T ay = tap_sum<T, 1, ORDER>([&](int o) { return at(1, 0, o, 0); });
-        const T az = tap_sum<T, 1, ORDER>([&](int o) { return at(2, 0, 0, Z3 ? o : 0); });
-        p.out[c] = Ar<T>::add(Ar<T>::add(Ar<T>::mul(ax, p.ihx), Ar<T>::mul(ay, p.ihy)),
-                              Ar<T>::mul(az, p.ihz));
-      } else {
-        // diff/Biharmonic.hpp:70-99: axial fourth derivatives, then the three
-        // mixed second-derivative products, outer loop over the second axis.
-        const T d4x = tap_sum<T, 4, ORDER>([&](int o) { return at(0, o, 0, 0); });
-        const T d4y = tap_sum<T, 4, ORDER>([&](int o) { return at(0, 0, o, 0); });
-        const T d4z = tap_sum<T, 4, ORDER>([&](int o) { return at(0, 0, 0, Z3 ? o : 0); });
-        constexpr int R2 = W<2, ORDER>::R;
-        T xy = T(0), xz = T(0), yz = T(0);
-#pragma unroll
-        for (int mb = 0; mb <= 2 * R2; ++mb) {
-#pragma unroll
-          for (int ma = 0; ma <= 2 * R2; ++ma) {
-            const double wab_d = W<2, ORDER>::w(ma) * W<2, ORDER>::w(mb);
-            const T wab = static_cast<T>(wab_d);
-            const int oa = ma - R2, ob = mb - R2;
-            const T vxy = at(0, oa, ob, 0);
-            const T vxz = at(0, oa, 0, Z3 ? ob : 0);
-            const T vyz = at(0, 0, oa, Z3 ? ob : 0);
-            if (wab_d == 1.0) {
-              xy = Ar<T>::add(xy, vxy);
-              xz = Ar<T>::add(xz, vxz);
-              yz = Ar<T>::add(yz, vyz);
-            } else {
-              xy = Ar<T>::mac(xy, wab, vxy);
-              xz = Ar<T>::mac(xz, wab, vxz);
-              yz = Ar<T>::mac(yz, wab, vyz);
-            }
-          }
-        }
-        const T axial = Ar<T>::add(Ar<T>::add(Ar<T>::mul(d4x, p.ihx4), Ar<T>::mul(d4y, p.ihy4)),
-                                   Ar<T>::mul(d4z, p.ihz4));
-        const T c1 = Ar<T>::mul(Ar<T>::mul(xy, p.ihx2), p.ihy2);
-        const T c2 = Ar<T>::mul(Ar<T>::mul(xz, p.ihx2), p.ihz2);
-        const T c3 = Ar<T>::mul(Ar<T>::mul(yz, p.ihy2), p.ihz2);
-        p.out[c] = Ar<T>::add(axial, Ar<T>::mul(T(2), Ar<T>::add(Ar<T>::add(c1, c2), c3)));
-      }
+      cell_op<T, OP, ORDER, Z3>(p, c, at);
     }
     __syncthreads();
   }
@@ -286,6 +296,112 @@ gc_status launch_zmarch(gc_context* ctx, const OpParams<T>& p0) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// 3-D kernel with asynchronous plane staging.  A 32 x 8 CTA owns a column of
+// cells and marches up a chunk of z planes.  Every plane (with its periodic
+// x/y halo) is copied into a ring of shared-memory slots by cp.async, kRing
+// planes ahead of the plane being computed, one commit group per plane, so
+// many planes' loads are in flight without holding registers; each thread
+// waits for its own copies, one barrier per plane makes them visible, and
+// the cell is computed from the ring exactly as in the ring kernel above.
+// The ring has 2R + 1 + kRing slots: the slot refilled after computing
+// plane z held plane z - R - 1, which no thread reads once all have passed
+// plane z's barrier.
+constexpr int kRing = 4;
+
+__device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, int bytes) {
+  const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <class T, int OP, int ORDER>
+__global__ void __launch_bounds__(NT) zring_kernel(const OpParams<T> p) {
+  constexpr int R = OpShape<OP, ORDER>::R;
+  constexpr int NF = OpShape<OP, ORDER>::NF;
+  constexpr int PW = BX + 2 * R, PH = BY + 2 * R, PS = PW * PH;
+  constexpr int NB = 2 * R + 1 + kRing;
+  constexpr int EPT = (PS + NT - 1) / NT;  // staged elements per thread per plane and field
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);  // [NF][NB][PS]
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+  const int z0 = blockIdx.z * p.zc;
+  const int z1 = min(z0 + p.zc, nz);
+  const size_t plane = static_cast<size_t>(nx) * ny;
+
+  // This thread's staged elements: the same in-plane offsets for every plane.
+  size_t goff[EPT];
+  int soff[EPT];
+#pragma unroll
+  for (int e = 0; e < EPT; ++e) {
+    const int idx = tid + e * NT;
+    soff[e] = idx < PS ? idx : -1;
+    const int r = idx / PW, cc = idx - r * PW;
+    goff[e] = idx < PS ? static_cast<size_t>(wrap(y0 - R + r, ny)) * nx + wrap(x0 - R + cc, nx) : 0;
+  }
+  auto slot_of = [&](int z) { return (z - z0 + R) % NB; };
+  auto issue = [&](int z) {  // plane z (wrapped) into its slot, as one commit group
+    if (z <= z1 - 1 + R) {
+      const size_t zo = static_cast<size_t>(wrap(z, nz)) * plane;
+      const int sl = slot_of(z);
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int e = 0; e < EPT; ++e)
+          if (soff[e] >= 0) cp_async_n(ring + (f * NB + sl) * PS + soff[e], p.in[f] + zo + goff[e], sizeof(T));
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  for (int z = z0 - R; z < z0 + R + kRing; ++z) issue(z);
+  const int gx = x0 + tx, gy = y0 + ty;
+  const bool active = gx < nx && gy < ny;
+  for (int z = z0; z < z1; ++z) {
+    // plane z + R landed: the kRing - 1 later groups may still be in flight
+    asm volatile("cp.async.wait_group %0;" ::"n"(kRing - 1) : "memory");
+    __syncthreads();
+    if (active) {
+      auto at = [&](int f, int dx, int dy, int dz) -> T {
+        return ring[(f * NB + slot_of(z + dz)) * PS + (ty + R + dy) * PW + (tx + R + dx)];
+      };
+      cell_op<T, OP, ORDER, true>(p, static_cast<size_t>(z) * plane + static_cast<size_t>(gy) * nx + gx, at);
+    }
+    issue(z + R + kRing);
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+template <class T, int OP, int ORDER>
+gc_status launch_zring(gc_context* ctx, const OpParams<T>& p0) {
+  constexpr int R = OpShape<OP, ORDER>::R;
+  constexpr int NF = OpShape<OP, ORDER>::NF;
+  constexpr size_t smem = sizeof(T) * NF * (2 * R + 1 + kRing) * (BX + 2 * R) * (BY + 2 * R);
+  OpParams<T> p = p0;
+  const int tiles_x = div_up(p.nx, BX), tiles_y = div_up(p.ny, BY);
+  const long long tiles = static_cast<long long>(tiles_x) * tiles_y;
+  // Enough CTAs to fill the GPU several times, chunks of at least 32 planes
+  // so the 2R + kRing prologue planes stay a small overhead.
+  const long long want = 16LL * ctx->num_sms;
+  int chunks = static_cast<int>(std::min<long long>((want + tiles - 1) / tiles, std::max(1, p.nz / 32)));
+  chunks = std::max(chunks, 1);
+  p.zc = div_up(p.nz, chunks);
+  chunks = div_up(p.nz, p.zc);
+  auto kern = zring_kernel<T, OP, ORDER>;
+  static bool attr = false;
+  if (!attr) {
+    if (smem > 48 * 1024)
+      GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr = true;
+  }
+  dim3 grid(tiles_x, tiles_y, chunks), block(BX, BY);
+  kern<<<grid, block, smem, ctx->stream>>>(p);
+  GC_CHECK_LAUNCH("zring_kernel");
+  return GC_OK;
+}
+
 template <class T, int OP, int ORDER, bool Z3>
 gc_status launch_one(gc_context* ctx, const OpParams<T>& p0) {
   constexpr int R = OpShape<OP, ORDER>::R;
@@ -317,22 +433,32 @@ gc_status launch_one(gc_context* ctx, const OpParams<T>& p0) {
 template <class T, int OP>
 gc_status dispatch_order(gc_context* ctx, int order, const OpParams<T>& p) {
   const bool z3 = p.nz > 1;
-  if constexpr (OP != OP_BIH) {
-    // 3-D axis-separable operators: z-march with a register queue.  The
-    // queue and the halo strips need the z extent and the tile to exceed
-    // the radius (degenerate and tiny axes keep the plane-ring kernel).
-    if (z3 && p.nz > 2 * OpShape<OP, 6>::R) {
-      switch (order) {
-        case 2: return launch_zmarch<T, OP, 2>(ctx, p);
-        case 4: return launch_zmarch<T, OP, 4>(ctx, p);
-        case 6: return launch_zmarch<T, OP, 6>(ctx, p);
+  // 3-D grids.  Gradient, divergence and the order-6 laplacian march with a
+  // register queue (one field's value per plane and thread, halo strips by
+  // a few threads); the order-2/4 laplacian and the biharmonic stage whole
+  // planes through the asynchronous ring (measured per operator and order
+  // on 256^3 and 512^3).  The z-march needs the z extent to exceed the
+  // radius; smaller extents take the ring (planes wrap).
+  if (z3) {
+    if constexpr (OP == OP_GRAD || OP == OP_DIV || OP == OP_LAP) {
+      if ((OP != OP_LAP || order == 6) && p.nz > 2 * OpShape<OP, 6>::R) {
+        switch (order) {
+          case 2: return launch_zmarch<T, OP, 2>(ctx, p);
+          case 4: return launch_zmarch<T, OP, 4>(ctx, p);
+          case 6: return launch_zmarch<T, OP, 6>(ctx, p);
+        }
       }
+    }
+    switch (order) {
+      case 2: return launch_zring<T, OP, 2>(ctx, p);
+      case 4: return launch_zring<T, OP, 4>(ctx, p);
+      case 6: return launch_zring<T, OP, 6>(ctx, p);
     }
   }
   switch (order) {
-    case 2: return z3 ? launch_one<T, OP, 2, true>(ctx, p) : launch_one<T, OP, 2, false>(ctx, p);
-    case 4: return z3 ? launch_one<T, OP, 4, true>(ctx, p) : launch_one<T, OP, 4, false>(ctx, p);
-    case 6: return z3 ? launch_one<T, OP, 6, true>(ctx, p) : launch_one<T, OP, 6, false>(ctx, p);
+    case 2: return launch_one<T, OP, 2, false>(ctx, p);
+    case 4: return launch_one<T, OP, 4, false>(ctx, p);
+    case 6: return launch_one<T, OP, 6, false>(ctx, p);
   }
   return fail(GC_ERR_UNSUPPORTED, "gridcalc_b200: order must be 2, 4 or 6; got " + std::to_string(order));
 }

@@ -45,7 +45,8 @@ def radius(op, order):
 
 SHAPES = [((8, 10, 12), (0.3, 0.25, 0.5)), ((1, 9, 17), (1.0, 1.0, 1.0)),
           ((7, 20, 33), (1.0, 1.0, 1.0)), ((24, 40, 70), (0.1, 0.2, 0.3)), ((1, 65, 130), (1.0, 1.0, 1.0)),
-          ((9, 1, 11), (1.0, 1.0, 1.0))]
+          ((9, 1, 11), (1.0, 1.0, 1.0)),
+          ((96, 20, 36), (0.5, 0.4, 0.3))]   # several z chunks per column of the 3-D plane ring
 
 
 @pytest.mark.parametrize("op", OPS)
