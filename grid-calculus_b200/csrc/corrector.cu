@@ -1,7 +1,8 @@
 // Learned coarse-step corrector for 2-D Cahn-Hilliard: a 6-layer periodic
 // 3x3 CNN (32 channels, GELU in tanh form), BF16 weights and activations, FP32
-// accumulation on the tensor cores (mma.sync m16n8k16 bf16), trained and run
-// by the kernels in this file.
+// accumulation on the tensor cores -- tcgen05 MMAs with tensor-memory
+// accumulators for the forward and backward-data convolutions, mma.sync
+// for the weight gradient -- trained and run by the kernels in this file.
 //
 // Network: x0 = [c, u, e, 0, ..., 0] (32 channels, NHWC), for l = 1..6:
 //   z_l = conv3x3_periodic(x_{l-1}, W_l) + b_l,  x_l = gelu(z_l) (l < 6);
@@ -16,11 +17,10 @@
 // (the trapezoid residual of the base step, f the Cahn-Hilliard RHS), with
 // rho = Dt rms(est): the correction is learned in units of the base step's
 // own error indicator, so small late-time errors are corrected as precisely
-// as large early ones.  Every layer is
-// computed as a 32 -> 32 convolution (the first layer's input channels
-// 1..31 are zero and the last layer's outputs 1..31 are unused), so one
-// implicit-GEMM kernel serves all layers: M = pixels, N = 32 output
-// channels, K = 9 taps x 32 input channels.
+// as large early ones.  Every layer is computed as a 32 -> 32 convolution
+// (the first layer's input channels 3..31 are zero and the last layer's
+// outputs 1..31 are unused), so one implicit-GEMM kernel serves all layers:
+// M = pixels, N = 32 output channels, K = 9 taps x 32 input channels.
 //
 // Parameters (FP32 master, packed): per layer W[9][32 ci][32 co] then b[32];
 // tap t covers offset (dy, dx) = (t / 3 - 1, t % 3 - 1).
@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace gcb {
 namespace {
@@ -42,18 +43,9 @@ constexpr int kC = 32;                       // channels
 constexpr int kTaps = 9;
 constexpr int kLayerParams = kTaps * kC * kC + kC;
 constexpr int kParams = kLayers * kLayerParams;
-constexpr int kPixStride = 40;               // bf16 per pixel in shared memory (80 B: conflict-free)
 // Weight-gradient tiles: 8 rows x 16 columns of pixels.
 constexpr int kTR = 8, kTC = 16;
 constexpr int kHaloR = kTR + 2, kHaloC = kTC + 2;
-// Forward / backward-data tiles: 4 rows x 64 columns (256 pixels), 8 warps;
-// warp w owns row w / 2, columns (w % 2) * 32 .. + 31 (two m16 tiles).
-constexpr int kCR = 4, kCC = 64;
-constexpr int kConvThreads = 256;
-constexpr int kInR = kCR + 2, kInC = kCC + 2, kInPix = kInR * kInC;
-constexpr int kConvSmemW = kTaps * kC * kPixStride * 2;     // 23,040 B
-constexpr int kConvSmemIn = kInPix * kPixStride * 2;         // 31,680 B per buffer
-constexpr int kConvSmem = kConvSmemW + 2 * kConvSmemIn;      // 86,400 B: two CTAs per SM
 
 // GELU in its tanh form (Hendrycks & Gimpel 2016):
 //   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
@@ -90,17 +82,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], const void* p) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-               : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void ldsm_x2(uint32_t (&r)[2], const void* p) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(smem_u32(p)));
-}
 __device__ __forceinline__ void cp_async16(void* s, const void* g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(s)), "l"(g) : "memory");
 }
@@ -108,139 +89,245 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// ---- forward / backward-data convolution ----------------------------------
-// out[p][n] = sum_t sum_k in[p + off_t][k] * Bw[t][n][k]  (+ epilogue)
-// Epilogue kinds:
+// Epilogue kinds of the convolution:
 //   EPI_FWD    z = acc + bias; store gelu(z) (bf16) and, for training, z (bf16)
 //   EPI_LAST   z0 = acc + bias (channel 0 only); store z0 (fp32)
 //   EPI_BWD    dz_prev = acc * gelu'(z_prev); store (bf16)
-// Persistent CTAs: the layer's weights are staged once; pixel tiles (with a
-// one-pixel periodic halo) are double-buffered with cp.async so the next
-// tile's loads overlap this tile's tensor-core work.  Operands reach the
-// tensor cores through ldmatrix from 80-byte pixel rows (conflict-free).
 enum Epi { EPI_FWD = 0, EPI_LAST = 1, EPI_BWD = 2 };
 
-template <int EPI, int NT, bool STORE_Z>
-__global__ void __launch_bounds__(kConvThreads, 2) conv3x3_kernel(
+// ---- tcgen05 (UMMA) forward / backward-data convolution ---------------------
+// The same implicit GEMM on the 5th-generation tensor cores.  A tile is two
+// image rows of 128 consecutive pixels; each row is one UMMA M = 128 with
+// N = 32 output channels and K = 9 taps x 32 input channels in 18 MMAs of
+// K = 16, accumulated in tensor memory.  Operands live in shared memory in
+// the K-major no-swizzle layout (8-row x 16-byte core matrices): the staged
+// input rows y-1 .. y+2 (130 pixels each with the periodic halo) are kept
+// as four planes of 8 channels, pixel-contiguous at 16 bytes, so the A
+// operand of output row j and tap (dy, dx) is the same plane started
+// (j + 1 + dy) rows and (1 + dx) pixels in -- a shift of the descriptor's
+// start address.  Weights are [tap][8-channel chunk][n][8].
+// Software pipeline per CTA: one thread issues tile i's 36 MMAs and commits
+// them to an mbarrier; meanwhile all warps wait for tile i-1's
+// accumulators, stage tile i+1 by cp.async into the buffer tile i-1 used,
+// and run tile i-1's epilogue (each warp reads its 32 TMEM lanes = pixels,
+// 32 columns = channels; 16-byte stores).  Tiles and accumulators are
+// double-buffered.  Every mbarrier wait is bounded; on expiry the CTA
+// records GC_ERR_TIMEOUT, stops, and frees its tensor memory.
+constexpr int kUM = 128;                       // pixels per tile row = UMMA M
+constexpr int kUR = 2;                         // output rows per tile
+constexpr int kUCols = kUM + 2;                // staged pixels per row
+constexpr int kUPix = (kUR + 2) * kUCols;      // staged pixels
+constexpr int kUChunk = kUPix * 16;            // bytes of one 8-channel plane
+constexpr int kUIn = 4 * kUChunk;              // one staged tile
+constexpr int kUW = kTaps * 4 * kC * 16;       // weights
+constexpr int kUSmem = kUW + 2 * kUIn + 64;    // + two mbarriers and the TMEM address
+constexpr int kUThreads = 256;                 // 8 warps: warp w reads TMEM lanes 32 (w % 4), channels 16 (w / 4) ..
+constexpr uint32_t kUTmemCols = 2 * kUR * 32;  // two tiles x kUR accumulators of 32 columns
+constexpr long long kUWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
+// Instruction descriptor: D f32, A and B bf16, both K-major, N = 32, M = 128.
+constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading byte
+// offset (between the two 8-element K chunks), stride byte offset (between
+// 8-row groups), version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(kUIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Epilogue of channels c0 .. c0 + 15 of one output pixel from their
+// accumulator values.
+template <int EPI, bool STORE_Z>
+__device__ __forceinline__ void conv_epilogue(const uint32_t (&r)[16], int c0, size_t gp,
+                                              const float* __restrict__ bias, __nv_bfloat16* __restrict__ out_z,
+                                              __nv_bfloat16* __restrict__ out_y, float* __restrict__ out_f,
+                                              const __nv_bfloat16* __restrict__ z_prev) {
+  if constexpr (EPI == EPI_LAST) {
+    if (c0 == 0) out_f[gp] = __uint_as_float(r[0]) + bias[0];
+  } else if constexpr (EPI == EPI_FWD) {
+    uint32_t o[8], zb[8];
+#pragma unroll
+    for (int n = 0; n < 16; n += 2) {
+      const float v0 = __uint_as_float(r[n]) + __ldg(bias + c0 + n);
+      const float v1 = __uint_as_float(r[n + 1]) + __ldg(bias + c0 + n + 1);
+      zb[n / 2] = pack_bf16(v0, v1);
+      o[n / 2] = pack_bf16(gelu(v0), gelu(v1));
+    }
+    if constexpr (STORE_Z) {
+      uint4* dz = reinterpret_cast<uint4*>(out_z + gp * kC + c0);
+      dz[0] = make_uint4(zb[0], zb[1], zb[2], zb[3]);
+      dz[1] = make_uint4(zb[4], zb[5], zb[6], zb[7]);
+    }
+    uint4* dy = reinterpret_cast<uint4*>(out_y + gp * kC + c0);
+    dy[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dy[1] = make_uint4(o[4], o[5], o[6], o[7]);
+  } else {
+    uint32_t o[8];
+    const uint4* zp = reinterpret_cast<const uint4*>(z_prev + gp * kC + c0);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const uint4 zz = __ldg(zp + q);
+      const uint32_t zw[4] = {zz.x, zz.y, zz.z, zz.w};
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const float2 zf = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&zw[h]));
+        const int n = 8 * q + 2 * h;
+        o[4 * q + h] = pack_bf16(__uint_as_float(r[n]) * gelu_grad(zf.x), __uint_as_float(r[n + 1]) * gelu_grad(zf.y));
+      }
+    }
+    uint4* dz = reinterpret_cast<uint4*>(out_z + gp * kC + c0);
+    dz[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dz[1] = make_uint4(o[4], o[5], o[6], o[7]);
+  }
+}
+
+template <int EPI, bool STORE_Z>
+__global__ void __launch_bounds__(kUThreads) conv3x3_umma_kernel(
     const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* __restrict__ bw, const float* __restrict__ bias,
     __nv_bfloat16* __restrict__ out_z, __nv_bfloat16* __restrict__ out_y, float* __restrict__ out_f,
-    const __nv_bfloat16* __restrict__ z_prev, int H, int W, int tiles_x, int tiles_per_img, int n_tiles) {
-  extern __shared__ __align__(16) unsigned char conv_smem[];
-  __nv_bfloat16* s_w = reinterpret_cast<__nv_bfloat16*>(conv_smem);
-  __nv_bfloat16* s_in = reinterpret_cast<__nv_bfloat16*>(conv_smem + kConvSmemW);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, tig = lane & 3;
-  const int wr = warp >> 1, wc = (warp & 1) * 32;
+    const __nv_bfloat16* __restrict__ z_prev, int H, int W, int tiles_x, int tiles_per_img, int n_tiles,
+    int* status) {
+  extern __shared__ __align__(128) unsigned char usm[];
+  unsigned char* s_w = usm;
+  unsigned char* s_in = usm + kUW;  // [2][4 chunks][kUPix][16 B]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(usm + kUW + 2 * kUIn);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  // Weights [t][n][k] (dense 32 x 32 per tap) -> rows of 40.
-  for (int v = tid; v < kTaps * kC * (kC / 8); v += kConvThreads)
-    cp_async16(&s_w[(v >> 2) * kPixStride + (v & 3) * 8], bw + static_cast<size_t>(v) * 8);
-
-  auto issue = [&](int tl, int buf) {
-    const int img = tl / tiles_per_img;
+  // Weights: global [t][n][k] -> [t][k / 8][n][8].
+  for (int v = tid; v < kTaps * kC * 4; v += kUThreads) {
+    const int t = v >> 7, n = (v >> 2) & 31, q = v & 3;
+    cp_async16(s_w + t * 2048 + q * 512 + n * 16, bw + (t * kC + n) * kC + q * 8);
+  }
+  auto origin = [&](int tl, int& img, int& y0, int& x0) {
+    img = tl / tiles_per_img;
     const int tile = tl - img * tiles_per_img;
-    const int y0 = (tile / tiles_x) * kCR, x0 = (tile % tiles_x) * kCC;
+    const int ty = tile / tiles_x;
+    y0 = ty * kUR;
+    x0 = (tile - ty * tiles_x) * kUM;
+  };
+  auto issue = [&](int tl, int buf) {
+    int img, y0, x0;
+    origin(tl, img, y0, x0);
     const size_t img_off = static_cast<size_t>(img) * H * W;
-    __nv_bfloat16* dst = s_in + buf * (kInPix * kPixStride);
-    for (int v = tid; v < kInPix * (kC / 8); v += kConvThreads) {
+    unsigned char* dst = s_in + buf * kUIn;
+    for (int v = tid; v < kUPix * 4; v += kUThreads) {
       const int pix = v >> 2, q = v & 3;
-      const int r = pix / kInC, c = pix - r * kInC;
+      const int r = pix / kUCols, c = pix - r * kUCols;
       const size_t gp = img_off + static_cast<size_t>(wrap(y0 - 1 + r, H)) * W + wrap(x0 - 1 + c, W);
-      cp_async16(dst + pix * kPixStride + q * 8, in + gp * kC + q * 8);
+      cp_async16(dst + q * kUChunk + pix * 16, in + gp * kC + q * 8);
     }
+  };
+  // Warp w: TMEM lanes (pixels) 32 (w % 4) .. + 31, channels 16 (w / 4) .. + 15.
+  const int quad = warp & 3, c0 = (warp >> 2) * 16;
+  auto epilogue = [&](int tl, int buf) {
+    int img, y0, x0;
+    origin(tl, img, y0, x0);
+    const int ox = x0 + quad * 32 + lane;
+#pragma unroll
+    for (int j = 0; j < kUR; ++j) {
+      uint32_t r[16];
+      tmem_ld16(*tmem_slot + (static_cast<uint32_t>(quad * 32) << 16) + buf * (kUR * 32) + j * 32 + c0, r);
+      const int oy = y0 + j;
+      if (ox < W && oy < H)
+        conv_epilogue<EPI, STORE_Z>(r, c0, static_cast<size_t>(img) * H * W + static_cast<size_t>(oy) * W + ox,
+                                    bias, out_z, out_y, out_f, z_prev);
+    }
+  };
+  // Bounded wait for the accumulators of the tile issued at iteration k.
+  auto wait_mma = [&](int k) -> bool {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(&bar[k & 1], (k >> 1) & 1))
+      if (clock64() - t0 > kUWaitCycles) {
+        if (status) atomicExch(status, static_cast<int>(GC_ERR_TIMEOUT));
+        return false;
+      }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return true;
   };
 
   issue(blockIdx.x, 0);  // the grid never exceeds n_tiles
   cp_commit();
-  int it = 0;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kUTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  bool failed = false;
+  int it = 0, prev = -1;
   for (int tl = blockIdx.x; tl < n_tiles; tl += gridDim.x, ++it) {
     const int buf = it & 1;
+    cp_wait<0>();              // this tile's copies
+    fence_proxy_async_smem();  // cp.async writes -> visible to the tensor core's reads
+    if (__syncthreads_or(failed)) break;
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(s_in + buf * kUIn), b0 = smem_u32(s_w);
+#pragma unroll
+      for (int j = 0; j < kUR; ++j) {
+        const uint32_t d = tmem + buf * (kUR * 32) + j * 32;
+#pragma unroll
+        for (int t = 0; t < kTaps; ++t) {
+          const int dy = t / 3 - 1, dx = t % 3 - 1;
+          const uint32_t pix0 = static_cast<uint32_t>((j + 1 + dy) * kUCols + 1 + dx);
+#pragma unroll
+          for (int kh = 0; kh < 2; ++kh) {
+            const uint64_t ad = umma_desc(a0 + 2 * kh * kUChunk + pix0 * 16, kUChunk, 128);
+            const uint64_t bd = umma_desc(b0 + t * 2048 + 2 * kh * 512, 512, 128);
+            umma_bf16(d, ad, bd, (t | kh) != 0);
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   ::"r"(smem_u32(&bar[buf])) : "memory");
+    }
+    // The previous tile's MMAs: once done, its staging buffer takes the next
+    // tile and its accumulators are written out while this tile's MMAs run.
+    if (prev >= 0 && !wait_mma(it - 1)) {
+      failed = true;
+      continue;  // the loop's barrier makes every thread stop
+    }
     if (tl + static_cast<int>(gridDim.x) < n_tiles) issue(tl + gridDim.x, buf ^ 1);
     cp_commit();
-    cp_wait<1>();
-    __syncthreads();
-    const __nv_bfloat16* sb = s_in + buf * (kInPix * kPixStride);
-
-    float acc[2][NT][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.f;
-
-#pragma unroll
-    for (int t = 0; t < kTaps; ++t) {
-      const int dy = t / 3 - 1, dx = t % 3 - 1;
-#pragma unroll
-      for (int kh = 0; kh < 2; ++kh) {
-        uint32_t b[NT][2];
-        if constexpr (NT == 4) {
-#pragma unroll
-          for (int pr = 0; pr < 2; ++pr) {
-            uint32_t r[4];
-            const int n = t * kC + pr * 16 + (lane & 7) + ((lane >> 4) << 3);
-            ldsm_x4(r, &s_w[n * kPixStride + kh * 16 + ((lane >> 3) & 1) * 8]);
-            b[2 * pr][0] = r[0];
-            b[2 * pr][1] = r[1];
-            b[2 * pr + 1][0] = r[2];
-            b[2 * pr + 1][1] = r[3];
-          }
-        } else {
-          uint32_t r[2];
-          ldsm_x2(r, &s_w[(t * kC + (lane & 7)) * kPixStride + kh * 16 + ((lane >> 3) & 1) * 8]);
-          b[0][0] = r[0];
-          b[0][1] = r[1];
-        }
-#pragma unroll
-        for (int mt = 0; mt < 2; ++mt) {
-          const int pix = (wr + 1 + dy) * kInC + (wc + mt * 16 + (lane & 15) + 1 + dx);
-          uint32_t a[4];
-          ldsm_x4(a, &sb[pix * kPixStride + kh * 16 + (lane >> 4) * 8]);
-#pragma unroll
-          for (int nt = 0; nt < NT; ++nt) mma_bf16(acc[mt][nt], a, b[nt]);
-        }
-      }
-    }
-
-    // Epilogue: C fragment rows are pixels g and g + 8 of the m16 tile,
-    // columns (channels) 2 tig, 2 tig + 1 of each n8 tile.
-    const int img = tl / tiles_per_img;
-    const int tile = tl - img * tiles_per_img;
-    const int oy = (tile / tiles_x) * kCR + wr, x0 = (tile % tiles_x) * kCC;
-    const size_t img_off = static_cast<size_t>(img) * H * W;
-    if (oy < H) {
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-          const int ox = x0 + wc + mt * 16 + g + half * 8;
-          if (ox >= W) continue;
-          const size_t gp = img_off + static_cast<size_t>(oy) * W + ox;
-#pragma unroll
-          for (int nt = 0; nt < NT; ++nt) {
-            const int n = nt * 8 + tig * 2;
-            float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
-            if constexpr (EPI == EPI_FWD) {
-              v0 += bias[n];
-              v1 += bias[n + 1];
-              if constexpr (STORE_Z) *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) = pack_bf16(v0, v1);
-              *reinterpret_cast<uint32_t*>(out_y + gp * kC + n) = pack_bf16(gelu(v0), gelu(v1));
-            } else if constexpr (EPI == EPI_LAST) {
-              if (n == 0) out_f[gp] = v0 + bias[0];
-            } else {
-              const __nv_bfloat162 zp = *reinterpret_cast<const __nv_bfloat162*>(z_prev + gp * kC + n);
-              const float2 zf = __bfloat1622float2(zp);
-              *reinterpret_cast<uint32_t*>(out_z + gp * kC + n) =
-                  pack_bf16(v0 * gelu_grad(zf.x), v1 * gelu_grad(zf.y));
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();  // every warp is done with buf before it is refilled
+    if (prev >= 0) epilogue(prev, buf ^ 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    prev = tl;
   }
+  if (!failed && prev >= 0 && wait_mma(it - 1)) epilogue(prev, (it - 1) & 1);
+  // Drain the copies in flight, then free the tensor memory.
   cp_wait<0>();
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUTmemCols));
+  }
 }
 
 // ---- weight gradient ------------------------------------------------------
@@ -662,22 +749,24 @@ gc_status sample_mean(gc_corrector* c, int batch, const float* f, int hw, float*
   return GC_OK;
 }
 
+// Convolution layer on the tcgen05 kernel (NT: output channels the
+// epilogue needs -- 32, or 1 for the last layer).
 template <int EPI, int NT, bool STORE_Z>
 gc_status launch_conv(gc_corrector* c, int batch, const __nv_bfloat16* in, const __nv_bfloat16* w,
                       const float* bias, __nv_bfloat16* oz, __nv_bfloat16* oy, float* of, const __nv_bfloat16* zp) {
-  auto kern = conv3x3_kernel<EPI, NT, STORE_Z>;
+  auto kern = conv3x3_umma_kernel<EPI, STORE_Z>;
   static bool attr = false;  // one flag per instantiation
   if (!attr) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvSmem));
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kUSmem));
     attr = true;
   }
-  const int tiles_x = div_up(c->W, kCC), tiles_y = div_up(c->H, kCR);
-  const int tpi = tiles_x * tiles_y;
+  const int tiles_x = div_up(c->W, kUM);
+  const int tpi = tiles_x * div_up(c->H, kUR);
   const int n_tiles = batch * tpi;
-  const int grid = std::min(n_tiles, 2 * c->ctx->num_sms);
-  kern<<<grid, kConvThreads, kConvSmem, c->ctx->stream>>>(in, w, bias, oz, oy, of, zp, c->H, c->W, tiles_x, tpi,
-                                                          n_tiles);
-  GC_CHECK_LAUNCH("conv3x3_kernel");
+  const int grid = std::min(n_tiles, 2 * c->ctx->num_sms);  // two CTAs per SM (shared memory)
+  kern<<<grid, kUThreads, kUSmem, c->ctx->stream>>>(in, w, bias, oz, oy, of, zp, c->H, c->W, tiles_x, tpi, n_tiles,
+                                                    c->ctx->device_status);
+  GC_CHECK_LAUNCH("conv3x3_umma_kernel");
   return GC_OK;
 }
 
