@@ -47,18 +47,41 @@ constexpr int kParams = kLayers * kLayerParams;
 constexpr int kTR = 8, kTC = 16;
 constexpr int kHaloR = kTR + 2, kHaloC = kTC + 2;
 
+__device__ __forceinline__ uint32_t pack_bf16_rn(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
 // GELU in its tanh form (Hendrycks & Gimpel 2016):
 //   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
 //   gelu'(z) = (1 + tanh(u))/2 + z/2 (1 - tanh(u)^2) sqrt(2/pi) (1 + 3 0.044715 z^2),
-// with the hardware tanh (tanh.approx.f32, relative error ~2^-11, below the
-// bf16 rounding of the activations it feeds).
+// with the hardware tanh: tanh.approx.f32 for one value, tanh.approx.bf16x2
+// for the pairs the convolution epilogues produce (one transcendental-unit
+// instruction per two values: that unit bounds the epilogue; the bf16
+// result is as precise as the bf16 activations it feeds).
 __device__ __forceinline__ float tanh_hw(float x) {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ float2 tanh_hw2(float a, float b) {
+  const uint32_t in = pack_bf16_rn(a, b);
+  uint32_t out;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(out) : "r"(in));
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&out));
+}
 constexpr float kGeluA = 0.7978845608028654f;   // sqrt(2/pi)
 constexpr float kGeluB = 0.044715f;
+__device__ __forceinline__ float2 gelu2(float z0, float z1) {
+  const float2 t = tanh_hw2(kGeluA * fmaf(kGeluB * z0 * z0, z0, z0), kGeluA * fmaf(kGeluB * z1 * z1, z1, z1));
+  return make_float2(0.5f * z0 * (1.0f + t.x), 0.5f * z1 * (1.0f + t.y));
+}
+__device__ __forceinline__ float2 gelu_grad2(float z0, float z1) {
+  const float a0 = z0 * z0, a1 = z1 * z1;
+  const float2 t = tanh_hw2(kGeluA * fmaf(kGeluB * a0, z0, z0), kGeluA * fmaf(kGeluB * a1, z1, z1));
+  return make_float2(0.5f * (1.0f + t.x) + 0.5f * z0 * (1.0f - t.x * t.x) * kGeluA * fmaf(3.0f * kGeluB, a0, 1.0f),
+                     0.5f * (1.0f + t.y) + 0.5f * z1 * (1.0f - t.y * t.y) * kGeluA * fmaf(3.0f * kGeluB, a1, 1.0f));
+}
 __device__ __forceinline__ float gelu(float z) {
   const float t = tanh_hw(kGeluA * fmaf(kGeluB * z * z, z, z));
   return 0.5f * z * (1.0f + t);
@@ -167,7 +190,8 @@ __device__ __forceinline__ void conv_epilogue(const uint32_t (&r)[16], int c0, s
       const float v0 = __uint_as_float(r[n]) + __ldg(bias + c0 + n);
       const float v1 = __uint_as_float(r[n + 1]) + __ldg(bias + c0 + n + 1);
       zb[n / 2] = pack_bf16(v0, v1);
-      o[n / 2] = pack_bf16(gelu(v0), gelu(v1));
+      const float2 gy = gelu2(v0, v1);
+      o[n / 2] = pack_bf16(gy.x, gy.y);
     }
     if constexpr (STORE_Z) {
       uint4* dz = reinterpret_cast<uint4*>(out_z + gp * kC + c0);
@@ -188,7 +212,8 @@ __device__ __forceinline__ void conv_epilogue(const uint32_t (&r)[16], int c0, s
       for (int h = 0; h < 4; ++h) {
         const float2 zf = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&zw[h]));
         const int n = 8 * q + 2 * h;
-        o[4 * q + h] = pack_bf16(__uint_as_float(r[n]) * gelu_grad(zf.x), __uint_as_float(r[n + 1]) * gelu_grad(zf.y));
+        const float2 gd = gelu_grad2(zf.x, zf.y);
+        o[4 * q + h] = pack_bf16(__uint_as_float(r[n]) * gd.x, __uint_as_float(r[n + 1]) * gd.y);
       }
     }
     uint4* dz = reinterpret_cast<uint4*>(out_z + gp * kC + c0);
