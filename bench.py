@@ -395,7 +395,9 @@ def form_learned(gc, n_train=32, n_eval=4, fine_steps=5000, t_end=200.0, tols=(0
 def run_forms(gc, names, peak):
     forms = {}
     table = {"operators": lambda: form_operators(gc, peak), "fvm": lambda: form_fvm(gc, peak),
-             "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc)}
+             "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc),
+             # the learned workload at its full size: 512 training trajectories, 64 held-out seeds
+             "learned_full": lambda: form_learned(gc, n_train=512, n_eval=64, tols=(0.003, 0.01))}
     for nm in names:
         t0 = time.perf_counter()
         try:
@@ -404,6 +406,23 @@ def run_forms(gc, names, peak):
             forms[nm] = {"error": f"{type(exc).__name__}: {exc}"}
         forms[nm]["wall_s"] = time.perf_counter() - t0
     return forms
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of the ranks' values (every rank gets it); the value
+    itself on a single process."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, cells: int, steps: int, ms: float) -> float:
+    """Mcell-steps/s of the whole job: every rank advances its own replica of
+    `cells` cells by `steps` steps; `ms` is the slowest rank's time."""
+    return world * cells * steps / (ms / 1e3) / 1e6
 
 
 def run_ours(args, rank: int, world: int, local: int):
@@ -443,13 +462,9 @@ def run_ours(args, rank: int, world: int, local: int):
         end.record()
         torch.cuda.synchronize()
     barrier()
-    ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), dist, f"cuda:{local}")
     cells = g.size
-    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    value = whole_job_rate(world, cells, args.steps, ms)
     ms_per_step = ms / args.steps
     achieved = BYTES_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e9
     peak, peak_kind = peaks()
@@ -471,12 +486,8 @@ def run_ours(args, rank: int, world: int, local: int):
         host_psi.copy_(dev_psi, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ems], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e = world * cells * chunk * n_chunks / (ems / 1e3) / 1e6
+    ems = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+    e2e = whole_job_rate(world, cells, chunk * n_chunks, ems)
 
     launches = 4 * args.steps  # four stage kernels per RK4 step
     cpu = None
@@ -528,7 +539,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--forms", default="all",
-                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned")
+                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full "
+                         "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
