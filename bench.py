@@ -425,6 +425,54 @@ def whole_job_rate(world: int, cells: int, steps: int, ms: float) -> float:
     return world * cells * steps / (ms / 1e3) / 1e6
 
 
+def run_case(name: str) -> None:
+    """Small fixed workloads for profiler captures (ncu -k on one kernel):
+    each runs a few launches of one kernel family and exits."""
+    import numpy as np
+    import torch
+    import gridcalc_b200 as gc
+    if name == "conv_b16_512":      # corrector forward, 16 x 512^2 (tcgen05 convolutions)
+        net = gc.Corrector(512, 512, max_batch=16)
+        net.set_params(gc.corrector_init_params(1))
+        x = torch.rand(16, 512, 512, device="cuda", dtype=torch.float64)
+        for _ in range(2):
+            net.forward(x)
+    elif name == "lap2_384":        # 3-D laplacian order 2, 384^3 FP64 (plane ring)
+        n = 384
+        g = gc.Grid(n, n, n, 1 / n, 1 / n, 1 / n)
+        f = torch.rand(n, n, n, device="cuda", dtype=torch.float64)
+        out = torch.empty_like(f)
+        for _ in range(3):
+            gc.laplacian(f, g, 2, out)
+    elif name == "fvm_256":         # FVM RK4 steps, 256^3 FP32
+        n = 256
+        g = gc.Grid(n, n, n)
+        D = (torch.rand(n, n, n, device="cuda") + 0.5).contiguous()
+        u = torch.rand(n, n, n, device="cuda").contiguous()
+        gc.diffuse(u, g, D, 0.05, 4, gc.RK4)
+    elif name == "batch64_f32":     # FP32 ensemble of 64 members, order 4, 16 steps
+        rng = np.random.default_rng(11)
+        members = []
+        for _ in range(64):
+            side = int(16 * round(64 * 16 ** rng.random() / 16))
+            kap = rng.uniform(0.5, 2.0)
+            lam = 2 * 16 / 3
+            members.append((side, side, 1.0, kap, 0.5 * 2.7853 / (lam * (kap * lam + 2))))
+        b = gc.ChBatch(members, order=4, dtype=torch.float32)
+        for i, (nx, ny, *_) in enumerate(members):
+            b.set_member(i, 0.05 * (2 * rng.random((ny, nx)) - 1))
+        b.run(16)
+    elif name == "ch_f32_4096":     # plain FP32 RK4 CH, 4096^2 (two-column tiles)
+        n = 4096
+        g = gc.Grid(n, n, 1)
+        x = (0.05 * (2 * torch.rand(1, n, n, device="cuda", dtype=torch.float64) - 1)).float()
+        gc.ch_integrate(x, g, gc.CahnHilliardRhs(1.0, 1.0, 2), DT, 32, gc.RK4)
+    else:
+        raise SystemExit(f"unknown case {name}")
+    torch.cuda.synchronize()
+    print(f"case {name}: ok", flush=True)
+
+
 def run_ours(args, rank: int, world: int, local: int):
     import numpy as np
     import torch
@@ -538,11 +586,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
+    ap.add_argument("--case", default=None,
+                    help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
+                         "batch64_f32, ch_f32_4096")
     ap.add_argument("--forms", default="all",
                     help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full "
                          "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
+    if args.case:
+        run_case(args.case)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
     else:
