@@ -173,8 +173,9 @@ struct TmaLayout {
   static constexpr size_t OB = al(sizeof(T) * TX * TY);   // one output-tile field
   static constexpr size_t BUF = YB + (KIN ? YB : 0) + (K12 ? 2 * OB : 0);
   static constexpr size_t OFF_BUF = 128;                  // after the barriers
-  static constexpr size_t OFF_YS = OFF_BUF + 2 * BUF;
-  static constexpr size_t OFF_MS = OFF_YS + (KIN ? YB : 0);
+  // y = psi + a k_prev is formed in place in the k_prev buffer (no separate
+  // y region), which keeps four CTAs per SM in double precision.
+  static constexpr size_t OFF_MS = OFF_BUF + 2 * BUF;
   static constexpr size_t BYTES = OFF_MS + al(sizeof(T) * MX * MY) + 128;  // + alignment slack
   static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(T) * YX * YY * (KIN ? 2 : 1) +
                                                              (K12 ? 2 * sizeof(T) * TX * TY : 0));
@@ -297,14 +298,20 @@ __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
       break;
     }
 
-    // y = psi + a k_prev (stage 1 and Euler read psi directly).
+    // y = psi + a k_prev, in place over k_prev (stage 1 and Euler read psi
+    // directly).  The last RK4 stage first keeps k3 at its own output cells.
     const T* ys = ps;
+    T r_k3[OS];
     if constexpr (KIN) {
-      T* yw = reinterpret_cast<T*>(base + L::OFF_YS);
-      const T* ks = buf_kin(b);
-      for (int e = tid; e < YX * YY; e += kTmaThreads) yw[e] = Ar<T>::add(ps[e], Ar<T>::mul(p.a, ks[e]));
+      T* ks = buf_kin(b);
+      if constexpr (MODE == MODE_RK4_FINAL) {
+#pragma unroll
+        for (int k = 0; k < OS; ++k) r_k3[k] = ks[(ty * OS + k + 2 * R) * YX + (tx + 2 * R)];
+        __syncthreads();
+      }
+      for (int e = tid; e < YX * YY; e += kTmaThreads) ks[e] = Ar<T>::add(ps[e], Ar<T>::mul(p.a, ks[e]));
       __syncthreads();
-      ys = yw;
+      ys = ks;
     }
 
     // Phase 2: mu at mu-row strip [m0, m1), column tx (y column tx + R).
@@ -363,7 +370,7 @@ __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
           p.out[gi] = rhs;
         } else if constexpr (MODE == MODE_RK4_FINAL) {
           const T s14 = Ar<T>::add(r_k1[k], rhs);
-          const T s23 = Ar<T>::add(r_k2[k], buf_kin(b)[yc_idx]);
+          const T s23 = Ar<T>::add(r_k2[k], r_k3[k]);
           p.out[gi] = Ar<T>::add(ps[yc_idx], Ar<T>::add(Ar<T>::mul(p.c6, s14), Ar<T>::mul(p.c3, s23)));
         } else {
           p.out[gi] = Ar<T>::add(ps[yc_idx], Ar<T>::mul(p.c6, rhs));
