@@ -87,6 +87,8 @@ gc_status scratch_get(gc_context* ctx, int slot, size_t bytes, void** out);
 // Validation helpers mirroring the reference contracts.
 gc_status check_grid(const gc_grid* g);
 gc_status require_axes(const gc_grid* g, int radius);
+// Per-axis radii (an axis with radius 0 accepts any extent).
+gc_status require_axes3(const gc_grid* g, int rx, int ry, int rz);
 gc_status check_ctx(gc_context* ctx);
 
 // Stream-ordered building blocks for other parts of the library (no
@@ -224,6 +226,29 @@ template <> struct W<4, 6> {
          : m == 2 || m == 6 ? 169.0 / 60.0
          : m == 3 || m == 5 ? -122.0 / 15.0
                             : 91.0 / 8.0;
+  }
+};
+
+// Kind 3 (third derivative): the reference tables for orders 2 and 4
+// (stencil/ThirdDerivative.hpp:49-84), order 6 the standard central set.
+template <> struct W<3, 2> {
+  static constexpr int R = 2;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 ? -1.0 / 2.0 : m == 1 ? 1.0 : m == 2 ? 0.0 : m == 3 ? -1.0 : 1.0 / 2.0;
+  }
+};
+template <> struct W<3, 4> {
+  static constexpr int R = 3;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 ? 1.0 / 8.0 : m == 1 ? -1.0 : m == 2 ? 13.0 / 8.0 : m == 3 ? 0.0
+         : m == 4 ? -13.0 / 8.0 : m == 5 ? 1.0 : -1.0 / 8.0;
+  }
+};
+template <> struct W<3, 6> {
+  static constexpr int R = 4;
+  static __host__ __device__ constexpr double w(int m) {
+    return m == 0 ? -7.0 / 240.0 : m == 1 ? 3.0 / 10.0 : m == 2 ? -169.0 / 120.0 : m == 3 ? 61.0 / 30.0
+         : m == 4 ? 0.0 : m == 5 ? -61.0 / 30.0 : m == 6 ? 169.0 / 120.0 : m == 7 ? -3.0 / 10.0 : 7.0 / 240.0;
   }
 };
 

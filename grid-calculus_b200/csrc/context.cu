@@ -82,6 +82,14 @@ gc_status require_axes(const gc_grid* g, int radius) {
   return require_axis("z", g->nz, radius);
 }
 
+gc_status require_axes3(const gc_grid* g, int rx, int ry, int rz) {
+  gc_status s = check_grid(g);
+  if (s != GC_OK) return s;
+  if ((s = require_axis("x", g->nx, rx)) != GC_OK) return s;
+  if ((s = require_axis("y", g->ny, ry)) != GC_OK) return s;
+  return require_axis("z", g->nz, rz);
+}
+
 gc_status scratch_get(gc_context* ctx, int slot, size_t bytes, void** out) {
   Scratch& s = ctx->scratch[slot];
   if (s.bytes < bytes) {

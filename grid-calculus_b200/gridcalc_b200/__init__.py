@@ -24,7 +24,7 @@ __all__ = [
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
-    "rkc_stability_bound",
+    "rkc_stability_bound", "partial", "PARTIALS",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -82,6 +82,7 @@ _SIGS = {
     "gc_diffuse_fvm": [_vp, _gp, _i32, _vp, _vp, _dbl, _i32, _i32, C.POINTER(C.c_int64)],
     "gc_d_max_face": [_vp, _gp, _i32, _vp, C.POINTER(C.c_double)],
     "gc_ch_rkc": [_vp, _gp, _i32, C.POINTER(gc_ch_params), _vp, _dbl, C.c_int32, C.c_int32],
+    "gc_partial": [_vp, _gp, _i32, _i32, _i32, _i32, _i32, _vp, _vp],
 }
 
 
@@ -288,6 +289,43 @@ def divergence(vfield, grid: Grid, order: int = 2, out=None, ctx=None):
     _check(lib.gc_divergence(_ctx(ctx), C.byref(grid.c()), _dtype_code(vfield), order,
                              vfield.data_ptr(), out.data_ptr()))
     return out
+
+
+def partial(field, grid: Grid, counts, order: int = 2, out=None, ctx=None):
+    """diff::detail::mixedDerivative<ax, ay, az, Order>
+    (diff/detail/MultiIndexDerivative.hpp:96-137): d^(ax+ay+az) f /
+    dx^ax dy^ay dz^az, counts (ax, ay, az) each 0..4."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    ax, ay, az = counts
+    _check(lib.gc_partial(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order, ax, ay, az,
+                          field.data_ptr(), out.data_ptr()))
+    return out
+
+
+# The reference's 31 named partials (diff/MixedPartial.hpp, ThirdOrder.hpp,
+# FourthOrder.hpp) by their per-axis derivative counts.
+PARTIALS = {
+    "dxx": (2, 0, 0), "dyy": (0, 2, 0), "dzz": (0, 0, 2), "dxy": (1, 1, 0), "dxz": (1, 0, 1), "dyz": (0, 1, 1),
+    "d3dx3": (3, 0, 0), "d3dy3": (0, 3, 0), "d3dz3": (0, 0, 3), "d3dx2dy": (2, 1, 0), "d3dxdy2": (1, 2, 0),
+    "d3dx2dz": (2, 0, 1), "d3dxdz2": (1, 0, 2), "d3dy2dz": (0, 2, 1), "d3dydz2": (0, 1, 2), "d3dxdydz": (1, 1, 1),
+    "d4dx4": (4, 0, 0), "d4dy4": (0, 4, 0), "d4dz4": (0, 0, 4), "d4dx3dy": (3, 1, 0), "d4dxdy3": (1, 3, 0),
+    "d4dx3dz": (3, 0, 1), "d4dxdz3": (1, 0, 3), "d4dy3dz": (0, 3, 1), "d4dydz3": (0, 1, 3),
+    "d4dx2dy2": (2, 2, 0), "d4dx2dz2": (2, 0, 2), "d4dy2dz2": (0, 2, 2), "d4dx2dydz": (2, 1, 1),
+    "d4dxdy2dz": (1, 2, 1), "d4dxdydz2": (1, 1, 2),
+}
+
+
+def _named_partial(name, counts):
+    def op(field, grid: Grid, order: int = 2, out=None, ctx=None):
+        return partial(field, grid, counts, order, out, ctx)
+    op.__name__ = name
+    op.__doc__ = f"diff::{name}<Order>: d^{sum(counts)} f / dx^{counts[0]} dy^{counts[1]} dz^{counts[2]}."
+    return op
+
+
+for _pname, _pcounts in PARTIALS.items():
+    globals()[_pname] = _named_partial(_pname, _pcounts)
 
 
 def biharmonic(field, grid: Grid, order: int = 2, out=None, ctx=None):

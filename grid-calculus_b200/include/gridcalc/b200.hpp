@@ -235,6 +235,65 @@ inline void laplacian(const core::DeviceField<T>& in, core::DeviceField<T>& out)
   b200::check(gc_laplacian(b200::context(), &g, b200::dtype_of<T>(), Order, in.data(), out.data()));
 }
 
+// diff::detail::mixedDerivative<Nx, Ny, Nz, Order>
+// (diff/detail/MultiIndexDerivative.hpp:96-137) and the 31 named partials
+// that forward to it (diff/MixedPartial.hpp, ThirdOrder.hpp, FourthOrder.hpp).
+namespace detail {
+template <int Nx, int Ny, int Nz, int Order>
+inline core::Field<double> mixedDerivative(const core::Field<double>& psi) {
+  return scalar_op(psi, [](const gc_grid* g, const double* in, double* out) {
+    return gc_partial(b200::context(), g, GC_F64, Order, Nx, Ny, Nz, in, out);
+  });
+}
+template <int Nx, int Ny, int Nz, int Order, class T>
+inline void mixedDerivative(const core::DeviceField<T>& in, core::DeviceField<T>& out) {
+  const gc_grid g = in.getGrid().c();
+  b200::check(gc_partial(b200::context(), &g, b200::dtype_of<T>(), Order, Nx, Ny, Nz, in.data(), out.data()));
+}
+}  // namespace detail
+
+#define GRIDCALC_B200_PARTIAL(name, nx, ny, nz)                                         \
+  template <int Order = 2>                                                              \
+  inline core::Field<double> name(const core::Field<double>& psi) {                     \
+    return detail::mixedDerivative<nx, ny, nz, Order>(psi);                             \
+  }                                                                                     \
+  template <int Order = 2, class T>                                                     \
+  inline void name(const core::DeviceField<T>& in, core::DeviceField<T>& out) {         \
+    detail::mixedDerivative<nx, ny, nz, Order>(in, out);                                \
+  }
+GRIDCALC_B200_PARTIAL(dxx, 2, 0, 0)
+GRIDCALC_B200_PARTIAL(dyy, 0, 2, 0)
+GRIDCALC_B200_PARTIAL(dzz, 0, 0, 2)
+GRIDCALC_B200_PARTIAL(dxy, 1, 1, 0)
+GRIDCALC_B200_PARTIAL(dxz, 1, 0, 1)
+GRIDCALC_B200_PARTIAL(dyz, 0, 1, 1)
+GRIDCALC_B200_PARTIAL(d3dx3, 3, 0, 0)
+GRIDCALC_B200_PARTIAL(d3dy3, 0, 3, 0)
+GRIDCALC_B200_PARTIAL(d3dz3, 0, 0, 3)
+GRIDCALC_B200_PARTIAL(d3dx2dy, 2, 1, 0)
+GRIDCALC_B200_PARTIAL(d3dxdy2, 1, 2, 0)
+GRIDCALC_B200_PARTIAL(d3dx2dz, 2, 0, 1)
+GRIDCALC_B200_PARTIAL(d3dxdz2, 1, 0, 2)
+GRIDCALC_B200_PARTIAL(d3dy2dz, 0, 2, 1)
+GRIDCALC_B200_PARTIAL(d3dydz2, 0, 1, 2)
+GRIDCALC_B200_PARTIAL(d3dxdydz, 1, 1, 1)
+GRIDCALC_B200_PARTIAL(d4dx4, 4, 0, 0)
+GRIDCALC_B200_PARTIAL(d4dy4, 0, 4, 0)
+GRIDCALC_B200_PARTIAL(d4dz4, 0, 0, 4)
+GRIDCALC_B200_PARTIAL(d4dx3dy, 3, 1, 0)
+GRIDCALC_B200_PARTIAL(d4dxdy3, 1, 3, 0)
+GRIDCALC_B200_PARTIAL(d4dx3dz, 3, 0, 1)
+GRIDCALC_B200_PARTIAL(d4dxdz3, 1, 0, 3)
+GRIDCALC_B200_PARTIAL(d4dy3dz, 0, 3, 1)
+GRIDCALC_B200_PARTIAL(d4dydz3, 0, 1, 3)
+GRIDCALC_B200_PARTIAL(d4dx2dy2, 2, 2, 0)
+GRIDCALC_B200_PARTIAL(d4dx2dz2, 2, 0, 2)
+GRIDCALC_B200_PARTIAL(d4dy2dz2, 0, 2, 2)
+GRIDCALC_B200_PARTIAL(d4dx2dydz, 2, 1, 1)
+GRIDCALC_B200_PARTIAL(d4dxdy2dz, 1, 2, 1)
+GRIDCALC_B200_PARTIAL(d4dxdydz2, 1, 1, 2)
+#undef GRIDCALC_B200_PARTIAL
+
 // diff::biharmonic<Order> / d4 (diff/Biharmonic.hpp:48-119).
 template <int Order = 2>
 inline core::Field<double> biharmonic(const core::Field<double>& field) {

@@ -117,6 +117,15 @@ GC_API gc_status gc_divergence(gc_context* ctx, const gc_grid* g, gc_dtype dt, i
 /* diff::biharmonic<Order> / diff::d4 (diff/Biharmonic.hpp:48-119). */
 GC_API gc_status gc_biharmonic(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
                                const void* in, void* out);
+
+/* diff::detail::mixedDerivative<ax, ay, az, Order> (diff/detail/MultiIndexDerivative.hpp:96-137):
+ * d^(ax+ay+az) in / dx^ax dy^ay dz^az, each count 0..4.  The reference's 31
+ * named partials forward here: dxx dyy dzz dxy dxz dyz (diff/MixedPartial.hpp),
+ * d3dx3 ... d3dxdydz (diff/ThirdOrder.hpp), d4dx4 ... d4dxdydz2
+ * (diff/FourthOrder.hpp).  Orders 2 and 4 as the reference, 6 added.  Each
+ * axis is checked against its own stencil radius (0 for a count of 0). */
+GC_API gc_status gc_partial(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order, int ax, int ay, int az,
+                            const void* in, void* out);
 /* fvm::cellLaplacian (fvm/CellLaplacian.hpp:91-143).  Checks D > 0 first;
  * on violation returns GC_ERR_NONPOSITIVE_D and the first flat index in
  * *bad_index (may be NULL). */

@@ -155,6 +155,49 @@ int oc_laplacian(int order, int nx, int ny, int nz, double hx, double hy, double
   return 0;
 }
 
+/* ---- diff/detail/MultiIndexDerivative.hpp:96-137: d^(ax+ay+az) f / dx^ax dy^ay dz^az
+   (the 31 named partials of diff/MixedPartial.hpp, ThirdOrder.hpp and
+   FourthOrder.hpp forward here).  scale = 1 / h_a, divided once per
+   derivative on each axis in x, y, z order; per point
+   sum += (wx * (wy * wz)) * f over z taps, then y taps, then x taps, from
+   0.0; result = sum * scale.  An axis with count 0 is the single tap 1.0. */
+int oc_mixed(int ax, int ay, int az, int order, int nx, int ny, int nz, double hx, double hy, double hz,
+             const double* f, double* out) {
+  double wx[2 * MAXR + 1], wy[2 * MAXR + 1], wz[2 * MAXR + 1];
+  int rx = 0, ry = 0, rz = 0;
+  if (ax < 0 || ax > 4 || ay < 0 || ay > 4 || az < 0 || az > 4) {
+    snprintf(g_err, sizeof g_err, "mixed: derivative counts must be in 0..4");
+    return 1;
+  }
+  if (ax) rx = oc_weights(ax, order, wx); else wx[0] = 1.0;
+  if (ay) ry = oc_weights(ay, order, wy); else wy[0] = 1.0;
+  if (az) rz = oc_weights(az, order, wz); else wz[0] = 1.0;
+  if (rx < 0 || ry < 0 || rz < 0) {
+    snprintf(g_err, sizeof g_err, "mixed: unsupported order %d", order);
+    return 1;
+  }
+  if (require_axis("x", nx, rx) || require_axis("y", ny, ry) || require_axis("z", nz, rz)) return 1;
+  double scale = 1.0;
+  for (int n = 0; n < ax; ++n) scale /= hx;
+  for (int n = 0; n < ay; ++n) scale /= hy;
+  for (int n = 0; n < az; ++n) scale /= hz;
+  wrap3 w; wrap3_init(&w, nx, ny, nz);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double sum = 0.0;
+        for (int mz = 0; mz <= 2 * rz; ++mz)
+          for (int my = 0; my <= 2 * ry; ++my) {
+            const double wyz = wy[my] * wz[mz];
+            for (int mx = 0; mx <= 2 * rx; ++mx)
+              sum += wx[mx] * wyz * f[lin(&w, i + mx - rx, j + my - ry, k + mz - rz)];
+          }
+        out[(size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)] = sum * scale;
+      }
+  wrap3_free(&w);
+  return 0;
+}
+
 /* ---- diff/Gradient.hpp:43-74 (scalar -> vector; output as three planes) */
 int oc_gradient(int order, int nx, int ny, int nz, double hx, double hy, double hz,
                 const double* f, double* out3) {

@@ -41,6 +41,9 @@ int oc_gradient(int order, int nx, int ny, int nz, double hx, double hy, double 
                 const double* in, double* out3);
 int oc_divergence(int order, int nx, int ny, int nz, double hx, double hy, double hz,
                   const double* in3, double* out);
+/* diff/detail/MultiIndexDerivative.hpp:96-137 (the 31 named partials). */
+int oc_mixed(int ax, int ay, int az, int order, int nx, int ny, int nz, double hx, double hy, double hz,
+             const double* f, double* out);
 int oc_biharmonic(int order, int nx, int ny, int nz, double hx, double hy, double hz,
                   const double* in, double* out);
 /* Returns 0, 1 (axis extent) or 2 (D not strictly positive; *bad_index set). */

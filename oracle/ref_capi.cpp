@@ -20,7 +20,10 @@
 #include <gridcalc/diff/Biharmonic.hpp>
 #include <gridcalc/diff/Divergence.hpp>
 #include <gridcalc/diff/Gradient.hpp>
+#include <gridcalc/diff/FourthOrder.hpp>
 #include <gridcalc/diff/Laplacian.hpp>
+#include <gridcalc/diff/MixedPartial.hpp>
+#include <gridcalc/diff/ThirdOrder.hpp>
 #include <gridcalc/func/Functional.hpp>
 #include <gridcalc/func/Integrate.hpp>
 #include <gridcalc/fvm/CellLaplacian.hpp>
@@ -92,9 +95,62 @@ Field<double> chRhs(const Field<double>& psi, double M, double kappa) {
   }
 }
 
+// The 31 named partials of diff/MixedPartial.hpp, ThirdOrder.hpp and
+// FourthOrder.hpp, keyed by their per-axis derivative counts.
+template <int O>
+Field<double> namedPartial(int ax, int ay, int az, const Field<double>& f) {
+  namespace d = gridcalc::diff;
+  const int key = ax * 100 + ay * 10 + az;
+  switch (key) {
+    case 200: return d::dxx<O>(f);
+    case 20: return d::dyy<O>(f);
+    case 2: return d::dzz<O>(f);
+    case 110: return d::dxy<O>(f);
+    case 101: return d::dxz<O>(f);
+    case 11: return d::dyz<O>(f);
+    case 300: return d::d3dx3<O>(f);
+    case 30: return d::d3dy3<O>(f);
+    case 3: return d::d3dz3<O>(f);
+    case 210: return d::d3dx2dy<O>(f);
+    case 120: return d::d3dxdy2<O>(f);
+    case 201: return d::d3dx2dz<O>(f);
+    case 102: return d::d3dxdz2<O>(f);
+    case 21: return d::d3dy2dz<O>(f);
+    case 12: return d::d3dydz2<O>(f);
+    case 111: return d::d3dxdydz<O>(f);
+    case 400: return d::d4dx4<O>(f);
+    case 40: return d::d4dy4<O>(f);
+    case 4: return d::d4dz4<O>(f);
+    case 310: return d::d4dx3dy<O>(f);
+    case 130: return d::d4dxdy3<O>(f);
+    case 301: return d::d4dx3dz<O>(f);
+    case 103: return d::d4dxdz3<O>(f);
+    case 31: return d::d4dy3dz<O>(f);
+    case 13: return d::d4dydz3<O>(f);
+    case 220: return d::d4dx2dy2<O>(f);
+    case 202: return d::d4dx2dz2<O>(f);
+    case 22: return d::d4dy2dz2<O>(f);
+    case 211: return d::d4dx2dydz<O>(f);
+    case 121: return d::d4dxdy2dz<O>(f);
+    case 112: return d::d4dxdydz2<O>(f);
+  }
+  throw std::invalid_argument("ref: no named partial with these derivative counts");
+}
+
 }  // namespace
 
 extern "C" {
+
+int ref_mixed(int ax, int ay, int az, int order, int nx, int ny, int nz, double hx, double hy, double hz,
+              const double* in, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, in);
+    if (order == 2) store(namedPartial<2>(ax, ay, az, f), out);
+    else if (order == 4) store(namedPartial<4>(ax, ay, az, f), out);
+    else throw std::invalid_argument("ref: partial order must be 2 or 4");
+  });
+}
 
 const char* ref_last_error(void) { return g_err.c_str(); }
 

@@ -7,7 +7,10 @@
 #include <gridcalc/core/Field.hpp>
 #include <gridcalc/core/Grid.hpp>
 #include <gridcalc/diff/Gradient.hpp>
+#include <gridcalc/diff/FourthOrder.hpp>
 #include <gridcalc/diff/Laplacian.hpp>
+#include <gridcalc/diff/MixedPartial.hpp>
+#include <gridcalc/diff/ThirdOrder.hpp>
 #include <gridcalc/func/Functional.hpp>
 #include <gridcalc/func/Integrate.hpp>
 #include <gridcalc/fvm/CellLaplacian.hpp>
@@ -106,6 +109,25 @@ int main() {
     const double F1 = gridcalc::func::evaluate(psi, gridcalc::func::FreeEnergy{1.0});
     const double m1 = gridcalc::func::integrate(psi, gridcalc::func::Kahan{});
     require(F1 < F0 && std::abs(m1 - m0) < 1e-10, "cahn-hilliard energy decay and mass");
+  }
+  {  // named partials on sin x sin y sin z (phase_8_test.cpp style): dxy, d3dxdydz, d4dx2dy2
+    const int N = 32;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<double> f(g, [](double x, double y, double z) { return std::sin(x) * std::sin(y) * std::sin(z); });
+    const auto fxy = gridcalc::diff::dxy<4>(f);
+    const auto fxyz = gridcalc::diff::d3dxdydz<4>(f);
+    const auto fxxyy = gridcalc::diff::d4dx2dy2<4>(f);
+    double e2 = 0, e3 = 0, e4 = 0;
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const double x = i * h, y = j * h, z = k * h;
+          e2 = std::max(e2, std::abs(fxy(i, j, k) - std::cos(x) * std::cos(y) * std::sin(z)));
+          e3 = std::max(e3, std::abs(fxyz(i, j, k) - std::cos(x) * std::cos(y) * std::cos(z)));
+          e4 = std::max(e4, std::abs(fxxyy(i, j, k) - std::sin(x) * std::sin(y) * std::sin(z)));
+        }
+    require(e2 < 2e-4 && e3 < 3e-4 && e4 < 1e-4, "named partials dxy, d3dxdydz, d4dx2dy2");
   }
   std::printf("version %s\n", gridcalc::version());
   return 0;

@@ -18,6 +18,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 import oracle_lib  # noqa: E402
 
+PARTIALS = oracle_lib.PARTIALS
+# Grids and orders the partials are stored for (all 31 each).
+PARTIAL_CASES = [("aniso3d", 4), ("flat2d", 2)]
+
 # (name, shape (nz, ny, nx), h)
 GRIDS = [
     ("aniso3d", (8, 10, 12), (0.3, 0.25, 0.5)),
@@ -50,6 +54,10 @@ def main() -> None:
         out[f"{name}/free_energy"] = np.array(ref.ch_free_energy(f, 0.8, h))
         out[f"{name}/gradient_energy"] = np.array(ref.ch_gradient_energy(f, h))
         out[f"{name}/mean"] = np.array(ref.ch_mean(f, h))
+        for pname, porder in PARTIAL_CASES:
+            if pname == name:
+                for c in PARTIALS:
+                    out[f"{name}/partial{c[0]}{c[1]}{c[2]}_{porder}"] = ref.mixed(c, porder, f, h)
 
     # Cahn-Hilliard trajectories on a 2-D grid (h = 1, stable dt).
     psi0 = 0.05 * (2.0 * rng.random((1, 24, 24)) - 1.0)

@@ -24,6 +24,20 @@ _d = C.c_double
 _i = C.c_int
 
 
+# Per-axis derivative counts (x, y, z) of the reference's 31 named partials
+# (diff/MixedPartial.hpp, ThirdOrder.hpp, FourthOrder.hpp), with their names.
+PARTIAL_NAMES = {
+    (2, 0, 0): "dxx", (0, 2, 0): "dyy", (0, 0, 2): "dzz", (1, 1, 0): "dxy", (1, 0, 1): "dxz", (0, 1, 1): "dyz",
+    (3, 0, 0): "d3dx3", (0, 3, 0): "d3dy3", (0, 0, 3): "d3dz3", (2, 1, 0): "d3dx2dy", (1, 2, 0): "d3dxdy2",
+    (2, 0, 1): "d3dx2dz", (1, 0, 2): "d3dxdz2", (0, 2, 1): "d3dy2dz", (0, 1, 2): "d3dydz2", (1, 1, 1): "d3dxdydz",
+    (4, 0, 0): "d4dx4", (0, 4, 0): "d4dy4", (0, 0, 4): "d4dz4", (3, 1, 0): "d4dx3dy", (1, 3, 0): "d4dxdy3",
+    (3, 0, 1): "d4dx3dz", (1, 0, 3): "d4dxdz3", (0, 3, 1): "d4dy3dz", (0, 1, 3): "d4dydz3", (2, 2, 0): "d4dx2dy2",
+    (2, 0, 2): "d4dx2dz2", (0, 2, 2): "d4dy2dz2", (2, 1, 1): "d4dx2dydz", (1, 2, 1): "d4dxdy2dz",
+    (1, 1, 2): "d4dxdydz2",
+}
+PARTIALS = list(PARTIAL_NAMES)
+
+
 def _ensure_built() -> None:
     src = os.path.join(ORACLE_DIR, "gc_oracle.c")
     if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
@@ -68,6 +82,14 @@ class _Lib:
         out_shape = (3,) + shape if name == "gradient" else shape
         out = np.zeros(out_shape)
         self._rc(self._f(name)(order, *self._g(shape, h), _ptr(f), _ptr(out)))
+        return out
+
+    def mixed(self, counts, order: int, f: np.ndarray, h=(1.0, 1.0, 1.0)) -> np.ndarray:
+        """d^(ax+ay+az) f / dx^ax dy^ay dz^az on an (nz, ny, nx) array."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        out = np.zeros(f.shape)
+        ax, ay, az = counts
+        self._rc(self._f("mixed")(ax, ay, az, order, *self._g(f.shape, h), _ptr(f), _ptr(out)))
         return out
 
     def cell_laplacian(self, psi, D, h=(1.0, 1.0, 1.0)):

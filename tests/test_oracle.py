@@ -50,6 +50,15 @@ def test_oracle_matches_reference_golden_operators(oracle, golden):
         assert oracle.ch_mean(f, h) == float(golden[f"{g}/mean"])
 
 
+def test_oracle_matches_reference_golden_partials(oracle, golden):
+    """diff/detail/MultiIndexDerivative.hpp: the 31 named partials, bit for bit."""
+    for name, order in (("aniso3d", 4), ("flat2d", 2)):   # the cases tests/golden/make_golden.py stores
+        f, h = golden[f"{name}/f"], tuple(golden[f"{name}/h"])
+        for c in oracle_lib.PARTIALS:
+            got = oracle.mixed(c, order, f, h)
+            assert np.array_equal(got, golden[f"{name}/partial{c[0]}{c[1]}{c[2]}_{order}"]), (name, c, order)
+
+
 def test_oracle_matches_reference_golden_trajectories(oracle, golden):
     psi0 = golden["ch2d/psi0"]
     for order in (2, 4):
