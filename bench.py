@@ -218,6 +218,18 @@ def fourier_field(n, seed, device, dtype):
     return f.to(dtype), lap, bih, grad
 
 
+def spectral_partial(f, counts):
+    """d^(ax+ay+az) f / dx^ax dy^ay dz^az of a periodic field on the unit cube
+    by FFT (exact for the band-limited Fourier-mode fields used here)."""
+    import torch
+    n = f.shape[-1]
+    k = torch.fft.fftfreq(n, d=1.0 / n, device=f.device, dtype=torch.float64) * 2 * torch.pi
+    kr = torch.fft.rfftfreq(n, d=1.0 / n, device=f.device, dtype=torch.float64) * 2 * torch.pi
+    ax, ay, az = counts
+    mult = ((1j * kr[None, None, :]) ** ax) * ((1j * k[None, :, None]) ** ay) * ((1j * k[:, None, None]) ** az)
+    return torch.fft.irfftn(torch.fft.rfftn(f) * mult, s=f.shape)
+
+
 def form_operators(gc, peak):
     import torch
     out = {}
@@ -249,6 +261,13 @@ def form_operators(gc, peak):
                 rec(f"biharmonic{order}", 2, lambda: gc.biharmonic(f, g, order, o), o, bih_a)
                 rec(f"gradient{order}", 4, lambda: gc.gradient(f, g, order, o3), o3, grad_a)
                 rec(f"divergence{order}", 4, lambda: gc.divergence(vec, g, order, o), o, div_a)
+            # Mixed and higher partials (the named dxy, d3dxdydz, d4dx2dy2), checked
+            # against the spectral derivative of the band-limited field.
+            for counts, pname in (((1, 1, 0), "dxy"), ((1, 1, 1), "d3dxdydz"), ((2, 2, 0), "d4dx2dy2")):
+                exact = spectral_partial(f64, counts)
+                for order in (2, 4, 6):
+                    rec(f"{pname}{order}", 2, lambda: gc.partial(f, g, counts, order, o), o, exact)
+                del exact
             ms = _cuda_time(lambda: gc.integrate(f, g))
             gbs = es * cells / ms / 1e6
             res["integrate"] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak,
@@ -258,7 +277,7 @@ def form_operators(gc, peak):
         del f64, lap_a, bih_a, grad_a, vec64, div_a
         torch.cuda.empty_cache()
     return {"workload": "operator sweep, 64 Fourier modes |k|<=16 on the unit cube (seed 2; vector field seeds 3,4,5)",
-            "bytes_per_cell": "laplacian/biharmonic 2s, gradient/divergence 4s, integrate 1s (s = 8 or 4)",
+            "bytes_per_cell": "laplacian/biharmonic/partials 2s, gradient/divergence 4s, integrate 1s (s = 8 or 4)",
             "results": out}
 
 
