@@ -514,6 +514,30 @@ gc_status run_op(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order, cons
   return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: unknown dtype");
 }
 
+// Rank-2 forms (diff/Gradient.hpp:100-137, diff/Divergence.hpp:100-135).
+// A matrix field is nine planes, plane 3*row + col holding M(row, col).
+// Row `comp` of grad v is the vector-gradient kernel over plane `comp` of v;
+// component `comp` of div M is the vector-divergence kernel over the three
+// planes of row `comp`.  Both reproduce the reference's per-component sums
+// exactly, and the three passes move exactly the rank-2 operator's bytes
+// (every input plane read once, every output plane written once), so a
+// fused kernel would save nothing but two launches.
+template <int OP>
+gc_status run_rank2(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order, const void* in, void* out) {
+  static_assert(OP == OP_GRAD || OP == OP_DIV, "rank-2 forms exist for gradient and divergence");
+  // The first pass validates the context, grid, order, dtype and pointers.
+  gc_status s = run_op<OP>(ctx, g, dt, order, in, out);
+  if (s != GC_OK) return s;
+  const size_t plane = cells(g) * dtype_size(dt);
+  const size_t in_row = (OP == OP_GRAD ? 1 : 3) * plane, out_row = (OP == OP_GRAD ? 3 : 1) * plane;
+  for (int comp = 1; comp < 3; ++comp) {
+    s = run_op<OP>(ctx, g, dt, order, static_cast<const char*>(in) + comp * in_row,
+                   static_cast<char*>(out) + comp * out_row);
+    if (s != GC_OK) return s;
+  }
+  return GC_OK;
+}
+
 }  // namespace
 }  // namespace gcb
 
@@ -539,6 +563,16 @@ GC_API gc_status gc_divergence(gc_context* ctx, const gc_grid* g, gc_dtype dt, i
 GC_API gc_status gc_biharmonic(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
                                const void* in, void* out) {
   return run_op<OP_BIH>(ctx, g, dt, order, in, out);
+}
+
+GC_API gc_status gc_gradient_vec(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                                 const void* in3, void* out9) {
+  return run_rank2<OP_GRAD>(ctx, g, dt, order, in3, out9);
+}
+
+GC_API gc_status gc_divergence_mat(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                                   const void* in9, void* out3) {
+  return run_rank2<OP_DIV>(ctx, g, dt, order, in9, out3);
 }
 
 }  // extern "C"

@@ -83,6 +83,8 @@ _SIGS = {
     "gc_d_max_face": [_vp, _gp, _i32, _vp, C.POINTER(C.c_double)],
     "gc_ch_rkc": [_vp, _gp, _i32, C.POINTER(gc_ch_params), _vp, _dbl, C.c_int32, C.c_int32],
     "gc_partial": [_vp, _gp, _i32, _i32, _i32, _i32, _i32, _vp, _vp],
+    "gc_gradient_vec": [_vp, _gp, _i32, _i32, _vp, _vp],
+    "gc_divergence_mat": [_vp, _gp, _i32, _i32, _vp, _vp],
 }
 
 
@@ -272,9 +274,24 @@ def laplacian(field, grid: Grid, order: int = 2, out=None, ctx=None):
     return out
 
 
+def _matrix_like_grid(t, grid: Grid):
+    import torch
+    return torch.empty((3, 3) + grid.shape, dtype=t.dtype, device=t.device)
+
+
 def gradient(field, grid: Grid, order: int = 2, out=None, ctx=None):
-    """diff::gradient<Order> scalar -> vector (diff/Gradient.hpp:43-74); out
-    has shape (3, nz, ny, nx)."""
+    """diff::gradient<Order>, overloaded on the field's rank like the
+    reference.  Scalar -> vector (diff/Gradient.hpp:43-74): out has shape
+    (3, nz, ny, nx).  Vector (3 * cells values) -> matrix
+    (diff/Gradient.hpp:100-137): out has shape (3, 3, nz, ny, nx) with
+    out[row, col] = d_col v_row."""
+    if field.numel() == 3 * grid.size and grid.size > 0:
+        _require(field, grid, 3)
+        out = _matrix_like_grid(field, grid) if out is None else out
+        _require(out, grid, 9)
+        _check(lib.gc_gradient_vec(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order,
+                                   field.data_ptr(), out.data_ptr()))
+        return out
     _require(field, grid)
     out = _empty_like_grid(field, grid, 3) if out is None else out
     _check(lib.gc_gradient(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), order,
@@ -283,7 +300,17 @@ def gradient(field, grid: Grid, order: int = 2, out=None, ctx=None):
 
 
 def divergence(vfield, grid: Grid, order: int = 2, out=None, ctx=None):
-    """diff::divergence<Order> vector -> scalar (diff/Divergence.hpp:43-74)."""
+    """diff::divergence<Order>, overloaded on the field's rank like the
+    reference.  Vector -> scalar (diff/Divergence.hpp:43-74).  Matrix
+    (9 * cells values, [row, col] planes) -> vector
+    (diff/Divergence.hpp:100-135): out[row] = sum over col of d_col M[row, col]."""
+    if vfield.numel() == 9 * grid.size and grid.size > 0:
+        _require(vfield, grid, 9)
+        out = _empty_like_grid(vfield, grid, 3) if out is None else out
+        _require(out, grid, 3)
+        _check(lib.gc_divergence_mat(_ctx(ctx), C.byref(grid.c()), _dtype_code(vfield), order,
+                                     vfield.data_ptr(), out.data_ptr()))
+        return out
     _require(vfield, grid, 3)
     out = _empty_like_grid(vfield, grid) if out is None else out
     _check(lib.gc_divergence(_ctx(ctx), C.byref(grid.c()), _dtype_code(vfield), order,

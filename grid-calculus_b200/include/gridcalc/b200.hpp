@@ -95,6 +95,7 @@ namespace core {
 
 #ifdef GRIDCALC_B200_HAVE_EIGEN
 using Vec3d = Eigen::Vector3d;
+using Mat3d = Eigen::Matrix3d;
 #else
 // Stand-in for Eigen::Vector3d when Eigen is not on the include path.
 class Vec3d {
@@ -106,6 +107,17 @@ class Vec3d {
   double squaredNorm() const { return v_[0] * v_[0] + v_[1] * v_[1] + v_[2] * v_[2]; }
  private:
   double v_[3];
+};
+
+// Stand-in for Eigen::Matrix3d: M(row, col), zero-initialised.
+class Mat3d {
+ public:
+  Mat3d() : m_{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0} {}
+  double& operator()(int r, int c) { return m_[3 * r + c]; }
+  const double& operator()(int r, int c) const { return m_[3 * r + c]; }
+  double trace() const { return m_[0] + m_[4] + m_[8]; }
+ private:
+  double m_[9];
 };
 #endif
 
@@ -335,6 +347,49 @@ inline core::Field<double> divergence(const core::Field<core::Vec3d>& vfield) {
   const gc_grid g = grid.c();
   b200::check(gc_divergence(b200::context(), &g, GC_F64, Order, in.data(), out.data()));
   return out.toHost();
+}
+
+// diff::gradient<Order>, Vec3d -> Mat3d (diff/Gradient.hpp:100-137):
+// M(row, col) = d_col v_row.
+template <int Order = 2>
+inline core::Field<core::Mat3d> gradient(const core::Field<core::Vec3d>& vfield) {
+  const core::Grid& grid = vfield.getGrid();
+  const size_t n = grid.getSize();
+  std::vector<double> planes(3 * n);
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) planes[c * n + i] = vfield.data()[i](c);
+  core::DeviceField<double> in(grid, 3), out(grid, 9);
+  in.upload(planes.data());
+  const gc_grid g = grid.c();
+  b200::check(gc_gradient_vec(b200::context(), &g, GC_F64, Order, in.data(), out.data()));
+  std::vector<double> m(9 * n);
+  out.download(m.data());
+  core::Field<core::Mat3d> r(grid);
+  for (size_t i = 0; i < n; ++i)
+    for (int row = 0; row < 3; ++row)
+      for (int col = 0; col < 3; ++col) r.data()[i](row, col) = m[(3 * row + col) * n + i];
+  return r;
+}
+
+// diff::divergence<Order>, Mat3d -> Vec3d (diff/Divergence.hpp:100-135):
+// (div M)_row = sum over col of d_col M(row, col).
+template <int Order = 2>
+inline core::Field<core::Vec3d> divergence(const core::Field<core::Mat3d>& mfield) {
+  const core::Grid& grid = mfield.getGrid();
+  const size_t n = grid.getSize();
+  std::vector<double> m(9 * n);
+  for (size_t i = 0; i < n; ++i)
+    for (int row = 0; row < 3; ++row)
+      for (int col = 0; col < 3; ++col) m[(3 * row + col) * n + i] = mfield.data()[i](row, col);
+  core::DeviceField<double> in(grid, 9), out(grid, 3);
+  in.upload(m.data());
+  const gc_grid g = grid.c();
+  b200::check(gc_divergence_mat(b200::context(), &g, GC_F64, Order, in.data(), out.data()));
+  std::vector<double> planes(3 * n);
+  out.download(planes.data());
+  core::Field<core::Vec3d> r(grid);
+  for (size_t i = 0; i < n; ++i) r.data()[i] = core::Vec3d(planes[i], planes[n + i], planes[2 * n + i]);
+  return r;
 }
 
 }  // namespace diff

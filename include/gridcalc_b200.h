@@ -114,6 +114,15 @@ GC_API gc_status gc_gradient(gc_context* ctx, const gc_grid* g, gc_dtype dt, int
 /* diff::divergence<Order>, vector -> scalar (diff/Divergence.hpp:43-74). */
 GC_API gc_status gc_divergence(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
                                const void* in3, void* out);
+/* diff::gradient<Order>, Vec3d -> Mat3d (diff/Gradient.hpp:100-137).  in3 is
+ * three planes (x, y, z components); out9 is nine planes, plane 3*row + col
+ * holding M(row, col) = d_col v_row. */
+GC_API gc_status gc_gradient_vec(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                                 const void* in3, void* out9);
+/* diff::divergence<Order>, Mat3d -> Vec3d (diff/Divergence.hpp:100-135):
+ * (div M)_row = sum over col of d_col M(row, col), same plane layouts. */
+GC_API gc_status gc_divergence_mat(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
+                                   const void* in9, void* out3);
 /* diff::biharmonic<Order> / diff::d4 (diff/Biharmonic.hpp:48-119). */
 GC_API gc_status gc_biharmonic(gc_context* ctx, const gc_grid* g, gc_dtype dt, int order,
                                const void* in, void* out);

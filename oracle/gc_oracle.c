@@ -254,6 +254,31 @@ int oc_divergence(int order, int nx, int ny, int nz, double hx, double hy, doubl
   return 0;
 }
 
+/* ---- diff/Gradient.hpp:100-137 (rank-2: Vec3d -> Mat3d).  Row `comp` of
+ * M = grad v is the scalar gradient of component `comp`, with the same taps,
+ * zero-initialised sums and 1/h scaling, so each row is one scalar pass.
+ * Layout: three input planes (x, y, z); nine output planes, plane
+ * 3*comp + axis holding M(comp, axis) = d_axis v_comp. */
+int oc_gradient_vec(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                    const double* v3, double* out9) {
+  const size_t n = (size_t)nx * ny * nz;
+  for (int comp = 0; comp < 3; ++comp)
+    if (oc_gradient(order, nx, ny, nz, hx, hy, hz, v3 + comp * n, out9 + 3 * comp * n)) return 1;
+  return 0;
+}
+
+/* ---- diff/Divergence.hpp:100-135 (rank-lowering: Mat3d -> Vec3d).
+ * (div M)_comp = d_x M(comp,0) + d_y M(comp,1) + d_z M(comp,2), summed as
+ * (dx/hx + dy/hy) + dz/hz exactly like the vector divergence, so component
+ * `comp` is the vector divergence of row `comp` (planes 3*comp .. 3*comp+2). */
+int oc_divergence_mat(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                      const double* m9, double* out3) {
+  const size_t n = (size_t)nx * ny * nz;
+  for (int comp = 0; comp < 3; ++comp)
+    if (oc_divergence(order, nx, ny, nz, hx, hy, hz, m9 + 3 * comp * n, out3 + comp * n)) return 1;
+  return 0;
+}
+
 /* ---- diff/Biharmonic.hpp:48-104 */
 int oc_biharmonic(int order, int nx, int ny, int nz, double hx, double hy, double hz,
                   const double* f, double* out) {

@@ -41,6 +41,12 @@ int oc_gradient(int order, int nx, int ny, int nz, double hx, double hy, double 
                 const double* in, double* out3);
 int oc_divergence(int order, int nx, int ny, int nz, double hx, double hy, double hz,
                   const double* in3, double* out);
+/* diff/Gradient.hpp:100-137: Vec3d (3 planes) -> Mat3d (9 planes, 3*row + col). */
+int oc_gradient_vec(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                    const double* v3, double* out9);
+/* diff/Divergence.hpp:100-135: Mat3d (9 planes, 3*row + col) -> Vec3d (3 planes). */
+int oc_divergence_mat(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                      const double* m9, double* out3);
 /* diff/detail/MultiIndexDerivative.hpp:96-137 (the 31 named partials). */
 int oc_mixed(int ax, int ay, int az, int order, int nx, int ny, int nz, double hx, double hy, double hz,
              const double* f, double* out);

@@ -36,6 +36,7 @@ namespace {
 
 using gridcalc::core::Field;
 using gridcalc::core::Grid;
+using gridcalc::core::Mat3d;
 using gridcalc::core::Vec3d;
 namespace ch = gridcalc::examples::cahn_hilliard;
 
@@ -194,6 +195,46 @@ int ref_divergence(int order, int nx, int ny, int nz, double hx, double hy, doub
     if (order == 2) store(gridcalc::diff::divergence<2>(v), out);
     else if (order == 4) store(gridcalc::diff::divergence<4>(v), out);
     else throw std::invalid_argument("ref: divergence order must be 2 or 4");
+  });
+}
+
+// Matrix fields cross this boundary as nine planes, plane 3*row + col
+// holding M(row, col); diff::gradient(Field<Vec3d>) puts d_col v_row there.
+int ref_gradient_vec(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                     const double* in3, double* out9) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<Vec3d> v(g);
+    const std::size_t n = g.getSize();
+    for (std::size_t i = 0; i < n; ++i) v.data()[i] = Vec3d(in3[i], in3[n + i], in3[2 * n + i]);
+    Field<Mat3d> r(g);
+    if (order == 2) r = gridcalc::diff::gradient<2>(v);
+    else if (order == 4) r = gridcalc::diff::gradient<4>(v);
+    else throw std::invalid_argument("ref: gradient order must be 2 or 4");
+    for (std::size_t i = 0; i < n; ++i)
+      for (int row = 0; row < 3; ++row)
+        for (int col = 0; col < 3; ++col) out9[(3 * row + col) * n + i] = r.data()[i](row, col);
+  });
+}
+
+int ref_divergence_mat(int order, int nx, int ny, int nz, double hx, double hy, double hz,
+                       const double* in9, double* out3) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    Field<Mat3d> m(g);
+    const std::size_t n = g.getSize();
+    for (std::size_t i = 0; i < n; ++i)
+      for (int row = 0; row < 3; ++row)
+        for (int col = 0; col < 3; ++col) m.data()[i](row, col) = in9[(3 * row + col) * n + i];
+    Field<Vec3d> r(g);
+    if (order == 2) r = gridcalc::diff::divergence<2>(m);
+    else if (order == 4) r = gridcalc::diff::divergence<4>(m);
+    else throw std::invalid_argument("ref: divergence order must be 2 or 4");
+    for (std::size_t i = 0; i < n; ++i) {
+      out3[i] = r.data()[i](0);
+      out3[n + i] = r.data()[i](1);
+      out3[2 * n + i] = r.data()[i](2);
+    }
   });
 }
 

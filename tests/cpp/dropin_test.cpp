@@ -129,6 +129,28 @@ int main() {
         }
     require(e2 < 2e-4 && e3 < 3e-4 && e4 < 1e-4, "named partials dxy, d3dxdydz, d4dx2dy2");
   }
+  {  // rank-2 forms (vector_tensor_test.cpp): trace(grad v) == div v, div(grad v) ~ -2 v
+    const int N = 32;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<Vec3d> v(g);
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const double x = i * h, y = j * h, z = k * h;
+          v(i, j, k) = Vec3d(std::sin(x) * std::cos(y), std::sin(y) * std::cos(z), std::sin(z) * std::cos(x));
+        }
+    const Field<gridcalc::core::Mat3d> M = gridcalc::diff::gradient(v);
+    const Field<double> div = gridcalc::diff::divergence(v);
+    const Field<Vec3d> lap = gridcalc::diff::divergence(M);
+    double dtr = 0, elap = 0;
+    for (size_t i = 0; i < v.size(); ++i) {
+      const auto& m = M.data()[i];
+      dtr = std::max(dtr, std::abs((m(0, 0) + m(1, 1)) + m(2, 2) - div.data()[i]));
+      for (int c = 0; c < 3; ++c) elap = std::max(elap, std::abs(lap.data()[i](c) + 2 * v.data()[i](c)));
+    }
+    require(dtr == 0.0 && elap < 3e-2, "rank-2 gradient and divergence");
+  }
   std::printf("version %s\n", gridcalc::version());
   return 0;
 }

@@ -33,6 +33,8 @@ GRIDS = [
 def main() -> None:
     ref = oracle_lib.reference()
     rng = np.random.default_rng(20261203)
+    # Matrix fields draw from their own stream so the earlier arrays keep their values.
+    rng_mat = np.random.default_rng(20261204)
     out: dict[str, np.ndarray] = {}
     for name, shape, h in GRIDS:
         f = rng.standard_normal(shape)
@@ -41,6 +43,8 @@ def main() -> None:
         out[f"{name}/f"] = f
         out[f"{name}/v"] = v
         out[f"{name}/D"] = D
+        m = rng_mat.standard_normal((3, 3) + shape)
+        out[f"{name}/m"] = m
         out[f"{name}/h"] = np.array(h)
         for order in (2, 4):
             out[f"{name}/laplacian{order}"] = ref.op("laplacian", order, f, h)
@@ -48,6 +52,8 @@ def main() -> None:
             out[f"{name}/divergence{order}"] = ref.op("divergence", order, v, h)
             out[f"{name}/biharmonic{order}"] = ref.op("biharmonic", order, f, h)
             out[f"{name}/ch_rhs{order}"] = ref.ch_rhs(order, 1.3, 0.7, 0.1 * f, h)
+            out[f"{name}/gradient_vec{order}"] = ref.op("gradient_vec", order, v, h)
+            out[f"{name}/divergence_mat{order}"] = ref.op("divergence_mat", order, m, h)
         out[f"{name}/cell_laplacian"] = ref.cell_laplacian(f, D, h)
         out[f"{name}/integrate_pairwise"] = np.array(ref.integrate(f, h, kahan=False))
         out[f"{name}/integrate_kahan"] = np.array(ref.integrate(f, h, kahan=True))

@@ -76,10 +76,13 @@ class _Lib:
 
     def op(self, name: str, order: int, f: np.ndarray, h=(1.0, 1.0, 1.0)) -> np.ndarray:
         """laplacian / gradient / divergence / biharmonic on an (nz, ny, nx)
-        array (vector fields: (3, nz, ny, nx))."""
+        array (vector fields: (3, nz, ny, nx)); gradient_vec maps a vector
+        field to a (3, 3, nz, ny, nx) matrix field M[row, col] = d_col v_row
+        and divergence_mat maps such a matrix field back to a vector field."""
         f = np.ascontiguousarray(f, dtype=np.float64)
         shape = f.shape[-3:]
-        out_shape = (3,) + shape if name == "gradient" else shape
+        out_shape = {"gradient": (3,) + shape, "gradient_vec": (3, 3) + shape,
+                     "divergence_mat": (3,) + shape}.get(name, shape)
         out = np.zeros(out_shape)
         self._rc(self._f(name)(order, *self._g(shape, h), _ptr(f), _ptr(out)))
         return out

@@ -42,6 +42,9 @@ def test_oracle_matches_reference_golden_operators(oracle, golden):
                 assert np.array_equal(got, golden[f"{g}/{op}{order}"]), (g, op, order)
             got = oracle.ch_rhs(order, 1.3, 0.7, 0.1 * f, h)
             assert np.array_equal(got, golden[f"{g}/ch_rhs{order}"]), (g, "ch_rhs", order)
+            assert np.array_equal(oracle.op("gradient_vec", order, v, h), golden[f"{g}/gradient_vec{order}"])
+            assert np.array_equal(oracle.op("divergence_mat", order, golden[f"{g}/m"], h),
+                                  golden[f"{g}/divergence_mat{order}"])
         assert np.array_equal(oracle.cell_laplacian(f, D, h), golden[f"{g}/cell_laplacian"])
         assert oracle.integrate(f, h, kahan=False) == float(golden[f"{g}/integrate_pairwise"])
         assert oracle.integrate(f, h, kahan=True) == float(golden[f"{g}/integrate_kahan"])
@@ -88,6 +91,10 @@ def test_oracle_matches_live_reference(oracle):
                 if any(1 < n < 2 * r + 1 for n in shape):
                     continue
                 assert np.array_equal(oracle.op(op, order, src, h), ref.op(op, order, src, h)), (shape, op, order)
+            if not any(1 < n < order + 1 for n in shape):
+                m = rng.standard_normal((3, 3) + shape)
+                assert np.array_equal(oracle.op("gradient_vec", order, v, h), ref.op("gradient_vec", order, v, h))
+                assert np.array_equal(oracle.op("divergence_mat", order, m, h), ref.op("divergence_mat", order, m, h))
         x = rng.standard_normal(4097)
         g = x.reshape(1, 1, -1)
         assert oracle.integrate(g) == ref.integrate(g)
