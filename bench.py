@@ -235,19 +235,29 @@ def form_operators(gc, peak):
     out = {}
     for n in (256, 512):
         f64, lap_a, bih_a, grad_a = fourier_field(n, 2, "cuda", torch.float64)
-        vec64, div_a = [], torch.zeros_like(f64)
+        vec64, div_a, gmat_a, vlap_a = [], torch.zeros_like(f64), [], []
         for d, sd in enumerate((3, 4, 5)):
-            comp, _, _, gcomp = fourier_field(n, sd, "cuda", torch.float64)
+            comp, clap, _, gcomp = fourier_field(n, sd, "cuda", torch.float64)
             vec64.append(comp)
             div_a += gcomp[d]
-            del gcomp
+            gmat_a.append(gcomp)
+            vlap_a.append(clap)
         vec64 = torch.stack(vec64)
+        # The analytic rank-2 gradient M(r, c) = d_c v_r; its divergence is the vector Laplacian.
+        gmat_a, vlap_a = torch.stack(gmat_a), torch.stack(vlap_a)
+        tr = gc.integrand.trace
+        progs = {
+            "free_energy": tr(lambda p, d: -0.5 * p * p + 0.25 * p * p * p * p + 0.5 * 0.7 * d.squaredNorm()),
+            "arity4": tr(lambda p, d, lap, bih: gc.maximum(p, 0.0) * bih + gc.minimum(lap, d[2]) + gc.sqrt(1.0 + p * p)),
+            "elastic_vec": tr(lambda u, M: 0.8 * M.doubleContract(M) + 0.5 * 1.3 * M.trace() * M.trace(), 3),
+        }
         g = gc.Grid(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n)
         cells = n ** 3
         rel = lambda a, b: float(torch.linalg.norm(a.double() - b) / torch.linalg.norm(b))
         for dtype, tag in ((torch.float64, "f64"), (torch.float32, "f32")):
-            f, vec = f64.to(dtype), vec64.to(dtype)
+            f, vec, mat = f64.to(dtype), vec64.to(dtype), gmat_a.to(dtype)
             o, o3 = torch.empty_like(f), torch.empty((3,) + g.shape, dtype=dtype, device="cuda")
+            o9 = torch.empty((3, 3) + g.shape, dtype=dtype, device="cuda")
             es = f.element_size()
             res = {}
 
@@ -268,16 +278,30 @@ def form_operators(gc, peak):
                 for order in (2, 4, 6):
                     rec(f"{pname}{order}", 2, lambda: gc.partial(f, g, counts, order, o), o, exact)
                 del exact
+            # Rank-2 forms: Vec3d -> Mat3d gradient, Mat3d -> Vec3d divergence.
+            for order in (2, 4):
+                rec(f"gradient_vec{order}", 12, lambda: gc.gradient(vec, g, order, o9), o9, gmat_a)
+                rec(f"divergence_mat{order}", 12, lambda: gc.divergence(mat, g, order, o3), o3, vlap_a)
             ms = _cuda_time(lambda: gc.integrate(f, g))
             gbs = es * cells / ms / 1e6
             res["integrate"] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak,
                                 "abs_err_vs_exact_zero": abs(gc.integrate(f, g))}
+            # func::evaluate with recorded callables: the field is read once
+            # (the algorithmic bytes); the integrand is formed in FP64 and
+            # reduced with the exact pairwise tree.
+            for pname, prog in progs.items():
+                src = f if prog.components == 1 else vec
+                ms = _cuda_time(lambda: gc.evaluate(src, g, prog))
+                gbs = prog.components * es * cells / ms / 1e6
+                res[f"evaluate_{pname}"] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak, "instructions": len(prog),
+                                            "arity": prog.arity}
             out[f"{tag}_{n}"] = res
-            del f, vec, o, o3
-        del f64, lap_a, bih_a, grad_a, vec64, div_a
+            del f, vec, mat, o, o3, o9
+        del f64, lap_a, bih_a, grad_a, vec64, div_a, gmat_a, vlap_a
         torch.cuda.empty_cache()
     return {"workload": "operator sweep, 64 Fourier modes |k|<=16 on the unit cube (seed 2; vector field seeds 3,4,5)",
-            "bytes_per_cell": "laplacian/biharmonic/partials 2s, gradient/divergence 4s, integrate 1s (s = 8 or 4)",
+            "bytes_per_cell": "laplacian/biharmonic/partials 2s, gradient/divergence 4s, rank-2 gradient/divergence "
+                              "12s, integrate 1s, evaluate 1s (scalar) or 3s (vector) (s = 8 or 4)",
             "results": out}
 
 

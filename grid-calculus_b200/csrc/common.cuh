@@ -102,6 +102,11 @@ gc_status ch_rhs_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const g
 gc_status ch_rkc_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
                          double dt_step, int stages, void* const (&scratch)[4]);
 
+// Sum of n values (double or float, as dt) on ctx->stream, exactly the
+// reference's pairwise tree (GC_SUM_PAIRWISE) or the deterministic
+// compensated sum (GC_SUM_KAHAN); synchronises and returns it on the host.
+gc_status sum_any(gc_context* ctx, gc_dtype dt, const void* x, long long n, gc_sum sum, double* result);
+
 // Scope of one API call: validates the context, orders the context stream
 // after the caller's stream on entry and the caller's stream after the
 // context stream on exit.

@@ -18,13 +18,17 @@ import ctypes as C
 import os
 from dataclasses import dataclass
 
+from . import integrand
+from . import integrand as _integrand
+from .integrand import maximum, minimum, sqrt
+
 __all__ = [
     "lib", "Grid", "Context", "context", "GcError", "F64", "F32",
     "Pairwise", "Kahan", "RK4", "ExplicitEuler", "CahnHilliardRhs",
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
-    "rkc_stability_bound", "partial", "PARTIALS",
+    "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -394,15 +398,55 @@ def integrate(field, grid: Grid, tag=Pairwise, ctx=None) -> float:
 INTEGRANDS = {"psi": 0, "psi_squared": 1, "ch_free_energy": 2, "grad_squared": 3}
 
 
-def evaluate(psi, grid: Grid, integrand: str, kappa: float = 0.0, tag=Pairwise, ctx=None) -> float:
-    """func::evaluate(psi, f, tag) (func/Functional.hpp:88-148) for the
-    integrands of the hot path: 'psi', 'psi_squared', 'ch_free_energy'
-    (-psi^2/2 + psi^4/4 + kappa/2 |grad psi|^2) and 'grad_squared'."""
-    _require(psi, grid)
-    f = gc_integrand(INTEGRANDS[integrand], kappa)
+class gc_instr(C.Structure):
+    _fields_ = [("op", C.c_int16), ("dst", C.c_int16), ("a", C.c_int16), ("b", C.c_int16), ("value", C.c_double)]
+
+
+class gc_program(C.Structure):
+    _fields_ = [("components", C.c_int32), ("arity", C.c_int32), ("n_instr", C.c_int32), ("reserved", C.c_int32),
+                ("instr", gc_instr * _integrand.MAX_INSTR)]
+
+
+lib.gc_evaluate_program.argtypes = [_vp, _gp, _i32, _vp, C.POINTER(gc_program), _i32, C.POINTER(C.c_double)]
+lib.gc_evaluate_program.restype = C.c_int
+
+
+def program_struct(prog: "_integrand.Program") -> gc_program:
+    """The C layout of a traced integrand program."""
+    p = gc_program(prog.components, prog.arity, len(prog.instr), 0)
+    for k, (op, dst, a, b, value) in enumerate(prog.instr):
+        p.instr[k] = gc_instr(op, dst, a, b, value)
+    return p
+
+
+def evaluate(field, grid: Grid, integrand, kappa: float = 0.0, tag=Pairwise, ctx=None) -> float:
+    """func::evaluate(field, f, tag).
+
+    f may be a Python callable, like the reference's callable
+    (func/Functional.hpp:88-148 for a scalar psi: f(psi), f(psi, grad),
+    f(psi, grad, lap), f(psi, grad, lap, bih); :183-220 for a vector field of
+    3 * cells values: f(u), f(u, M) with M[row, col] = d_col u_row).  It is
+    traced once into a device program (gridcalc_b200.integrand) and the
+    integrand is formed and reduced on the GPU.  A traced
+    ``integrand.Program`` is accepted as well, and the hot-path integrands
+    by name: 'psi', 'psi_squared', 'ch_free_energy' (-psi^2/2 + psi^4/4 +
+    kappa/2 |grad psi|^2) and 'grad_squared'."""
+    if isinstance(integrand, str):
+        _require(field, grid)
+        f = gc_integrand(INTEGRANDS[integrand], kappa)
+        r = C.c_double()
+        _check(lib.gc_evaluate(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                               C.byref(f), tag.code, C.byref(r)))
+        return r.value
+    comps = 3 if grid.size > 0 and field.numel() == 3 * grid.size else 1
+    prog = integrand if isinstance(integrand, _integrand.Program) else _integrand.trace(integrand, comps)
+    if prog.components != comps:
+        raise ValueError(f"gridcalc_b200: program is for {prog.components} component(s), field has {comps}")
+    _require(field, grid, comps)
+    p = program_struct(prog)
     r = C.c_double()
-    _check(lib.gc_evaluate(_ctx(ctx), C.byref(grid.c()), _dtype_code(psi), psi.data_ptr(),
-                           C.byref(f), tag.code, C.byref(r)))
+    _check(lib.gc_evaluate_program(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                                   C.byref(p), tag.code, C.byref(r)))
     return r.value
 
 

@@ -453,6 +453,293 @@ inline double evaluate(const core::Field<double>& psi, F f, Tag = {}) {
   return r;
 }
 
+// Integrand programs.  The reference's func::evaluate calls a host callable
+// per cell (func/Functional.hpp:88-148 scalar, :183-220 Vec3d).  Here a
+// generic callable (auto parameters) is called once on symbolic arguments;
+// the operations it performs are recorded in order and become a gc_program
+// that the device runs for every cell with the same correctly rounded double
+// arithmetic, so the integrand is the one the callable computes, bit for
+// bit.  Supported: + - * / (and the compound forms) with doubles on either
+// side, unary -, func::sqrt / abs / fabs / min / max (std::min / std::max
+// semantics); Vec3 offers (i), [i], dot, squaredNorm, norm; Mat3 offers
+// (row, col), trace, squaredNorm, doubleContract, with Eigen's summation
+// order (components in order; matrices in column-major storage order from
+// 0.0).  std:: math functions and comparisons cannot be recorded.
+namespace program {
+
+class Recorder {
+ public:
+  struct Node {
+    int op, a, b;  // operand node ids; for GC_OPC_INPUT, a is the input number
+    double value;
+  };
+  int add(int op, int a = -1, int b = -1, double value = 0.0) {
+    nodes_.push_back(Node{op, a, b, value});
+    return static_cast<int>(nodes_.size()) - 1;
+  }
+  int input(int k) {
+    for (const auto& kv : inputs_)
+      if (kv.first == k) return kv.second;
+    const int id = add(GC_OPC_INPUT, k);
+    inputs_.push_back({k, id});
+    return id;
+  }
+  // Emits the nodes the result depends on, in recording order, on at most
+  // GC_PROGRAM_REGS registers (a register is reused after its last read).
+  gc_program compile(int components, int arity, int root) const {
+    const int n = static_cast<int>(nodes_.size());
+    std::vector<char> live(n, 0);
+    std::vector<int> stack{root};
+    while (!stack.empty()) {
+      const int k = stack.back();
+      stack.pop_back();
+      if (live[k]) continue;
+      live[k] = 1;
+      if (nodes_[k].op != GC_OPC_INPUT && nodes_[k].op != GC_OPC_CONST) {
+        if (nodes_[k].a >= 0) stack.push_back(nodes_[k].a);
+        if (nodes_[k].b >= 0) stack.push_back(nodes_[k].b);
+      }
+    }
+    std::vector<int> order;
+    for (int k = 0; k < n; ++k)
+      if (live[k]) order.push_back(k);
+    if (order.size() > GC_PROGRAM_MAX_INSTR)
+      throw std::invalid_argument("gridcalc: func::evaluate: integrand needs " + std::to_string(order.size()) +
+                                  " instructions, at most " + std::to_string(GC_PROGRAM_MAX_INSTR));
+    std::vector<int> last(n, -1);
+    for (size_t pos = 0; pos < order.size(); ++pos) {
+      const Node& nd = nodes_[order[pos]];
+      if (nd.op == GC_OPC_INPUT || nd.op == GC_OPC_CONST) continue;
+      if (nd.a >= 0) last[nd.a] = static_cast<int>(pos);
+      if (nd.b >= 0) last[nd.b] = static_cast<int>(pos);
+    }
+    last[root] = static_cast<int>(order.size());
+    gc_program p{};
+    p.components = components;
+    p.arity = arity;
+    p.n_instr = static_cast<int32_t>(order.size());
+    std::vector<int> reg(n, -1), free_regs;
+    for (int r = GC_PROGRAM_REGS - 1; r >= 0; --r) free_regs.push_back(r);
+    for (size_t pos = 0; pos < order.size(); ++pos) {
+      const Node& nd = nodes_[order[pos]];
+      const bool ops = nd.op != GC_OPC_INPUT && nd.op != GC_OPC_CONST;
+      const int ra = ops && nd.a >= 0 ? reg[nd.a] : 0;
+      const int rb = ops && nd.b >= 0 ? reg[nd.b] : 0;
+      if (ops && nd.a >= 0 && last[nd.a] == static_cast<int>(pos)) free_regs.push_back(reg[nd.a]);
+      if (ops && nd.b >= 0 && nd.b != nd.a && last[nd.b] == static_cast<int>(pos)) free_regs.push_back(reg[nd.b]);
+      if (free_regs.empty())
+        throw std::invalid_argument("gridcalc: func::evaluate: integrand keeps more than " +
+                                    std::to_string(GC_PROGRAM_REGS) + " values live");
+      const int dst = free_regs.back();
+      free_regs.pop_back();
+      reg[order[pos]] = dst;
+      gc_instr& I = p.instr[pos];
+      I.op = static_cast<int16_t>(nd.op);
+      I.dst = static_cast<int16_t>(dst);
+      I.a = static_cast<int16_t>(nd.op == GC_OPC_INPUT ? nd.a : ra);
+      I.b = static_cast<int16_t>(rb);
+      I.value = nd.op == GC_OPC_CONST ? nd.value : 0.0;
+    }
+    return p;
+  }
+
+ private:
+  std::vector<Node> nodes_;
+  std::vector<std::pair<int, int>> inputs_;
+};
+
+class Sym {
+ public:
+  Sym(Recorder* r, int id) : r_(r), id_(id) {}
+  Recorder* rec() const { return r_; }
+  int id() const { return id_; }
+
+ private:
+  Recorder* r_;
+  int id_;
+};
+
+inline Sym constant(Recorder* r, double v) { return Sym(r, r->add(GC_OPC_CONST, -1, -1, v)); }
+inline Sym op2(int op, const Sym& a, const Sym& b) { return Sym(a.rec(), a.rec()->add(op, a.id(), b.id())); }
+inline Sym op1(int op, const Sym& a) { return Sym(a.rec(), a.rec()->add(op, a.id())); }
+
+#define GRIDCALC_B200_SYM_BINARY(SYM, OPC)                                                               \
+  inline Sym operator SYM(const Sym& a, const Sym& b) { return op2(OPC, a, b); }                        \
+  inline Sym operator SYM(const Sym& a, double b) { return op2(OPC, a, constant(a.rec(), b)); }         \
+  inline Sym operator SYM(double a, const Sym& b) { return op2(OPC, constant(b.rec(), a), b); }         \
+  inline Sym& operator SYM##=(Sym& a, const Sym& b) { return a = a SYM b; }                              \
+  inline Sym& operator SYM##=(Sym& a, double b) { return a = a SYM b; }
+GRIDCALC_B200_SYM_BINARY(+, GC_OPC_ADD)
+GRIDCALC_B200_SYM_BINARY(-, GC_OPC_SUB)
+GRIDCALC_B200_SYM_BINARY(*, GC_OPC_MUL)
+GRIDCALC_B200_SYM_BINARY(/, GC_OPC_DIV)
+#undef GRIDCALC_B200_SYM_BINARY
+
+inline Sym operator-(const Sym& a) { return op1(GC_OPC_NEG, a); }
+inline Sym operator+(const Sym& a) { return a; }
+inline Sym sqrt(const Sym& a) { return op1(GC_OPC_SQRT, a); }
+inline Sym abs(const Sym& a) { return op1(GC_OPC_ABS, a); }
+inline Sym fabs(const Sym& a) { return op1(GC_OPC_ABS, a); }
+inline Sym min(const Sym& a, const Sym& b) { return op2(GC_OPC_MIN, a, b); }
+inline Sym max(const Sym& a, const Sym& b) { return op2(GC_OPC_MAX, a, b); }
+inline Sym min(const Sym& a, double b) { return op2(GC_OPC_MIN, a, constant(a.rec(), b)); }
+inline Sym max(const Sym& a, double b) { return op2(GC_OPC_MAX, a, constant(a.rec(), b)); }
+inline Sym min(double a, const Sym& b) { return op2(GC_OPC_MIN, constant(b.rec(), a), b); }
+inline Sym max(double a, const Sym& b) { return op2(GC_OPC_MAX, constant(b.rec(), a), b); }
+
+// Vec3d of one cell.
+struct Vec3 {
+  Sym v[3];
+  Sym operator()(int i) const { return v[i]; }
+  Sym operator[](int i) const { return v[i]; }
+  Sym x() const { return v[0]; }
+  Sym y() const { return v[1]; }
+  Sym z() const { return v[2]; }
+  Sym dot(const Vec3& o) const { return (v[0] * o.v[0] + v[1] * o.v[1]) + v[2] * o.v[2]; }
+  Sym squaredNorm() const { return dot(*this); }
+  Sym norm() const { return sqrt(squaredNorm()); }
+};
+
+// Mat3d of one cell, M(row, col).
+struct Mat3 {
+  Sym m[3][3];
+  Sym operator()(int r, int c) const { return m[r][c]; }
+  Sym trace() const { return (m[0][0] + m[1][1]) + m[2][2]; }
+  Sym doubleContract(const Mat3& o) const {
+    Sym acc = constant(m[0][0].rec(), 0.0);
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) acc = acc + m[r][c] * o.m[r][c];
+    return acc;
+  }
+  Sym squaredNorm() const { return doubleContract(*this); }
+};
+
+template <class F>
+constexpr int scalar_arity() {
+  if constexpr (std::is_invocable_v<F&, Sym, Vec3, Sym, Sym>) return 4;
+  else if constexpr (std::is_invocable_v<F&, Sym, Vec3, Sym>) return 3;
+  else if constexpr (std::is_invocable_v<F&, Sym, Vec3>) return 2;
+  else if constexpr (std::is_invocable_v<F&, Sym>) return 1;
+  else return 0;
+}
+
+template <class F>
+constexpr int vector_arity() {
+  if constexpr (std::is_invocable_v<F&, Vec3, Mat3>) return 2;
+  else if constexpr (std::is_invocable_v<F&, Vec3>) return 1;
+  else return 0;
+}
+
+// Lazy forms for overload selection: a generic callable is only probed with
+// the symbols of the field kind it is called on (probing a vector callable
+// with scalar symbols would instantiate its body and fail to compile).
+template <class F>
+struct scalar_callable : std::bool_constant<(scalar_arity<F>() > 0)> {};
+template <class F>
+struct vector_callable : std::bool_constant<(vector_arity<F>() > 0)> {};
+
+inline int root_of(Recorder&, const Sym& s) { return s.id(); }
+inline int root_of(Recorder& rec, double v) { return rec.add(GC_OPC_CONST, -1, -1, v); }
+
+template <class F>
+gc_program record_scalar(F& f) {
+  constexpr int arity = scalar_arity<F>();
+  Recorder rec;
+  const Sym psi(&rec, rec.input(GC_IN_PSI));
+  const Vec3 g{{Sym(&rec, rec.input(GC_IN_GRAD_X)), Sym(&rec, rec.input(GC_IN_GRAD_Y)),
+                Sym(&rec, rec.input(GC_IN_GRAD_Z))}};
+  const Sym lap(&rec, rec.input(GC_IN_LAP));
+  const Sym bih(&rec, rec.input(GC_IN_BIH));
+  int root;
+  if constexpr (arity == 4) root = root_of(rec, f(psi, g, lap, bih));
+  else if constexpr (arity == 3) root = root_of(rec, f(psi, g, lap));
+  else if constexpr (arity == 2) root = root_of(rec, f(psi, g));
+  else root = root_of(rec, f(psi));
+  return rec.compile(1, arity, root);
+}
+
+template <class F>
+gc_program record_vector(F& f) {
+  constexpr int arity = vector_arity<F>();
+  Recorder rec;
+  Vec3 u{{Sym(&rec, rec.input(GC_IN_U_X)), Sym(&rec, rec.input(GC_IN_U_Y)), Sym(&rec, rec.input(GC_IN_U_Z))}};
+  auto du = [&](int r, int c) { return Sym(&rec, rec.input(GC_IN_DU + 3 * r + c)); };
+  const Mat3 M{{{du(0, 0), du(0, 1), du(0, 2)}, {du(1, 0), du(1, 1), du(1, 2)}, {du(2, 0), du(2, 1), du(2, 2)}}};
+  int root;
+  if constexpr (arity == 2) root = root_of(rec, f(u, M));
+  else root = root_of(rec, f(u));
+  return rec.compile(3, arity, root);
+}
+
+template <class Tag>
+constexpr gc_sum sum_of() { return std::is_same_v<Tag, Kahan> ? GC_SUM_KAHAN : GC_SUM_PAIRWISE; }
+
+}  // namespace program
+
+using program::abs;
+using program::fabs;
+using program::max;
+using program::min;
+using program::sqrt;
+
+// func::evaluate(psi, f, tag) for a generic callable of arity 1..4
+// (func/Functional.hpp:88-148).
+template <class FieldT, class F, class Tag = Pairwise,
+          std::enable_if_t<std::conjunction_v<std::is_same<FieldT, core::Field<double>>, program::scalar_callable<F>>,
+                           int> = 0>
+inline double evaluate(const FieldT& psi, F f, Tag = {}) {
+  const gc_program p = program::record_scalar(f);
+  core::DeviceField<double> d(psi);
+  const gc_grid g = psi.getGrid().c();
+  double r = 0.0;
+  b200::check(gc_evaluate_program(b200::context(), &g, GC_F64, d.data(), &p, program::sum_of<Tag>(), &r));
+  return r;
+}
+
+// func::evaluate(u, f, tag) for a Vec3d field and a generic callable f(u) or
+// f(u, grad u) (func/Functional.hpp:183-220).
+template <class FieldT, class F, class Tag = Pairwise,
+          std::enable_if_t<
+              std::conjunction_v<std::is_same<FieldT, core::Field<core::Vec3d>>, program::vector_callable<F>>, int> = 0>
+inline double evaluate(const FieldT& u, F f, Tag = {}) {
+  const gc_program p = program::record_vector(f);
+  const core::Grid& grid = u.getGrid();
+  const size_t n = grid.getSize();
+  std::vector<double> planes(3 * n);
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) planes[c * n + i] = u.data()[i](c);
+  core::DeviceField<double> d(grid, 3);
+  d.upload(planes.data());
+  const gc_grid g = grid.c();
+  double r = 0.0;
+  b200::check(gc_evaluate_program(b200::context(), &g, GC_F64, d.data(), &p, program::sum_of<Tag>(), &r));
+  return r;
+}
+
+// The same on device-resident fields: a scalar field with f(psi[, grad[,
+// lap[, bih]]]), and a vector field (three planes) with f(u[, grad_u]).
+template <class T, class F, class Tag = Pairwise, std::enable_if_t<program::scalar_callable<F>::value, int> = 0>
+inline double evaluate(const core::DeviceField<T>& psi, F f, Tag = {}) {
+  if (psi.components() != 1)
+    throw std::invalid_argument("gridcalc: func::evaluate: a scalar integrand needs a one-component field");
+  const gc_program p = program::record_scalar(f);
+  const gc_grid g = psi.getGrid().c();
+  double r = 0.0;
+  b200::check(gc_evaluate_program(b200::context(), &g, b200::dtype_of<T>(), psi.data(), &p, program::sum_of<Tag>(), &r));
+  return r;
+}
+template <class T, class F, class Tag = Pairwise>
+inline double evaluateVector(const core::DeviceField<T>& u, F f, Tag = {}) {
+  static_assert(program::vector_callable<F>::value, "func::evaluateVector: f must be invocable as f(u) or f(u, grad_u)");
+  if (u.components() != 3)
+    throw std::invalid_argument("gridcalc: func::evaluateVector: a vector integrand needs a three-component field");
+  const gc_program p = program::record_vector(f);
+  const gc_grid g = u.getGrid().c();
+  double r = 0.0;
+  b200::check(gc_evaluate_program(b200::context(), &g, b200::dtype_of<T>(), u.data(), &p, program::sum_of<Tag>(), &r));
+  return r;
+}
+
 }  // namespace func
 
 namespace solve {

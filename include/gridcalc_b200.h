@@ -187,6 +187,63 @@ typedef struct gc_integrand {
 GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
                              const gc_integrand* f, gc_sum sum, double* result);
 
+/* General integrands.  func::evaluate (func/Functional.hpp:88-148 for a
+ * scalar psi, :183-220 for a Vec3d field u) calls a host callable per cell
+ * whose arity picks the derivative fields it receives.  Across the C ABI the
+ * callable is a straight-line program over double registers r[0..31]: each
+ * instruction writes r[dst] from r[a], r[b], a constant or an input, with
+ * correctly rounded + - * / and sqrt, so a program that performs the
+ * callable's operations in the callable's order yields the same integrand,
+ * bit for bit.  The program's value is r[dst] of its last instruction.
+ *
+ * Inputs (order-2 derivatives, the reference's default), by arity:
+ *   scalar (components 1): arity 1: GC_IN_PSI; 2 adds GC_IN_GRAD_X..Z;
+ *     3 adds GC_IN_LAP; 4 adds GC_IN_BIH.
+ *   vector (components 3): arity 1: GC_IN_U_X..Z; 2 adds GC_IN_DU + 3*row + col,
+ *     the rank-2 gradient M(row, col) = d_col u_row (diff/Gradient.hpp:100-137). */
+#define GC_PROGRAM_MAX_INSTR 128
+#define GC_PROGRAM_REGS 32
+
+typedef enum gc_opcode {
+  GC_OPC_CONST = 0,  /* r[dst] = value */
+  GC_OPC_INPUT = 1,  /* r[dst] = input number a */
+  GC_OPC_ADD = 2,    /* r[dst] = r[a] + r[b] */
+  GC_OPC_SUB = 3,    /* r[dst] = r[a] - r[b] */
+  GC_OPC_MUL = 4,    /* r[dst] = r[a] * r[b] */
+  GC_OPC_DIV = 5,    /* r[dst] = r[a] / r[b] */
+  GC_OPC_NEG = 6,    /* r[dst] = -r[a] */
+  GC_OPC_ABS = 7,    /* r[dst] = |r[a]| */
+  GC_OPC_SQRT = 8,   /* r[dst] = sqrt(r[a]) */
+  GC_OPC_MIN = 9,    /* r[dst] = std::min(r[a], r[b]) = r[b] < r[a] ? r[b] : r[a] */
+  GC_OPC_MAX = 10    /* r[dst] = std::max(r[a], r[b]) = r[a] < r[b] ? r[b] : r[a] */
+} gc_opcode;
+
+enum {
+  GC_IN_PSI = 0, GC_IN_GRAD_X = 1, GC_IN_GRAD_Y = 2, GC_IN_GRAD_Z = 3, GC_IN_LAP = 4, GC_IN_BIH = 5,
+  GC_IN_U_X = 0, GC_IN_U_Y = 1, GC_IN_U_Z = 2, GC_IN_DU = 3
+};
+
+typedef struct gc_instr {
+  int16_t op, dst, a, b;  /* gc_opcode; register or input numbers (unused ones 0) */
+  double value;           /* GC_OPC_CONST only */
+} gc_instr;
+
+typedef struct gc_program {
+  int32_t components;  /* 1: scalar psi; 3: vector u (three planes) */
+  int32_t arity;       /* 1..4 (scalar) or 1..2 (vector), as the callable's */
+  int32_t n_instr;     /* 1..GC_PROGRAM_MAX_INSTR */
+  int32_t reserved;    /* 0 */
+  gc_instr instr[GC_PROGRAM_MAX_INSTR];
+} gc_program;
+
+/* func::evaluate(field, f, tag) for a program f.  The derivative fields of
+ * f's arity are checked against the axis extents in the reference's order
+ * (gradient, Laplacian, biharmonic), the integrand is formed on the device
+ * and reduced like gc_integrate.  A malformed program (bad opcode, register
+ * read before it is written, input beyond the arity) is GC_ERR_INVALID_ARG. */
+GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field,
+                                     const gc_program* f, gc_sum sum, double* result);
+
 /* ---- time integration (solve::) ----------------------------------------- */
 
 /* Cahn-Hilliard right-hand side M lap(-psi + psi^3 - kappa lap psi)

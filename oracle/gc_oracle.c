@@ -628,3 +628,82 @@ int oc_diffuse_fvm(int nx, int ny, int nz, double hx, double hy, double hz, doub
   wrap3_free(&w);
   return 0;
 }
+
+/* ---- func/Functional.hpp:88-148 (scalar) and :183-220 (vector): evaluate a
+ * callable per cell into an integrand field, then func::integrate.  The
+ * derivative fields of the callable's arity are materialised first, at the
+ * reference's default order 2 and in its order (gradient, Laplacian,
+ * biharmonic), so the first failing extent check is the reference's. */
+static double oc_run_program(const oc_instr* prog, int n_instr, const double* in) {
+  double r[32];
+  for (int pc = 0; pc < n_instr; ++pc) {
+    const oc_instr* I = &prog[pc];
+    double v;
+    switch (I->op) {
+      case 0: v = I->value; break;
+      case 1: v = in[I->a]; break;
+      case 2: v = r[I->a] + r[I->b]; break;
+      case 3: v = r[I->a] - r[I->b]; break;
+      case 4: v = r[I->a] * r[I->b]; break;
+      case 5: v = r[I->a] / r[I->b]; break;
+      case 6: v = -r[I->a]; break;
+      case 7: v = fabs(r[I->a]); break;
+      case 8: v = sqrt(r[I->a]); break;
+      case 9: v = r[I->b] < r[I->a] ? r[I->b] : r[I->a]; break;
+      default: v = r[I->a] < r[I->b] ? r[I->b] : r[I->a]; break;
+    }
+    r[I->dst] = v;
+  }
+  return r[prog[n_instr - 1].dst];
+}
+
+int oc_evaluate_program(int components, int arity, int nx, int ny, int nz, double hx, double hy, double hz,
+                        const double* field, const oc_instr* prog, int n_instr, int kahan, double* result) {
+  if (!((components == 1 && arity >= 1 && arity <= 4) || (components == 3 && arity >= 1 && arity <= 2)) ||
+      n_instr < 1 || n_instr > 128) {
+    snprintf(g_err, sizeof g_err, "evaluate: bad program shape");
+    return 3;
+  }
+  for (int pc = 0; pc < n_instr; ++pc)
+    if (prog[pc].op < 0 || prog[pc].op > 10 || prog[pc].dst < 0 || prog[pc].dst >= 32 || prog[pc].a < 0 ||
+        prog[pc].a >= 32 || prog[pc].b < 0 || prog[pc].b >= 32) {
+      snprintf(g_err, sizeof g_err, "evaluate: bad instruction %d", pc);
+      return 3;
+    }
+  const size_t n = (size_t)nx * ny * nz;
+  const int nin = components == 1 ? (arity == 1 ? 1 : arity + 2) : (arity == 1 ? 3 : 12);
+  for (int pc = 0; pc < n_instr; ++pc)
+    if (prog[pc].op == 1 && prog[pc].a >= nin) {
+      snprintf(g_err, sizeof g_err, "evaluate: input %d beyond the arity", prog[pc].a);
+      return 3;
+    }
+  double* d1 = NULL; double* d2 = NULL; double* d4 = NULL;
+  double* integrand = (double*)malloc(sizeof(double) * (n ? n : 1));
+  int rc = 0;
+  if (components == 1) {
+    if (arity >= 2) { d1 = (double*)malloc(sizeof(double) * 3 * n); rc = oc_gradient(2, nx, ny, nz, hx, hy, hz, field, d1); }
+    if (!rc && arity >= 3) { d2 = (double*)malloc(sizeof(double) * n); rc = oc_laplacian(2, nx, ny, nz, hx, hy, hz, field, d2); }
+    if (!rc && arity >= 4) { d4 = (double*)malloc(sizeof(double) * n); rc = oc_biharmonic(2, nx, ny, nz, hx, hy, hz, field, d4); }
+  } else if (arity >= 2) {
+    d1 = (double*)malloc(sizeof(double) * 9 * n);
+    rc = oc_gradient_vec(2, nx, ny, nz, hx, hy, hz, field, d1);
+  }
+  if (!rc) {
+    for (size_t c = 0; c < n; ++c) {
+      double in[12];
+      if (components == 1) {
+        in[0] = field[c];
+        if (arity >= 2) { in[1] = d1[c]; in[2] = d1[n + c]; in[3] = d1[2 * n + c]; }
+        if (arity >= 3) in[4] = d2[c];
+        if (arity >= 4) in[5] = d4[c];
+      } else {
+        for (int q = 0; q < 3; ++q) in[q] = field[q * n + c];
+        if (arity >= 2) for (int q = 0; q < 9; ++q) in[3 + q] = d1[q * n + c];
+      }
+      integrand[c] = oc_run_program(prog, n_instr, in);
+    }
+    if (!rc) *result = oc_integrate(nx, ny, nz, hx, hy, hz, integrand, kahan);
+  }
+  free(d1); free(d2); free(d4); free(integrand);
+  return rc;
+}

@@ -61,6 +61,17 @@ double oc_sum_neumaier(const double* x, size_t n);
 double oc_integrate(int nx, int ny, int nz, double hx, double hy, double hz,
                     const double* in, int kahan);
 
+/* func::evaluate with a general callable (func/Functional.hpp:88-148 scalar,
+ * :183-220 vector), the callable given as a straight-line register program:
+ * op 0 const, 1 input a, 2 add, 3 sub, 4 mul, 5 div, 6 neg, 7 abs, 8 sqrt,
+ * 9 std::min, 10 std::max; value = r[dst] of the last instruction.  Inputs:
+ * scalar psi, grad x/y/z, lap, biharmonic (order 2) up to the arity; vector
+ * u x/y/z then M(row, col) = d_col u_row at 3 + 3*row + col.  Returns 0, 1
+ * (axis extent) or 3 (malformed program). */
+typedef struct oc_instr { int16_t op, dst, a, b; double value; } oc_instr;
+int oc_evaluate_program(int components, int arity, int nx, int ny, int nz, double hx, double hy, double hz,
+                        const double* field, const oc_instr* prog, int n_instr, int kahan, double* result);
+
 int oc_ch_rhs(int order, double M, double kappa, int nx, int ny, int nz, double hx,
               double hy, double hz, const double* psi, double* out);
 /* integrator: 0 = explicit Euler, 1 = RK4.  psi advanced in place. */

@@ -10,6 +10,8 @@
 // cross this boundary as three planes (x, y, z components, N values each).
 // std::invalid_argument is caught and turned into return code 1 with the
 // message available from ref_last_error().
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -41,6 +43,36 @@ using gridcalc::core::Vec3d;
 namespace ch = gridcalc::examples::cahn_hilliard;
 
 thread_local std::string g_err;
+
+// A straight-line register program standing in for a callable (the layout
+// of gc_instr / oc_instr): r[dst] = op(r[a], r[b]), a constant or input a.
+struct RefInstr {
+  int16_t op, dst, a, b;
+  double value;
+};
+
+double runProgram(const RefInstr* prog, int n, const double* in) {
+  double r[32];
+  for (int pc = 0; pc < n; ++pc) {
+    const RefInstr& I = prog[pc];
+    double v;
+    switch (I.op) {
+      case 0: v = I.value; break;
+      case 1: v = in[I.a]; break;
+      case 2: v = r[I.a] + r[I.b]; break;
+      case 3: v = r[I.a] - r[I.b]; break;
+      case 4: v = r[I.a] * r[I.b]; break;
+      case 5: v = r[I.a] / r[I.b]; break;
+      case 6: v = -r[I.a]; break;
+      case 7: v = std::fabs(r[I.a]); break;
+      case 8: v = std::sqrt(r[I.a]); break;
+      case 9: v = std::min(r[I.a], r[I.b]); break;
+      default: v = std::max(r[I.a], r[I.b]); break;
+    }
+    r[I.dst] = v;
+  }
+  return r[prog[n - 1].dst];
+}
 
 Grid makeGrid(int nx, int ny, int nz, double hx, double hy, double hz) {
   return Grid(nx, ny, nz, Vec3d(hx, hy, hz));
@@ -234,6 +266,58 @@ int ref_divergence_mat(int order, int nx, int ny, int nz, double hx, double hy, 
       out3[i] = r.data()[i](0);
       out3[n + i] = r.data()[i](1);
       out3[2 * n + i] = r.data()[i](2);
+    }
+  });
+}
+
+// func::evaluate (func/Functional.hpp:88-148, :183-220) with a callable of
+// the program's arity; the reference materialises the derivative fields and
+// integrates the integrand itself.
+int ref_evaluate_program(int components, int arity, int nx, int ny, int nz, double hx, double hy, double hz,
+                         const double* field, const RefInstr* prog, int n_instr, int kahan, double* result) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    auto run = [&](const double* in) { return runProgram(prog, n_instr, in); };
+    if (components == 1) {
+      const Field<double> f = load(g, field);
+      auto ev = [&](auto&& fn) {
+        *result = kahan ? gridcalc::func::evaluate(f, fn, gridcalc::func::Kahan{}) : gridcalc::func::evaluate(f, fn);
+      };
+      if (arity == 1) {
+        ev([&](double p) { const double in[1] = {p}; return run(in); });
+      } else if (arity == 2) {
+        ev([&](double p, const Vec3d& d) { const double in[4] = {p, d(0), d(1), d(2)}; return run(in); });
+      } else if (arity == 3) {
+        ev([&](double p, const Vec3d& d, double l) { const double in[5] = {p, d(0), d(1), d(2), l}; return run(in); });
+      } else if (arity == 4) {
+        ev([&](double p, const Vec3d& d, double l, double b) {
+          const double in[6] = {p, d(0), d(1), d(2), l, b};
+          return run(in);
+        });
+      } else {
+        throw std::invalid_argument("ref: scalar arity must be 1..4");
+      }
+    } else if (components == 3) {
+      Field<Vec3d> u(g);
+      const std::size_t n = g.getSize();
+      for (std::size_t i = 0; i < n; ++i) u.data()[i] = Vec3d(field[i], field[n + i], field[2 * n + i]);
+      auto ev = [&](auto&& fn) {
+        *result = kahan ? gridcalc::func::evaluate(u, fn, gridcalc::func::Kahan{}) : gridcalc::func::evaluate(u, fn);
+      };
+      if (arity == 1) {
+        ev([&](const Vec3d& v) { const double in[3] = {v(0), v(1), v(2)}; return run(in); });
+      } else if (arity == 2) {
+        ev([&](const Vec3d& v, const Mat3d& M) {
+          double in[12] = {v(0), v(1), v(2)};
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) in[3 + 3 * r + c] = M(r, c);
+          return run(in);
+        });
+      } else {
+        throw std::invalid_argument("ref: vector arity must be 1 or 2");
+      }
+    } else {
+      throw std::invalid_argument("ref: components must be 1 or 3");
     }
   });
 }

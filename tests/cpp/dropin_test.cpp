@@ -151,6 +151,27 @@ int main() {
     }
     require(dtr == 0.0 && elap < 3e-2, "rank-2 gradient and divergence");
   }
+  {  // func::evaluate with generic callables: recorded free energy == the device functor,
+     // trace(grad u) integrates to the integral of div u, bit for bit
+    const int N = 24;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<double> psi(g, [](double x, double y, double z) { return 0.3 * std::sin(x) * std::cos(2 * y) + 0.1 * z; });
+    const double fe = gridcalc::func::evaluate(
+        psi, [](auto p, const auto& d) { return -0.5 * p * p + 0.25 * p * p * p * p + 0.5 * 1.0 * d.squaredNorm(); });
+    const double fe_dev = gridcalc::func::evaluate(psi, gridcalc::func::FreeEnergy{1.0});
+    const double b4 = gridcalc::func::evaluate(psi, [](auto p, const auto&, auto lap, auto bih) {
+      return gridcalc::func::max(p, 0.0) + lap * bih / (1.0 + gridcalc::func::abs(p));
+    });
+    Field<Vec3d> u(g);
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i)
+          u(i, j, k) = Vec3d(std::sin(i * h) * std::cos(j * h), std::sin(j * h) * std::cos(k * h), std::sin(k * h));
+    const double tr = gridcalc::func::evaluate(u, [](const auto&, const auto& M) { return M.trace(); });
+    const double dv = gridcalc::func::integrate(gridcalc::diff::divergence(u));
+    require(fe == fe_dev && std::isfinite(b4) && tr == dv, "func::evaluate with recorded callables");
+  }
   std::printf("version %s\n", gridcalc::version());
   return 0;
 }

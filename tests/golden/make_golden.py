@@ -16,6 +16,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
+import integrand_cases  # noqa: E402
 import oracle_lib  # noqa: E402
 
 PARTIALS = oracle_lib.PARTIALS
@@ -60,6 +61,13 @@ def main() -> None:
         out[f"{name}/free_energy"] = np.array(ref.ch_free_energy(f, 0.8, h))
         out[f"{name}/gradient_energy"] = np.array(ref.ch_gradient_energy(f, h))
         out[f"{name}/mean"] = np.array(ref.ch_mean(f, h))
+        # func::evaluate with callables of every arity (tests/integrand_cases.py).
+        for cname, (comps, _) in integrand_cases.CASES.items():
+            prog = integrand_cases.program(cname)
+            src = f if comps == 1 else v
+            out[f"{name}/evaluate_{cname}"] = np.array(ref.evaluate_program(comps, prog.arity, prog.instr, src, h))
+            out[f"{name}/evaluate_{cname}_kahan"] = np.array(
+                ref.evaluate_program(comps, prog.arity, prog.instr, src, h, kahan=True))
         for pname, porder in PARTIAL_CASES:
             if pname == name:
                 for c in PARTIALS:
@@ -86,6 +94,12 @@ def main() -> None:
 
     # The reference initial-condition generator (mt19937_64, mean removed).
     out["ic/seed42_16x16"] = ref.make_random_ic((1, 16, 16), 42, 0.05)
+
+    # The programs those values were computed with (rows op, dst, a, b, value).
+    for cname in integrand_cases.CASES:
+        prog = integrand_cases.program(cname)
+        out[f"program/{cname}"] = integrand_cases.rows(prog)
+        out[f"program/{cname}_shape"] = np.array([prog.components, prog.arity])
 
     path = os.path.join(HERE, "reference_vectors.npz")
     np.savez_compressed(path, **out)

@@ -49,6 +49,11 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_P)
 
 
+class _Instr(C.Structure):
+    """One integrand-program instruction (gc_instr / oc_instr layout)."""
+    _fields_ = [("op", C.c_int16), ("dst", C.c_int16), ("a", C.c_int16), ("b", C.c_int16), ("value", C.c_double)]
+
+
 class _Lib:
     """Common numpy front end over either library (prefix oc_ or ref_)."""
 
@@ -94,6 +99,18 @@ class _Lib:
         ax, ay, az = counts
         self._rc(self._f("mixed")(ax, ay, az, order, *self._g(f.shape, h), _ptr(f), _ptr(out)))
         return out
+
+    def evaluate_program(self, components: int, arity: int, instr, field, h=(1.0, 1.0, 1.0),
+                         kahan=False) -> float:
+        """func::evaluate with the callable given as a register program
+        (rows op, dst, a, b, value); field (nz, ny, nx) or (3, nz, ny, nx)."""
+        field = np.ascontiguousarray(field, dtype=np.float64)
+        rows = [_Instr(int(o), int(d), int(a), int(b), float(v)) for o, d, a, b, v in instr]
+        arr = (_Instr * len(rows))(*rows)
+        out = C.c_double()
+        self._rc(self._f("evaluate_program")(components, arity, *self._g(field.shape[-3:], h), _ptr(field), arr,
+                                             len(rows), int(kahan), C.byref(out)))
+        return out.value
 
     def cell_laplacian(self, psi, D, h=(1.0, 1.0, 1.0)):
         psi = np.ascontiguousarray(psi, dtype=np.float64)
