@@ -102,6 +102,25 @@ gc_status ch_rhs_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const g
 gc_status ch_rkc_enqueue(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
                          double dt_step, int stages, void* const (&scratch)[4]);
 
+// The reduction's building blocks, for kernels that produce the summands
+// themselves.  Pairwise: 2^depth chunks of at most 8192 values, reduced per
+// chunk into partial[0, nchunks) and finished by pairwise_finish (which uses
+// the rest of scratch_bytes after the chunk sums).  Compensated: kKahanBlocks
+// blocks of kKahanThreads threads, each thread over the values
+// i = block * kKahanThreads + thread + m * kKahanBlocks * kKahanThreads, the
+// block's (sum, compensation) at part[2 * block]; kahan_finish merges them.
+struct PairwisePlan {
+  int depth = 0;
+  long long nchunks = 1;
+  size_t scratch_bytes = 0;
+};
+PairwisePlan pairwise_plan(long long n);
+gc_status pairwise_finish(gc_context* ctx, double* partial, long long nchunks, double* result);
+constexpr int kKahanBlocks = 1024;
+constexpr int kKahanThreads = 256;
+constexpr size_t kKahanScratchBytes = sizeof(double) * (2 * kKahanBlocks + 8);
+gc_status kahan_finish(gc_context* ctx, double* part, double* result);
+
 // Sum of n values (double or float, as dt) on ctx->stream, exactly the
 // reference's pairwise tree (GC_SUM_PAIRWISE) or the deterministic
 // compensated sum (GC_SUM_KAHAN); synchronises and returns it on the host.

@@ -4,198 +4,304 @@
 // The reference materialises the derivative fields the callable's arity asks
 // for (order-2 gradient, Laplacian, biharmonic; for a vector field the
 // order-2 rank-2 gradient), evaluates the callable per cell into an integrand
-// field and reduces it with func::integrate.  Here one kernel forms every
-// derivative a cell needs from its neighbours (read through L1/L2; one HBM
-// read per value), runs the integrand program on them and writes the
-// integrand; the reduction is the exact pairwise tree of gc_integrate (or
-// its compensated sum).  No derivative field is materialised.
+// field and reduces it with func::integrate.  Here the callable arrives as a
+// straight-line register program (gc_program), which is turned into CUDA
+// source, compiled once per distinct program with NVRTC for sm_100a and
+// cached: the integrand becomes a device functor inlined into the
+// reduction.  One kernel walks the reduction's chunks, forms at every cell
+// the derivatives of the arity from its neighbours (read through L1/L2; one
+// HBM read per value), evaluates the integrand and reduces it in place, so
+// neither a derivative field nor the integrand field is ever written.
 //
-// The program is a straight-line list of register instructions passed by
-// value as a kernel parameter, so every thread of a warp reads the same
-// instruction from the constant bank and the interpreter's branches are
-// uniform.  Every sum, product and quotient is rounded on its own, in the
-// reference's order, so double results are bit-identical to the reference
-// when the program performs the callable's operations in the callable's
-// order.
+// Exactness: every sum, product, quotient and square root in the generated
+// code is an explicitly rounded intrinsic (__dadd_rn ...), the derivative
+// sums run in the reference's tap order from 0.0, and the reduction is the
+// reference's pairwise tree (the chunk walk of pairwise_chunks), so double
+// results are bit-identical to the reference when the program performs the
+// callable's operations in the callable's order.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <nvrtc.h>
+
 #include <algorithm>
+#include <cinttypes>
+#include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
 namespace gcb {
 namespace {
 
-constexpr int kEvX = 32;
-constexpr int kEvY = 8;
+constexpr int kChunkCells = 8192;   // pairwise chunk bound (pairwise.cuh kChunkMax)
+constexpr int kEvalThreads = 256;
 
-struct EvalArgs {
+// Kernel argument; the device source declares the same layout.
+struct EvalGrid {
   const void* field;
-  double* out;
-  int nx, ny, nz, zc;
-  size_t n;
+  long long n;
+  int nx, ny, nz;
+  int step_i, step_j, step_k;     // kEvalThreads cells as (di, dj, dk)
+  int kstep_i, kstep_j, kstep_k;  // the compensated sum's stride as (di, dj, dk)
+  int pad;
   double ihx, ihy, ihz;     // 1 / h
   double ihx2, ihy2, ihz2;  // 1 / h^2
   double ihx4, ihy4, ihz4;  // (1 / h^2)^2
-  int n_instr, result_reg;
-  gc_instr prog[GC_PROGRAM_MAX_INSTR];
 };
 
-constexpr int n_inputs(int comps, int arity) {
-  return comps == 1 ? (arity == 1 ? 1 : arity == 2 ? 4 : arity == 3 ? 5 : 6) : (arity == 1 ? 3 : 12);
+// Device code shared by every program.  gc_cell forms the inputs of the
+// arity at one cell and calls the generated gc_integrand; the two kernels are
+// the pairwise chunk walk (as pairwise_chunks) and the compensated block sum
+// (as kahan_blocks) with the summand computed in place.
+const char kDeviceSource[] = R"GCSRC(
+typedef long long gc_i64;
+struct EvalGrid {
+  const void* field;
+  gc_i64 n;
+  int nx, ny, nz;
+  int step_i, step_j, step_k;
+  int kstep_i, kstep_j, kstep_k;
+  int pad;
+  double ihx, ihy, ihz, ihx2, ihy2, ihz2, ihx4, ihy4, ihz4;
+};
+
+__device__ __forceinline__ double gc_integrand(const double* in);
+
+#define GC_R (GC_COMPS == 1 ? (GC_ARITY >= 4 ? 2 : GC_ARITY >= 2 ? 1 : 0) : (GC_ARITY >= 2 ? 1 : 0))
+#define GC_NIN (GC_COMPS == 1 ? (GC_ARITY == 1 ? 1 : GC_ARITY + 2) : (GC_ARITY == 1 ? 3 : 12))
+
+__device__ __forceinline__ int gc_wrap(int i, int n) {
+  if (i >= 0 && i < n) return i;
+  const int r = i % n;
+  return r < 0 ? r + n : r;
 }
 
-__device__ __forceinline__ double run_program(const EvalArgs& a, const double* in) {
-  double r[GC_PROGRAM_REGS];
-  for (int pc = 0; pc < a.n_instr; ++pc) {
-    const gc_instr& I = a.prog[pc];
-    double v;
-    switch (I.op) {
-      case GC_OPC_CONST: v = I.value; break;
-      case GC_OPC_INPUT: v = in[I.a]; break;
-      case GC_OPC_ADD: v = __dadd_rn(r[I.a], r[I.b]); break;
-      case GC_OPC_SUB: v = __dsub_rn(r[I.a], r[I.b]); break;
-      case GC_OPC_MUL: v = __dmul_rn(r[I.a], r[I.b]); break;
-      case GC_OPC_DIV: v = __ddiv_rn(r[I.a], r[I.b]); break;
-      case GC_OPC_NEG: v = -r[I.a]; break;
-      case GC_OPC_ABS: v = fabs(r[I.a]); break;
-      case GC_OPC_SQRT: v = __dsqrt_rn(r[I.a]); break;
-      case GC_OPC_MIN: v = r[I.b] < r[I.a] ? r[I.b] : r[I.a]; break;
-      default: v = r[I.a] < r[I.b] ? r[I.b] : r[I.a]; break;  // GC_OPC_MAX (validated on the host)
-    }
-    r[I.dst] = v;
-  }
-  return r[a.result_reg];
-}
-
-// Order-2 first derivative along one axis: every tap of (-1, 0, 1) with
-// weights (-0.5, 0, 0.5) summed from 0.0 (diff/Gradient.hpp:59-66).
+// Order-2 first derivative: taps (-1, 0, 1), weights (-0.5, 0, 0.5), from 0.0.
 template <class Tap>
-__device__ __forceinline__ double d1(const Tap& tap) {
+__device__ __forceinline__ double gc_d1(const Tap& tap) {
   double s = 0.0;
-#pragma unroll
-  for (int m = 0; m < 3; ++m) s = __dadd_rn(s, __dmul_rn(W<1, 2>::w(m), tap(m - 1)));
-  return s;
+  s = __dadd_rn(s, __dmul_rn(-0.5, tap(-1)));
+  s = __dadd_rn(s, __dmul_rn(0.0, tap(0)));
+  return __dadd_rn(s, __dmul_rn(0.5, tap(1)));
 }
 
-// A thread walks a column of cells (i, j, z0..z1).  R is the largest stencil
-// radius the arity needs: 0 (values only), 1 (gradient, Laplacian) or 2
-// (biharmonic).
-template <class T, int COMPS, int ARITY>
-__global__ void __launch_bounds__(kEvX * kEvY) evaluate_kernel(const __grid_constant__ EvalArgs a) {
-  constexpr int R = COMPS == 1 ? (ARITY >= 4 ? 2 : ARITY >= 2 ? 1 : 0) : (ARITY >= 2 ? 1 : 0);
-  const int i = blockIdx.x * kEvX + threadIdx.x;
-  const int j = blockIdx.y * kEvY + threadIdx.y;
-  if (i >= a.nx || j >= a.ny) return;
-  const int nx = a.nx, ny = a.ny, nz = a.nz;
-  const T* __restrict__ f = static_cast<const T*>(a.field);
-  int xs[2 * R + 1];
-  size_t ys[2 * R + 1];
+__device__ __forceinline__ double gc_cell(const EvalGrid& g, int i, int j, int k) {
+  const GC_T* __restrict__ f = (const GC_T*)g.field;
+  int xs[2 * GC_R + 1];
+  gc_i64 ys[2 * GC_R + 1], zs[2 * GC_R + 1];
+  const gc_i64 plane = (gc_i64)g.nx * g.ny;
 #pragma unroll
-  for (int m = 0; m <= 2 * R; ++m) {
-    xs[m] = wrap(i + m - R, nx);
-    ys[m] = static_cast<size_t>(wrap(j + m - R, ny)) * nx;
+  for (int m = 0; m <= 2 * GC_R; ++m) {
+    xs[m] = gc_wrap(i + m - GC_R, g.nx);
+    ys[m] = (gc_i64)gc_wrap(j + m - GC_R, g.ny) * g.nx;
+    zs[m] = (gc_i64)gc_wrap(k + m - GC_R, g.nz) * plane;
   }
-  const size_t plane = static_cast<size_t>(nx) * ny;
-  const int z0 = blockIdx.z * a.zc;
-  const int z1 = min(z0 + a.zc, nz);
-  for (int k = z0; k < z1; ++k) {
-    size_t zs[2 * R + 1];
+  auto v = [&](int c, int ox, int oy, int oz) -> double {
+    return (double)__ldg(f + (gc_i64)c * g.n + zs[oz + GC_R] + ys[oy + GC_R] + xs[ox + GC_R]);
+  };
+  double in[GC_NIN];
+#if GC_COMPS == 1
+  in[0] = v(0, 0, 0, 0);
+#if GC_ARITY >= 2
+  in[1] = __dmul_rn(gc_d1([&](int o) { return v(0, o, 0, 0); }), g.ihx);
+  in[2] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, o, 0); }), g.ihy);
+  in[3] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, 0, o); }), g.ihz);
+#endif
+#if GC_ARITY >= 3
+  {  // Laplacian, taps (1, -2, 1) from 0.0 (diff/Laplacian.hpp:60-69)
+    const double w2[3] = {1.0, -2.0, 1.0};
+    double dxx = 0.0, dyy = 0.0, dzz = 0.0;
 #pragma unroll
-    for (int m = 0; m <= 2 * R; ++m) zs[m] = static_cast<size_t>(wrap(k + m - R, nz)) * plane;
-    auto v = [&](int comp, int ox, int oy, int oz) -> double {
-      return static_cast<double>(__ldg(f + comp * a.n + zs[oz + R] + ys[oy + R] + xs[ox + R]));
-    };
-    double in[n_inputs(COMPS, ARITY)];
-    if constexpr (COMPS == 1) {
-      in[GC_IN_PSI] = v(0, 0, 0, 0);
-      if constexpr (ARITY >= 2) {
-        in[GC_IN_GRAD_X] = __dmul_rn(d1([&](int o) { return v(0, o, 0, 0); }), a.ihx);
-        in[GC_IN_GRAD_Y] = __dmul_rn(d1([&](int o) { return v(0, 0, o, 0); }), a.ihy);
-        in[GC_IN_GRAD_Z] = __dmul_rn(d1([&](int o) { return v(0, 0, 0, o); }), a.ihz);
-      }
-      if constexpr (ARITY >= 3) {
-        // diff/Laplacian.hpp:60-69 at order 2.
-        double dxx = 0.0, dyy = 0.0, dzz = 0.0;
+    for (int m = 0; m < 3; ++m) {
+      dxx = __dadd_rn(dxx, __dmul_rn(w2[m], v(0, m - 1, 0, 0)));
+      dyy = __dadd_rn(dyy, __dmul_rn(w2[m], v(0, 0, m - 1, 0)));
+      dzz = __dadd_rn(dzz, __dmul_rn(w2[m], v(0, 0, 0, m - 1)));
+    }
+    in[4] = __dadd_rn(__dadd_rn(__dmul_rn(dxx, g.ihx2), __dmul_rn(dyy, g.ihy2)), __dmul_rn(dzz, g.ihz2));
+  }
+#endif
+#if GC_ARITY >= 4
+  {  // biharmonic (diff/Biharmonic.hpp:70-99)
+    const double w4[5] = {1.0, -4.0, 6.0, -4.0, 1.0};
+    const double w2[3] = {1.0, -2.0, 1.0};
+    double dx4 = 0.0, dy4 = 0.0, dz4 = 0.0;
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          const double w = W<2, 2>::w(m);
-          dxx = __dadd_rn(dxx, __dmul_rn(w, v(0, m - 1, 0, 0)));
-          dyy = __dadd_rn(dyy, __dmul_rn(w, v(0, 0, m - 1, 0)));
-          dzz = __dadd_rn(dzz, __dmul_rn(w, v(0, 0, 0, m - 1)));
-        }
-        in[GC_IN_LAP] = __dadd_rn(__dadd_rn(__dmul_rn(dxx, a.ihx2), __dmul_rn(dyy, a.ihy2)), __dmul_rn(dzz, a.ihz2));
-      }
-      if constexpr (ARITY >= 4) {
-        // diff/Biharmonic.hpp:70-99 at order 2.
-        double dx4 = 0.0, dy4 = 0.0, dz4 = 0.0;
+    for (int m = 0; m < 5; ++m) {
+      dx4 = __dadd_rn(dx4, __dmul_rn(w4[m], v(0, m - 2, 0, 0)));
+      dy4 = __dadd_rn(dy4, __dmul_rn(w4[m], v(0, 0, m - 2, 0)));
+      dz4 = __dadd_rn(dz4, __dmul_rn(w4[m], v(0, 0, 0, m - 2)));
+    }
+    double xy = 0.0, xz = 0.0, yz = 0.0;
 #pragma unroll
-        for (int m = 0; m < 5; ++m) {
-          const double w = W<4, 2>::w(m);
-          dx4 = __dadd_rn(dx4, __dmul_rn(w, v(0, m - 2, 0, 0)));
-          dy4 = __dadd_rn(dy4, __dmul_rn(w, v(0, 0, m - 2, 0)));
-          dz4 = __dadd_rn(dz4, __dmul_rn(w, v(0, 0, 0, m - 2)));
-        }
-        double xy = 0.0, xz = 0.0, yz = 0.0;
+    for (int mb = 0; mb < 3; ++mb) {
 #pragma unroll
-        for (int mb = 0; mb < 3; ++mb) {
-#pragma unroll
-          for (int ma = 0; ma < 3; ++ma) {
-            const double wab = W<2, 2>::w(ma) * W<2, 2>::w(mb);  // exact: products of 1 and -2
-            xy = __dadd_rn(xy, __dmul_rn(wab, v(0, ma - 1, mb - 1, 0)));
-            xz = __dadd_rn(xz, __dmul_rn(wab, v(0, ma - 1, 0, mb - 1)));
-            yz = __dadd_rn(yz, __dmul_rn(wab, v(0, 0, ma - 1, mb - 1)));
-          }
-        }
-        const double axial =
-            __dadd_rn(__dadd_rn(__dmul_rn(dx4, a.ihx4), __dmul_rn(dy4, a.ihy4)), __dmul_rn(dz4, a.ihz4));
-        const double c1 = __dmul_rn(__dmul_rn(xy, a.ihx2), a.ihy2);
-        const double c2 = __dmul_rn(__dmul_rn(xz, a.ihx2), a.ihz2);
-        const double c3 = __dmul_rn(__dmul_rn(yz, a.ihy2), a.ihz2);
-        in[GC_IN_BIH] = __dadd_rn(axial, __dmul_rn(2.0, __dadd_rn(__dadd_rn(c1, c2), c3)));
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) in[GC_IN_U_X + c] = v(c, 0, 0, 0);
-      if constexpr (ARITY >= 2) {
-        // diff/Gradient.hpp:115-131: row = component, column = axis.
-#pragma unroll
-        for (int row = 0; row < 3; ++row) {
-          in[GC_IN_DU + 3 * row + 0] = __dmul_rn(d1([&](int o) { return v(row, o, 0, 0); }), a.ihx);
-          in[GC_IN_DU + 3 * row + 1] = __dmul_rn(d1([&](int o) { return v(row, 0, o, 0); }), a.ihy);
-          in[GC_IN_DU + 3 * row + 2] = __dmul_rn(d1([&](int o) { return v(row, 0, 0, o); }), a.ihz);
-        }
+      for (int ma = 0; ma < 3; ++ma) {
+        const double wab = __dmul_rn(w2[ma], w2[mb]);
+        xy = __dadd_rn(xy, __dmul_rn(wab, v(0, ma - 1, mb - 1, 0)));
+        xz = __dadd_rn(xz, __dmul_rn(wab, v(0, ma - 1, 0, mb - 1)));
+        yz = __dadd_rn(yz, __dmul_rn(wab, v(0, 0, ma - 1, mb - 1)));
       }
     }
-    a.out[static_cast<size_t>(k) * plane + static_cast<size_t>(j) * nx + i] = run_program(a, in);
+    const double axial = __dadd_rn(__dadd_rn(__dmul_rn(dx4, g.ihx4), __dmul_rn(dy4, g.ihy4)), __dmul_rn(dz4, g.ihz4));
+    const double c1 = __dmul_rn(__dmul_rn(xy, g.ihx2), g.ihy2);
+    const double c2 = __dmul_rn(__dmul_rn(xz, g.ihx2), g.ihz2);
+    const double c3 = __dmul_rn(__dmul_rn(yz, g.ihy2), g.ihz2);
+    in[5] = __dadd_rn(axial, __dmul_rn(2.0, __dadd_rn(__dadd_rn(c1, c2), c3)));
+  }
+#endif
+#else
+#pragma unroll
+  for (int c = 0; c < 3; ++c) in[c] = v(c, 0, 0, 0);
+#if GC_ARITY >= 2
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {  // M(r, c) = d_c u_r (diff/Gradient.hpp:115-131)
+    in[3 + 3 * r + 0] = __dmul_rn(gc_d1([&](int o) { return v(r, o, 0, 0); }), g.ihx);
+    in[3 + 3 * r + 1] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, o, 0); }), g.ihy);
+    in[3 + 3 * r + 2] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, 0, o); }), g.ihz);
+  }
+#endif
+#endif
+  return gc_integrand(in);
+}
+
+// (i, j, k) += a step given as (di, dj, dk) with di < nx, dj < ny.
+__device__ __forceinline__ void gc_advance(int& i, int& j, int& k, int nx, int ny, int di, int dj, int dk) {
+  i += di;
+  if (i >= nx) { i -= nx; ++j; }
+  j += dj;
+  if (j >= ny) { j -= ny; ++k; }
+  k += dk;
+}
+
+__device__ __forceinline__ void gc_locate(const EvalGrid& g, gc_i64 c, int& i, int& j, int& k) {
+  i = (int)(c % g.nx);
+  const gc_i64 rest = c / g.nx;
+  j = (int)(rest % g.ny);
+  k = (int)(rest / g.ny);
+}
+
+__device__ __forceinline__ int gc_padpos(int e) { return e + (e >> 6); }
+
+__device__ __forceinline__ void gc_descend(gc_i64& lo, gc_i64& hi, gc_i64 idx, int depth) {
+  for (int b = depth - 1; b >= 0; --b) {
+    const gc_i64 mid = lo + (hi - lo) / 2;
+    if ((idx >> b) & 1) lo = mid;
+    else hi = mid;
   }
 }
 
-template <class T, int COMPS, int ARITY>
-gc_status launch(gc_context* ctx, const EvalArgs& a) {
-  const int gx = (a.nx + kEvX - 1) / kEvX, gy = (a.ny + kEvY - 1) / kEvY;
-  const int gz = (a.nz + a.zc - 1) / a.zc;
-  evaluate_kernel<T, COMPS, ARITY><<<dim3(gx, gy, gz), dim3(kEvX, kEvY), 0, ctx->stream>>>(a);
-  GC_CHECK_LAUNCH("evaluate_kernel");
-  return GC_OK;
+__device__ __forceinline__ double gc_seq_sum(const double* s, int a, int b) {
+  double acc = 0.0;
+  for (int e = a; e < b; ++e) acc = __dadd_rn(acc, s[gc_padpos(e)]);
+  return acc;
 }
 
-template <class T>
-gc_status dispatch(gc_context* ctx, int comps, int arity, const EvalArgs& a) {
-  if (comps == 1) {
-    switch (arity) {
-      case 1: return launch<T, 1, 1>(ctx, a);
-      case 2: return launch<T, 1, 2>(ctx, a);
-      case 3: return launch<T, 1, 3>(ctx, a);
-      default: return launch<T, 1, 4>(ctx, a);
+extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
+                                                                   double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = (double*)smem_raw;
+  double* ns = s + gc_padpos(8192) + 8;
+  for (gc_i64 c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    gc_i64 lo = 0, hi = g.n;
+    gc_descend(lo, hi, c, depth);
+    const int len = (int)(hi - lo);
+    int i, j, k;
+    gc_locate(g, lo + threadIdx.x, i, j, k);
+    for (int e = threadIdx.x; e < len; e += 256) {
+      s[gc_padpos(e)] = gc_cell(g, i, j, k);
+      gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
+    }
+    int d2 = 0;
+    while (((len + (1 << d2) - 1) >> d2) > 128) ++d2;
+    const int nodes = 1 << d2;
+    __syncthreads();
+    if (threadIdx.x < nodes) {
+      gc_i64 a = 0, b = len;
+      gc_descend(a, b, threadIdx.x, d2);
+      const int m = (int)(b - a);
+      double v;
+      if (m <= 64) {
+        v = gc_seq_sum(s, (int)a, (int)b);
+      } else {
+        const int h = m / 2;
+        v = __dadd_rn(gc_seq_sum(s, (int)a, (int)a + h), gc_seq_sum(s, (int)a + h, (int)b));
+      }
+      ns[threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int w = nodes >> 1; w >= 1; w >>= 1) {
+      double v = 0.0;
+      if (threadIdx.x < w) v = __dadd_rn(ns[2 * threadIdx.x], ns[2 * threadIdx.x + 1]);
+      __syncthreads();
+      if (threadIdx.x < w) ns[threadIdx.x] = v;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[c] = ns[0];
+    __syncthreads();
+  }
+}
+
+struct GcSumC { double s, c; };
+
+__device__ __forceinline__ GcSumC gc_neumaier_add(GcSumC a, double v) {
+  const double t = __dadd_rn(a.s, v);
+  if (fabs(a.s) >= fabs(v)) a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(a.s, t), v));
+  else a.c = __dadd_rn(a.c, __dadd_rn(__dsub_rn(v, t), a.s));
+  a.s = t;
+  return a;
+}
+
+__device__ __forceinline__ GcSumC gc_merge(GcSumC a, GcSumC b) {
+  const double t = __dadd_rn(a.s, b.s);
+  const double bp = __dsub_rn(t, a.s);
+  const double err = __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, bp)), __dsub_rn(b.s, bp));
+  GcSumC r;
+  r.s = t;
+  r.c = __dadd_rn(__dadd_rn(a.c, b.c), err);
+  return r;
+}
+
+extern "C" __global__ void __launch_bounds__(256) gc_eval_kahan(const EvalGrid g, double* __restrict__ out) {
+  __shared__ GcSumC sh[256];
+  GcSumC acc;
+  acc.s = 0.0;
+  acc.c = 0.0;
+  const gc_i64 first = (gc_i64)blockIdx.x * 256 + threadIdx.x;
+  if (first < g.n) {
+    int i, j, k;
+    gc_locate(g, first, i, j, k);
+    for (gc_i64 c = first; c < g.n; c += (gc_i64)1024 * 256) {
+      acc = gc_neumaier_add(acc, gc_cell(g, i, j, k));
+      gc_advance(i, j, k, g.nx, g.ny, g.kstep_i, g.kstep_j, g.kstep_k);
     }
   }
-  return arity == 1 ? launch<T, 3, 1>(ctx, a) : launch<T, 3, 2>(ctx, a);
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w >= 1; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = gc_merge(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = sh[0].s;
+    out[2 * blockIdx.x + 1] = sh[0].c;
+  }
+}
+)GCSRC";
+
+static_assert(kKahanBlocks == 1024 && kKahanThreads == 256, "the device source bakes in the compensated sum's shape");
+static_assert(kEvalThreads == 256, "the device source bakes in 256 threads per block");
+
+constexpr int n_inputs(int comps, int arity) {
+  return comps == 1 ? (arity == 1 ? 1 : arity + 2) : (arity == 1 ? 3 : 12);
 }
 
 // Checks the program's shape and that every register is written before it
-// is read; returns the result register.
-gc_status check_program(const gc_program* f, int* result_reg) {
+// is read.
+gc_status check_program(const gc_program* f) {
   auto bad = [](const std::string& m) { return fail(GC_ERR_INVALID_ARG, "gc_evaluate_program: " + m); };
   if (f->components != 1 && f->components != 3) return bad("components must be 1 (scalar) or 3 (vector)");
   const int max_arity = f->components == 1 ? 4 : 2;
@@ -221,8 +327,142 @@ gc_status check_program(const gc_program* f, int* result_reg) {
     }
     defined |= 1u << I.dst;
   }
-  *result_reg = f->instr[f->n_instr - 1].dst;
   return GC_OK;
+}
+
+// The program as a device function: one named value per instruction, each
+// an explicitly rounded operation on the values its registers held.
+std::string integrand_source(const gc_program* f) {
+  std::string out = "__device__ __forceinline__ double gc_integrand(const double* in) {\n";
+  std::string reg[GC_PROGRAM_REGS];
+  char buf[96];
+  for (int pc = 0; pc < f->n_instr; ++pc) {
+    const gc_instr& I = f->instr[pc];
+    const std::string A = I.op > GC_OPC_INPUT ? reg[I.a] : "";
+    const std::string B = I.op > GC_OPC_INPUT ? reg[I.b] : "";
+    std::string e;
+    switch (I.op) {
+      case GC_OPC_CONST: {
+        uint64_t bits;
+        std::memcpy(&bits, &I.value, sizeof bits);
+        std::snprintf(buf, sizeof buf, "__longlong_as_double(0x%016" PRIx64 "LL)", bits);
+        e = buf;
+        break;
+      }
+      case GC_OPC_INPUT: e = "in[" + std::to_string(I.a) + "]"; break;
+      case GC_OPC_ADD: e = "__dadd_rn(" + A + ", " + B + ")"; break;
+      case GC_OPC_SUB: e = "__dsub_rn(" + A + ", " + B + ")"; break;
+      case GC_OPC_MUL: e = "__dmul_rn(" + A + ", " + B + ")"; break;
+      case GC_OPC_DIV: e = "__ddiv_rn(" + A + ", " + B + ")"; break;
+      case GC_OPC_NEG: e = "-" + A; break;
+      case GC_OPC_ABS: e = "fabs(" + A + ")"; break;
+      case GC_OPC_SQRT: e = "__dsqrt_rn(" + A + ")"; break;
+      case GC_OPC_MIN: e = "(" + B + " < " + A + " ? " + B + " : " + A + ")"; break;
+      default: e = "(" + A + " < " + B + " ? " + B + " : " + A + ")"; break;  // GC_OPC_MAX
+    }
+    const std::string name = "v" + std::to_string(pc);
+    out += "  const double " + name + " = " + e + ";\n";
+    reg[I.dst] = name;
+  }
+  out += "  return " + reg[f->instr[f->n_instr - 1].dst] + ";\n}\n";
+  return out;
+}
+
+std::string program_source(const gc_program* f, gc_dtype dt) {
+  std::string s = "#define GC_T " + std::string(dt == GC_F64 ? "double" : "float") + "\n";
+  s += "#define GC_COMPS " + std::to_string(f->components) + "\n";
+  s += "#define GC_ARITY " + std::to_string(f->arity) + "\n";
+  s += kDeviceSource;
+  s += integrand_source(f);
+  return s;
+}
+
+// ---- NVRTC compilation and the module cache ------------------------------
+// Driver entry points are fetched through the runtime, so the library does
+// not link libcuda itself.
+struct Driver {
+  PFN_cuModuleLoadData load = nullptr;
+  PFN_cuModuleGetFunction get = nullptr;
+  PFN_cuFuncSetAttribute attr = nullptr;
+  PFN_cuLaunchKernel launch = nullptr;
+};
+
+struct Compiled {
+  CUfunction pairwise = nullptr;
+  CUfunction kahan = nullptr;
+};
+
+std::mutex g_jit_mu;
+std::map<std::pair<int, std::string>, Compiled> g_jit;  // (device, source) -> kernels; modules live for the process
+
+gc_status driver(Driver* d) {
+  static Driver drv;
+  static bool ok = false;
+  if (!ok) {
+    cudaDriverEntryPointQueryResult q;
+    auto get = [&](const char* name, void** slot) -> bool {
+      return cudaGetDriverEntryPoint(name, slot, cudaEnableDefault, &q) == cudaSuccess &&
+             q == cudaDriverEntryPointSuccess && *slot;
+    };
+    if (!get("cuModuleLoadData", reinterpret_cast<void**>(&drv.load)) ||
+        !get("cuModuleGetFunction", reinterpret_cast<void**>(&drv.get)) ||
+        !get("cuFuncSetAttribute", reinterpret_cast<void**>(&drv.attr)) ||
+        !get("cuLaunchKernel", reinterpret_cast<void**>(&drv.launch)))
+      return fail(GC_ERR_CUDA, "gc_evaluate_program: CUDA driver entry points unavailable");
+    ok = true;
+  }
+  *d = drv;
+  return GC_OK;
+}
+
+gc_status compile(gc_context* ctx, const std::string& src, Compiled* out) {
+  std::lock_guard<std::mutex> lock(g_jit_mu);
+  const auto key = std::make_pair(ctx->device, src);
+  auto it = g_jit.find(key);
+  if (it != g_jit.end()) {
+    *out = it->second;
+    return GC_OK;
+  }
+  Driver drv;
+  gc_status s = driver(&drv);
+  if (s != GC_OK) return s;
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, src.c_str(), "gc_integrand.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+    return fail(GC_ERR_CUDA, "gc_evaluate_program: nvrtcCreateProgram failed");
+  const char* opts[] = {"--gpu-architecture=sm_100a", "--fmad=false", "-std=c++17"};
+  const nvrtcResult rc = nvrtcCompileProgram(prog, 3, opts);
+  if (rc != NVRTC_SUCCESS) {
+    size_t n = 0;
+    nvrtcGetProgramLogSize(prog, &n);
+    std::string log(n, '\0');
+    if (n) nvrtcGetProgramLog(prog, &log[0]);
+    nvrtcDestroyProgram(&prog);
+    return fail(GC_ERR_CUDA, std::string("gc_evaluate_program: NVRTC: ") + nvrtcGetErrorString(rc) + "\n" + log);
+  }
+  size_t cubin_size = 0;
+  nvrtcGetCUBINSize(prog, &cubin_size);
+  std::vector<char> cubin(cubin_size);
+  nvrtcGetCUBIN(prog, cubin.data());
+  nvrtcDestroyProgram(&prog);
+  CUmodule mod;
+  Compiled c;
+  if (drv.load(&mod, cubin.data()) != CUDA_SUCCESS || drv.get(&c.pairwise, mod, "gc_eval_pairwise") != CUDA_SUCCESS ||
+      drv.get(&c.kahan, mod, "gc_eval_kahan") != CUDA_SUCCESS)
+    return fail(GC_ERR_CUDA, "gc_evaluate_program: loading the compiled integrand failed");
+  const int smem = static_cast<int>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+  if (drv.attr(c.pairwise, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS)
+    return fail(GC_ERR_CUDA, "gc_evaluate_program: shared-memory attribute refused");
+  g_jit.emplace(key, c);
+  *out = c;
+  return GC_OK;
+}
+
+// A step of `cells` flat cells as (di, dj, dk) with di < nx, dj < ny.
+void split_step(long long cells, int nx, int ny, int* di, int* dj, int* dk) {
+  *di = static_cast<int>(cells % nx);
+  const long long rows = cells / nx;
+  *dj = static_cast<int>(rows % ny);
+  *dk = static_cast<int>(rows / ny);
 }
 
 }  // namespace
@@ -240,35 +480,62 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   if ((s = check_grid(g)) != GC_OK) return s;
   if (!field || !f || !result) return fail(GC_ERR_INVALID_ARG, "gc_evaluate_program: null pointer");
   if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gc_evaluate_program: unknown dtype");
-  EvalArgs a{};
-  if ((s = check_program(f, &a.result_reg)) != GC_OK) return s;
+  if ((s = check_program(f)) != GC_OK) return s;
   // The derivative fields of the arity, checked in the reference's order:
   // gradient (radius 1), Laplacian (radius 1), biharmonic (radius 2).
   if (f->arity >= 2 && (s = require_axes(g, 1)) != GC_OK) return s;
   if (f->components == 1 && f->arity >= 4 && (s = require_axes(g, 2)) != GC_OK) return s;
-  const size_t n = cells(g);
-  void* buf = nullptr;
-  if ((s = scratch_get(ctx, kSlotIntegrand, sizeof(double) * n, &buf)) != GC_OK) return s;
+  Compiled k;
+  if ((s = compile(ctx, program_source(f, dt), &k)) != GC_OK) return s;
+  Driver drv;
+  if ((s = driver(&drv)) != GC_OK) return s;
+
+  const long long n = static_cast<long long>(cells(g));
+  EvalGrid a{};
   a.field = field;
-  a.out = static_cast<double*>(buf);
-  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
   a.n = n;
+  a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
+  split_step(kEvalThreads, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
+  split_step(static_cast<long long>(kKahanBlocks) * kKahanThreads, g->nx, g->ny, &a.kstep_i, &a.kstep_j, &a.kstep_k);
   a.ihx = 1.0 / g->hx; a.ihy = 1.0 / g->hy; a.ihz = 1.0 / g->hz;
   a.ihx2 = 1.0 / (g->hx * g->hx); a.ihy2 = 1.0 / (g->hy * g->hy); a.ihz2 = 1.0 / (g->hz * g->hz);
   a.ihx4 = a.ihx2 * a.ihx2; a.ihy4 = a.ihy2 * a.ihy2; a.ihz4 = a.ihz2 * a.ihz2;
-  a.n_instr = f->n_instr;
-  std::memcpy(a.prog, f->instr, sizeof(gc_instr) * static_cast<size_t>(f->n_instr));
-  // Enough z chunks for about eight CTAs per SM.
-  const long long columns = static_cast<long long>((g->nx + kEvX - 1) / kEvX) * ((g->ny + kEvY - 1) / kEvY);
-  const long long want = std::max<long long>(1, (static_cast<long long>(ctx->num_sms) * 8 + columns - 1) / columns);
-  a.zc = static_cast<int>((g->nz + std::min<long long>(want, g->nz) - 1) / std::min<long long>(want, g->nz));
-  s = dt == GC_F64 ? dispatch<double>(ctx, f->components, f->arity, a)
-                   : dispatch<float>(ctx, f->components, f->arity, a);
-  if (s != GC_OK) return s;
+  const double vol = g->hx * g->hy * g->hz;
   double total = 0.0;
-  if ((s = sum_any(ctx, GC_F64, a.out, static_cast<long long>(n), sum, &total)) != GC_OK) return s;
-  *result = (g->hx * g->hy * g->hz) * total;
+  void* buf = nullptr;
+  if (sum == GC_SUM_KAHAN) {
+    if ((s = scratch_get(ctx, kSlotReduce, kKahanScratchBytes, &buf)) != GC_OK) return s;
+    double* part = static_cast<double*>(buf);
+    void* args[] = {&a, &part};
+    if (drv.launch(k.kahan, kKahanBlocks, 1, 1, kKahanThreads, 1, 1, 0, ctx->stream, args, nullptr) != CUDA_SUCCESS)
+      return fail(GC_ERR_CUDA, "gc_evaluate_program: launch failed");
+    if ((s = kahan_finish(ctx, part, &total)) != GC_OK) return s;
+  } else {
+    const PairwisePlan plan = pairwise_plan(n);
+    if ((s = scratch_get(ctx, kSlotReduce, plan.scratch_bytes, &buf)) != GC_OK) return s;
+    double* partial = static_cast<double*>(buf);
+    int depth = plan.depth;
+    long long nchunks = plan.nchunks;
+    void* args[] = {&a, &depth, &nchunks, &partial};
+    const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3));
+    const unsigned smem = static_cast<unsigned>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+    if (drv.launch(k.pairwise, grid, 1, 1, kEvalThreads, 1, 1, smem, ctx->stream, args, nullptr) != CUDA_SUCCESS)
+      return fail(GC_ERR_CUDA, "gc_evaluate_program: launch failed");
+    if ((s = pairwise_finish(ctx, partial, nchunks, &total)) != GC_OK) return s;
+  }
+  *result = vol * total;
   return GC_OK;
+}
+
+GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap) {
+  if (!f || check_program(f) != GC_OK) return 0;
+  const std::string src = program_source(f, dt);
+  if (buf && cap) {
+    const size_t n = std::min(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = '\0';
+  }
+  return src.size() + 1;
 }
 
 }  // extern "C"

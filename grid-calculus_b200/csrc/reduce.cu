@@ -33,9 +33,6 @@ namespace {
 // (sum, compensation) pairs merge up a fixed tree with an error-free
 // two-sum.  Grid and block sizes are constants, so the result does not
 // depend on the device.
-constexpr int kKahanBlocks = 1024;
-constexpr int kKahanThreads = 256;
-
 struct SumC { double s, c; };
 
 __device__ __forceinline__ SumC neumaier_add(SumC a, double v) {
@@ -169,36 +166,19 @@ __global__ void first_nonpositive_kernel(const T* __restrict__ D, long long n,
 
 }  // namespace
 
-// Exact pairwise sum of n values on the context's stream; result on the host.
-template <class T>
-gc_status pairwise_sum(gc_context* ctx, const T* x, long long n, double* result) {
-  if (n == 0) {
-    *result = 0.0;
-    return GC_OK;
-  }
-  int depth = 0;
-  while (((n + (1LL << depth) - 1) >> depth) > kChunkMax) ++depth;
-  const long long nchunks = 1LL << depth;
-  // Partials: level buffers for the chunk sums and the group reductions.
-  const size_t need = sizeof(double) * static_cast<size_t>(nchunks + nchunks / 1024 + 64);
-  void* buf = nullptr;
-  gc_status s = scratch_get(ctx, kSlotReduce, need, &buf);
-  if (s != GC_OK) return s;
-  double* a = static_cast<double*>(buf);
-  double* b = a + nchunks;
-  const size_t smem = sizeof(double) * (padpos(kChunkMax) + 8 + kNodeMax);
-  static bool attr_set[2] = {false, false};
-  auto kern = pairwise_chunks<T>;
-  if (!attr_set[sizeof(T) == 8]) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    attr_set[sizeof(T) == 8] = true;
-  }
-  const long long grid = std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3);
-  kern<<<static_cast<unsigned>(grid), kSumThreads, smem, ctx->stream>>>(x, n, depth, nchunks, a);
-  GC_CHECK_LAUNCH("pairwise_chunks");
+PairwisePlan pairwise_plan(long long n) {
+  PairwisePlan p;
+  while (((n + (1LL << p.depth) - 1) >> p.depth) > kChunkMax) ++p.depth;
+  p.nchunks = 1LL << p.depth;
+  // Chunk sums, then the group-reduction levels.
+  p.scratch_bytes = sizeof(double) * static_cast<size_t>(p.nchunks + p.nchunks / 1024 + 64);
+  return p;
+}
+
+gc_status pairwise_finish(gc_context* ctx, double* partial, long long nchunks, double* result) {
   long long count = nchunks;
-  double* src = a;
-  double* dst = b;
+  double* src = partial;
+  double* dst = partial + nchunks;
   while (count > 1) {
     const int group = static_cast<int>(std::min<long long>(count, 1024));
     const long long blocks = count / group;
@@ -214,14 +194,7 @@ gc_status pairwise_sum(gc_context* ctx, const T* x, long long n, double* result)
   return GC_OK;
 }
 
-template <class T>
-gc_status kahan_sum(gc_context* ctx, const T* x, long long n, double* result) {
-  void* buf = nullptr;
-  gc_status s = scratch_get(ctx, kSlotReduce, sizeof(double) * (2 * kKahanBlocks + 8), &buf);
-  if (s != GC_OK) return s;
-  double* part = static_cast<double*>(buf);
-  kahan_blocks<T><<<kKahanBlocks, kKahanThreads, 0, ctx->stream>>>(x, n, part);
-  GC_CHECK_LAUNCH("kahan_blocks");
+gc_status kahan_finish(gc_context* ctx, double* part, double* result) {
   kahan_final<<<1, kKahanBlocks, 0, ctx->stream>>>(part, part + 2 * kKahanBlocks);
   GC_CHECK_LAUNCH("kahan_final");
   double* host = static_cast<double*>(ctx->host_pinned);
@@ -229,6 +202,42 @@ gc_status kahan_sum(gc_context* ctx, const T* x, long long n, double* result) {
   GC_CUDA(cudaStreamSynchronize(ctx->stream));
   *result = host[0];
   return GC_OK;
+}
+
+// Exact pairwise sum of n values on the context's stream; result on the host.
+template <class T>
+gc_status pairwise_sum(gc_context* ctx, const T* x, long long n, double* result) {
+  if (n == 0) {
+    *result = 0.0;
+    return GC_OK;
+  }
+  const PairwisePlan plan = pairwise_plan(n);
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotReduce, plan.scratch_bytes, &buf);
+  if (s != GC_OK) return s;
+  double* a = static_cast<double*>(buf);
+  const size_t smem = sizeof(double) * (padpos(kChunkMax) + 8 + kNodeMax);
+  static bool attr_set[2] = {false, false};
+  auto kern = pairwise_chunks<T>;
+  if (!attr_set[sizeof(T) == 8]) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    attr_set[sizeof(T) == 8] = true;
+  }
+  const long long grid = std::min<long long>(plan.nchunks, static_cast<long long>(ctx->num_sms) * 3);
+  kern<<<static_cast<unsigned>(grid), kSumThreads, smem, ctx->stream>>>(x, n, plan.depth, plan.nchunks, a);
+  GC_CHECK_LAUNCH("pairwise_chunks");
+  return pairwise_finish(ctx, a, plan.nchunks, result);
+}
+
+template <class T>
+gc_status kahan_sum(gc_context* ctx, const T* x, long long n, double* result) {
+  void* buf = nullptr;
+  gc_status s = scratch_get(ctx, kSlotReduce, kKahanScratchBytes, &buf);
+  if (s != GC_OK) return s;
+  double* part = static_cast<double*>(buf);
+  kahan_blocks<T><<<kKahanBlocks, kKahanThreads, 0, ctx->stream>>>(x, n, part);
+  GC_CHECK_LAUNCH("kahan_blocks");
+  return kahan_finish(ctx, part, result);
 }
 
 template gc_status pairwise_sum<double>(gc_context*, const double*, long long, double*);

@@ -439,7 +439,8 @@ def evaluate(field, grid: Grid, integrand, kappa: float = 0.0, tag=Pairwise, ctx
                                C.byref(f), tag.code, C.byref(r)))
         return r.value
     comps = 3 if grid.size > 0 and field.numel() == 3 * grid.size else 1
-    prog = integrand if isinstance(integrand, _integrand.Program) else _integrand.trace(integrand, comps)
+    is_program = hasattr(integrand, "instr") and hasattr(integrand, "arity") and hasattr(integrand, "components")
+    prog = integrand if is_program else _integrand.trace(integrand, comps)
     if prog.components != comps:
         raise ValueError(f"gridcalc_b200: program is for {prog.components} component(s), field has {comps}")
     _require(field, grid, comps)

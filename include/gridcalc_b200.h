@@ -243,6 +243,11 @@ typedef struct gc_program {
  * read before it is written, input beyond the arity) is GC_ERR_INVALID_ARG. */
 GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field,
                                      const gc_program* f, gc_sum sum, double* result);
+/* The CUDA source gc_evaluate_program compiles for f (NVRTC, sm_100a), for
+ * inspection: copies at most cap - 1 characters and a terminating NUL into
+ * buf and returns the full size including the NUL (0 for a malformed
+ * program).  Each distinct source is compiled once per process and device. */
+GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap);
 
 /* ---- time integration (solve::) ----------------------------------------- */
 

@@ -8,11 +8,16 @@ import os
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-_spec = importlib.util.spec_from_file_location(
-    "gc_integrand", os.path.join(ROOT, "grid-calculus_b200", "gridcalc_b200", "integrand.py"))
-integrand = importlib.util.module_from_spec(_spec)
-sys.modules.setdefault("gc_integrand", integrand)
-_spec.loader.exec_module(integrand)
+# The package's own recorder module, shared with the package when both are
+# imported (so symbols and programs are the same classes on either side).
+if "gridcalc_b200.integrand" in sys.modules:
+    integrand = sys.modules["gridcalc_b200.integrand"]
+else:
+    _spec = importlib.util.spec_from_file_location(
+        "gridcalc_b200.integrand", os.path.join(ROOT, "grid-calculus_b200", "gridcalc_b200", "integrand.py"))
+    integrand = importlib.util.module_from_spec(_spec)
+    sys.modules["gridcalc_b200.integrand"] = integrand
+    _spec.loader.exec_module(integrand)
 sqrt, minimum, maximum = integrand.sqrt, integrand.minimum, integrand.maximum
 
 # name -> (components, callable)

@@ -141,3 +141,35 @@ def test_oracle_rejects_inputs_beyond_arity(oracle):
     f = np.zeros((4, 4, 4))
     with pytest.raises(ValueError, match="beyond the arity"):
         oracle.evaluate_program(1, 1, [(1, 0, 1, 0, 0.0)], f)
+
+
+def test_generated_sources_compile_for_sm100a():
+    """The CUDA source gc_evaluate_program generates for every recorded case
+    (both storage types) compiles under NVRTC for sm_100a with the options
+    the library uses (evaluate.cu); no GPU is needed to compile."""
+    import ctypes as C
+    import gridcalc_b200 as gc
+    nv = C.CDLL("/usr/local/cuda/lib64/libnvrtc.so.12")
+    gc.lib.gc_program_source.restype = C.c_size_t
+    gc.lib.gc_program_source.argtypes = [C.POINTER(gc.gc_program), C.c_int, C.c_char_p, C.c_size_t]
+    opts = (C.c_char_p * 3)(b"--gpu-architecture=sm_100a", b"--fmad=false", b"-std=c++17")
+    for name, (comps, fn) in IC.CASES.items():
+        p = gc.program_struct(gc.integrand.trace(fn, comps))
+        for dt in (gc.F64, gc.F32):
+            n = gc.lib.gc_program_source(C.byref(p), dt, None, 0)
+            buf = C.create_string_buffer(n)
+            assert gc.lib.gc_program_source(C.byref(p), dt, buf, n) == n
+            src = buf.value
+            assert (b"#define GC_T double" if dt == gc.F64 else b"#define GC_T float") in src
+            h = C.c_void_p()
+            assert nv.nvrtcCreateProgram(C.byref(h), src, b"gc_integrand.cu", 0, None, None) == 0
+            rc = nv.nvrtcCompileProgram(h, 3, opts)
+            size = C.c_size_t()
+            nv.nvrtcGetProgramLogSize(h, C.byref(size))
+            log = C.create_string_buffer(size.value)
+            nv.nvrtcGetProgramLog(h, log)
+            nv.nvrtcDestroyProgram(C.byref(h))
+            assert rc == 0, (name, dt, log.value.decode())
+    bad = gc.gc_program(1, 1, 1, 0)
+    bad.instr[0] = gc.gc_instr(2, 0, 0, 0, 0.0)   # reads a register never written
+    assert gc.lib.gc_program_source(C.byref(bad), gc.F64, None, 0) == 0
