@@ -510,6 +510,13 @@ def run_case(name: str) -> None:
         g = gc.Grid(n, n, 1)
         x = (0.05 * (2 * torch.rand(1, n, n, device="cuda", dtype=torch.float64) - 1)).float()
         gc.ch_integrate(x, g, gc.CahnHilliardRhs(1.0, 1.0, 2), DT, 32, gc.RK4)
+    elif name == "eval_fe_320":     # func::evaluate of the recorded free energy, 320^3 FP64 (fused NVRTC kernel)
+        n = 320
+        g = gc.Grid(n, n, n, 1 / n, 1 / n, 1 / n)
+        psi = 0.1 * torch.randn(n, n, n, device="cuda", dtype=torch.float64)
+        prog = gc.integrand.trace(lambda p, d: -0.5 * p * p + 0.25 * p * p * p * p + 0.5 * 0.7 * d.squaredNorm())
+        for _ in range(3):
+            gc.evaluate(psi, g, prog)
     else:
         raise SystemExit(f"unknown case {name}")
     torch.cuda.synchronize()
@@ -631,7 +638,7 @@ def main():
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--case", default=None,
                     help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
-                         "batch64_f32, ch_f32_4096")
+                         "batch64_f32, ch_f32_4096, eval_fe_320")
     ap.add_argument("--forms", default="all",
                     help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full "
                          "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")

@@ -74,42 +74,49 @@ __device__ __forceinline__ double gc_integrand(const double* in);
 #define GC_R (GC_COMPS == 1 ? (GC_ARITY >= 4 ? 2 : GC_ARITY >= 2 ? 1 : 0) : (GC_ARITY >= 2 ? 1 : 0))
 #define GC_NIN (GC_COMPS == 1 ? (GC_ARITY == 1 ? 1 : GC_ARITY + 2) : (GC_ARITY == 1 ? 3 : 12))
 
-__device__ __forceinline__ int gc_wrap(int i, int n) {
-  if (i >= 0 && i < n) return i;
-  const int r = i % n;
-  return r < 0 ? r + n : r;
-}
-
-// Order-2 first derivative: taps (-1, 0, 1), weights (-0.5, 0, 0.5), from 0.0.
+// Order-2 first derivative: taps (-1, 0, 1), weights (-0.5, 0, 0.5), from
+// 0.0.  The zero-weight centre tap changes the sum only when the centre is
+// not finite (0 * inf is NaN; for a finite centre s + (+-0) == s, since s
+// is never -0 here), so it is only added then.
 template <class Tap>
-__device__ __forceinline__ double gc_d1(const Tap& tap) {
-  double s = 0.0;
-  s = __dadd_rn(s, __dmul_rn(-0.5, tap(-1)));
-  s = __dadd_rn(s, __dmul_rn(0.0, tap(0)));
+__device__ __forceinline__ double gc_d1(const Tap& tap, double centre) {
+  double s = __dadd_rn(0.0, __dmul_rn(-0.5, tap(-1)));
+  if (!isfinite(centre)) s = __dadd_rn(s, __dmul_rn(0.0, centre));
   return __dadd_rn(s, __dmul_rn(0.5, tap(1)));
 }
 
-__device__ __forceinline__ double gc_cell(const EvalGrid& g, int i, int j, int k) {
-  const GC_T* __restrict__ f = (const GC_T*)g.field;
-  int xs[2 * GC_R + 1];
-  gc_i64 ys[2 * GC_R + 1], zs[2 * GC_R + 1];
+// wrap(i + o, n) - i.  The extent checks leave n >= 2 R + 1 or n == 1, so
+// one correction suffices.
+__device__ __forceinline__ int gc_off(int i, int o, int n) {
+  if (n == 1) return 0;
+  const int t = i + o;
+  return o + (t < 0 ? n : 0) - (t >= n ? n : 0);
+}
+
+__device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
+  const GC_T* __restrict__ p = (const GC_T*)g.field + c;
+  gc_i64 xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
   const gc_i64 plane = (gc_i64)g.nx * g.ny;
 #pragma unroll
   for (int m = 0; m <= 2 * GC_R; ++m) {
-    xs[m] = gc_wrap(i + m - GC_R, g.nx);
-    ys[m] = (gc_i64)gc_wrap(j + m - GC_R, g.ny) * g.nx;
-    zs[m] = (gc_i64)gc_wrap(k + m - GC_R, g.nz) * plane;
+    xo[m] = gc_off(i, m - GC_R, g.nx);
+    yo[m] = (gc_i64)gc_off(j, m - GC_R, g.ny) * g.nx;
+    zo[m] = (gc_i64)gc_off(k, m - GC_R, g.nz) * plane;
   }
-  auto v = [&](int c, int ox, int oy, int oz) -> double {
-    return (double)__ldg(f + (gc_i64)c * g.n + zs[oz + GC_R] + ys[oy + GC_R] + xs[ox + GC_R]);
+  auto v = [&](int comp, int ox, int oy, int oz) -> double {
+    gc_i64 off = (gc_i64)comp * g.n;
+    if (ox) off += xo[ox + GC_R];
+    if (oy) off += yo[oy + GC_R];
+    if (oz) off += zo[oz + GC_R];
+    return (double)__ldg(p + off);
   };
   double in[GC_NIN];
 #if GC_COMPS == 1
   in[0] = v(0, 0, 0, 0);
 #if GC_ARITY >= 2
-  in[1] = __dmul_rn(gc_d1([&](int o) { return v(0, o, 0, 0); }), g.ihx);
-  in[2] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, o, 0); }), g.ihy);
-  in[3] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, 0, o); }), g.ihz);
+  in[1] = __dmul_rn(gc_d1([&](int o) { return v(0, o, 0, 0); }, in[0]), g.ihx);
+  in[2] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, o, 0); }, in[0]), g.ihy);
+  in[3] = __dmul_rn(gc_d1([&](int o) { return v(0, 0, 0, o); }, in[0]), g.ihz);
 #endif
 #if GC_ARITY >= 3
   {  // Laplacian, taps (1, -2, 1) from 0.0 (diff/Laplacian.hpp:60-69)
@@ -159,9 +166,9 @@ __device__ __forceinline__ double gc_cell(const EvalGrid& g, int i, int j, int k
 #if GC_ARITY >= 2
 #pragma unroll
   for (int r = 0; r < 3; ++r) {  // M(r, c) = d_c u_r (diff/Gradient.hpp:115-131)
-    in[3 + 3 * r + 0] = __dmul_rn(gc_d1([&](int o) { return v(r, o, 0, 0); }), g.ihx);
-    in[3 + 3 * r + 1] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, o, 0); }), g.ihy);
-    in[3 + 3 * r + 2] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, 0, o); }), g.ihz);
+    in[3 + 3 * r + 0] = __dmul_rn(gc_d1([&](int o) { return v(r, o, 0, 0); }, in[r]), g.ihx);
+    in[3 + 3 * r + 1] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, o, 0); }, in[r]), g.ihy);
+    in[3 + 3 * r + 2] = __dmul_rn(gc_d1([&](int o) { return v(r, 0, 0, o); }, in[r]), g.ihz);
   }
 #endif
 #endif
@@ -212,7 +219,7 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGri
     int i, j, k;
     gc_locate(g, lo + threadIdx.x, i, j, k);
     for (int e = threadIdx.x; e < len; e += 256) {
-      s[gc_padpos(e)] = gc_cell(g, i, j, k);
+      s[gc_padpos(e)] = gc_cell(g, lo + e, i, j, k);
       gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
     }
     int d2 = 0;
@@ -275,7 +282,7 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_kahan(const EvalGrid g
     int i, j, k;
     gc_locate(g, first, i, j, k);
     for (gc_i64 c = first; c < g.n; c += (gc_i64)1024 * 256) {
-      acc = gc_neumaier_add(acc, gc_cell(g, i, j, k));
+      acc = gc_neumaier_add(acc, gc_cell(g, c, i, j, k));
       gc_advance(i, j, k, g.nx, g.ny, g.kstep_i, g.kstep_j, g.kstep_k);
     }
   }

@@ -136,3 +136,19 @@ def test_malformed_programs_are_rejected(gc, comps, arity, rows, msg):
                                     field.data_ptr(), C.byref(p), 0, C.byref(r))
     assert gc.STATUS[st] == "GC_ERR_INVALID_ARG"
     assert msg in gc.lib.gc_last_error().decode()
+
+
+def test_non_finite_values_propagate_like_the_reference(gc, oracle):
+    """An infinite value: the zero-weight centre tap of the gradient gives
+    0 * inf = NaN in the reference's sum, and so here; a value-only
+    integrand keeps the infinity."""
+    import math
+    shape, h = (6, 7, 8), (1.0, 1.0, 1.0)
+    f = np.random.default_rng(8).standard_normal(shape)
+    f[3, 4, 5] = np.inf
+    g = _grid(gc, shape, h)
+    grad_only = lambda p, d: d[0] * d[0]  # noqa: E731
+    want = oracle.evaluate_program(1, 2, IC.integrand.trace(grad_only).instr, f, h)
+    got = gc.evaluate(_dev(f), g, grad_only)
+    assert math.isnan(want) and math.isnan(got)
+    assert gc.evaluate(_dev(f), g, lambda p: p) == oracle.evaluate_program(1, 1, IC.integrand.trace(lambda p: p).instr, f, h) == math.inf
