@@ -38,13 +38,12 @@ namespace gcb {
 namespace {
 
 constexpr int kChunkCells = 8192;   // pairwise chunk bound (pairwise.cuh kChunkMax)
-constexpr int kEvalThreads = 1024;  // chunk-walk block (the compensated sum keeps its own shape)
+constexpr int kEvalThreads = 256;
 
 // Kernel argument; the device source declares the same layout.
 struct EvalGrid {
   const void* field;
   long long n;
-  long long sx, sy, sz;           // flat stride of one step along x, y, z (0 on an axis of extent 1)
   int nx, ny, nz;
   int step_i, step_j, step_k;     // kEvalThreads cells as (di, dj, dk)
   int kstep_i, kstep_j, kstep_k;  // the compensated sum's stride as (di, dj, dk)
@@ -63,7 +62,6 @@ typedef long long gc_i64;
 struct EvalGrid {
   const void* field;
   gc_i64 n;
-  gc_i64 sx, sy, sz;
   int nx, ny, nz;
   int step_i, step_j, step_k;
   int kstep_i, kstep_j, kstep_k;
@@ -95,14 +93,22 @@ __device__ __forceinline__ int gc_off(int i, int o, int n) {
   return o + (t < 0 ? n : 0) - (t >= n ? n : 0);
 }
 
-__device__ __forceinline__ bool gc_inside(int i, int n) { return n == 1 || (i >= GC_R && i < n - GC_R); }
-
-// Inputs of the arity and the integrand at the cell p points to; off(ox, oy,
-// oz) is the flat offset of a neighbour.
-template <class Off>
-__device__ __forceinline__ double gc_cell_at(const EvalGrid& g, const GC_T* __restrict__ p, const Off& off) {
+__device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
+  const GC_T* __restrict__ p = (const GC_T*)g.field + c;
+  gc_i64 xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+  const gc_i64 plane = (gc_i64)g.nx * g.ny;
+#pragma unroll
+  for (int m = 0; m <= 2 * GC_R; ++m) {
+    xo[m] = gc_off(i, m - GC_R, g.nx);
+    yo[m] = (gc_i64)gc_off(j, m - GC_R, g.ny) * g.nx;
+    zo[m] = (gc_i64)gc_off(k, m - GC_R, g.nz) * plane;
+  }
   auto v = [&](int comp, int ox, int oy, int oz) -> double {
-    return (double)__ldg(p + (gc_i64)comp * g.n + off(ox, oy, oz));
+    gc_i64 off = (gc_i64)comp * g.n;
+    if (ox) off += xo[ox + GC_R];
+    if (oy) off += yo[oy + GC_R];
+    if (oz) off += zo[oz + GC_R];
+    return (double)__ldg(p + off);
   };
   double in[GC_NIN];
 #if GC_COMPS == 1
@@ -169,25 +175,6 @@ __device__ __forceinline__ double gc_cell_at(const EvalGrid& g, const GC_T* __re
   return gc_integrand(in);
 }
 
-// Interior cells (the common case) take neighbour offsets that are
-// multiples of the axis strides; cells within R of a face wrap.
-__device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
-  const GC_T* __restrict__ p = (const GC_T*)g.field + c;
-  if (gc_inside(i, g.nx) && gc_inside(j, g.ny) && gc_inside(k, g.nz))
-    return gc_cell_at(g, p, [&](int ox, int oy, int oz) { return ox * g.sx + oy * g.sy + oz * g.sz; });
-  int xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
-#pragma unroll
-  for (int m = 0; m <= 2 * GC_R; ++m) {
-    xo[m] = gc_off(i, m - GC_R, g.nx);
-    yo[m] = gc_off(j, m - GC_R, g.ny);
-    zo[m] = gc_off(k, m - GC_R, g.nz);
-  }
-  const gc_i64 plane = (gc_i64)g.nx * g.ny;
-  return gc_cell_at(g, p, [&](int ox, int oy, int oz) {
-    return (gc_i64)xo[ox + GC_R] + (gc_i64)yo[oy + GC_R] * g.nx + (gc_i64)zo[oz + GC_R] * plane;
-  });
-}
-
 // (i, j, k) += a step given as (di, dj, dk) with di < nx, dj < ny.
 __device__ __forceinline__ void gc_advance(int& i, int& j, int& k, int nx, int ny, int di, int dj, int dk) {
   i += di;
@@ -220,7 +207,7 @@ __device__ __forceinline__ double gc_seq_sum(const double* s, int a, int b) {
   return acc;
 }
 
-extern "C" __global__ void __launch_bounds__(1024) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
+extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
                                                                    double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* s = (double*)smem_raw;
@@ -231,7 +218,7 @@ extern "C" __global__ void __launch_bounds__(1024) gc_eval_pairwise(const EvalGr
     const int len = (int)(hi - lo);
     int i, j, k;
     gc_locate(g, lo + threadIdx.x, i, j, k);
-    for (int e = threadIdx.x; e < len; e += 1024) {
+    for (int e = threadIdx.x; e < len; e += 256) {
       s[gc_padpos(e)] = gc_cell(g, lo + e, i, j, k);
       gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
     }
@@ -313,7 +300,7 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_kahan(const EvalGrid g
 )GCSRC";
 
 static_assert(kKahanBlocks == 1024 && kKahanThreads == 256, "the device source bakes in the compensated sum's shape");
-static_assert(kEvalThreads == 1024, "the device source bakes in 1024 threads per chunk-walk block");
+static_assert(kEvalThreads == 256, "the device source bakes in 256 threads per block");
 
 constexpr int n_inputs(int comps, int arity) {
   return comps == 1 ? (arity == 1 ? 1 : arity + 2) : (arity == 1 ? 3 : 12);
@@ -515,9 +502,6 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   a.field = field;
   a.n = n;
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-  a.sx = g->nx == 1 ? 0 : 1;
-  a.sy = g->ny == 1 ? 0 : static_cast<long long>(g->nx);
-  a.sz = g->nz == 1 ? 0 : static_cast<long long>(g->nx) * g->ny;
   split_step(kEvalThreads, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
   split_step(static_cast<long long>(kKahanBlocks) * kKahanThreads, g->nx, g->ny, &a.kstep_i, &a.kstep_j, &a.kstep_k);
   a.ihx = 1.0 / g->hx; a.ihy = 1.0 / g->hy; a.ihz = 1.0 / g->hz;
@@ -540,8 +524,7 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
     int depth = plan.depth;
     long long nchunks = plan.nchunks;
     void* args[] = {&a, &depth, &nchunks, &partial};
-    // Two 1024-thread blocks (64 KB of chunk each) fill an SM.
-    const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 2));
+    const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3));
     const unsigned smem = static_cast<unsigned>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
     if (drv.launch(k.pairwise, grid, 1, 1, kEvalThreads, 1, 1, smem, ctx->stream, args, nullptr) != CUDA_SUCCESS)
       return fail(GC_ERR_CUDA, "gc_evaluate_program: launch failed");
