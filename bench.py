@@ -435,9 +435,76 @@ def form_learned(gc, n_train=32, n_eval=4, fine_steps=5000, t_end=200.0, tols=(0
             "train": tr, "residual_profile": prof["rows"], "eval": ev}
 
 
+def form_snapshots(gc, steps=2000, every=500):
+    """The headline run (8192^2 FP64 RK4 Cahn-Hilliard) with a checkpoint of
+    the state every `every` steps through the asynchronous snapshotter,
+    against the same chunked run without: what snapshots add to the device
+    timeline.  Plus the synchronous ASCII VTK writer's rate at 1024^2."""
+    import shutil
+    import tempfile
+    import numpy as np
+    import torch
+    g = gc.Grid(NX, NX, 1)
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    psi0 = 0.05 * (2 * torch.rand((1, NX, NX), generator=gen, device="cuda", dtype=torch.float64) - 1)
+    chunks = steps // every
+    out = {"workload": f"{NX}x{NX} FP64 RK4 CH, {steps} steps, checkpoint every {every}",
+           "bytes_per_snapshot": NX * NX * 8}
+
+    def run(snap, d):
+        psi = psi0.clone()
+        gc.ch_integrate(psi, g, rhs, DT, 2, gc.RK4)
+        psi.copy_(psi0)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        s.record()
+        for c in range(chunks):
+            gc.ch_integrate(psi, g, rhs, DT, every, gc.RK4)
+            if snap is not None:
+                snap.checkpoint(psi, g, os.path.join(d, f"state_{c}.gcb"), {"step": (c + 1) * every})
+        e.record()
+        torch.cuda.synchronize()
+        device_ms = s.elapsed_time(e)
+        if snap is not None:
+            snap.flush()
+        return psi, device_ms, time.perf_counter() - t0
+
+    _, plain_ms, _ = run(None, None)
+    d = tempfile.mkdtemp(prefix="gc_snapshots_")
+    try:
+        with gc.Snapshotter(depth=3) as snap:
+            psi, snap_ms, wall = run(snap, d)
+        back, _, meta = gc.load_checkpoint(os.path.join(d, f"state_{chunks - 1}.gcb"), device="cuda")
+        out["last_checkpoint_equals_state"] = bool(torch.equal(back, psi)) and meta == {"step": chunks * every}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    out.update({"ms_per_step_plain": plain_ms / steps, "ms_per_step_with_snapshots": snap_ms / steps,
+                "overhead_pct": 100.0 * (snap_ms - plain_ms) / plain_ms, "snapshots": chunks,
+                "wall_s_until_all_written": wall,
+                "written_GB_per_s": chunks * NX * NX * 8 / wall / 1e9})
+    f = np.random.default_rng(1).standard_normal((1, 1024, 1024))
+    d = tempfile.mkdtemp(prefix="gc_vtk_")
+    try:
+        t0 = time.perf_counter()
+        gc.write_vtk(f, gc.Grid(1024, 1024, 1), os.path.join(d, "psi.vtk"), "psi")
+        dt_ascii = time.perf_counter() - t0
+        size = os.path.getsize(os.path.join(d, "psi.vtk"))
+        t0 = time.perf_counter()
+        gc.write_vtk(f, gc.Grid(1024, 1024, 1), os.path.join(d, "psi_b.vtk"), "psi", binary=True)
+        dt_bin = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    out["vtk_1024x1024"] = {"ascii_s": dt_ascii, "ascii_MB": size / 1e6, "binary_s": dt_bin,
+                            "ascii_Mvalues_per_s": 1024 * 1024 / dt_ascii / 1e6}
+    return out
+
+
 def run_forms(gc, names, peak):
     forms = {}
     table = {"operators": lambda: form_operators(gc, peak), "fvm": lambda: form_fvm(gc, peak),
+             "snapshots": lambda: form_snapshots(gc),
              "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc),
              # the learned workload at its full size: 512 training trajectories, 64 held-out seeds
              "learned_full": lambda: form_learned(gc, n_train=512, n_eval=64, tols=(0.003, 0.01))}
@@ -640,7 +707,7 @@ def main():
                     help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
                          "batch64_f32, ch_f32_4096, eval_fe_320")
     ap.add_argument("--forms", default="all",
-                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full "
+                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full,snapshots "
                          "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)

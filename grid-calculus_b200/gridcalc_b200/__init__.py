@@ -29,6 +29,7 @@ __all__ = [
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
     "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct",
+    "write_vtk", "save_checkpoint", "checkpoint_info", "load_checkpoint", "Snapshotter",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -723,5 +724,131 @@ class Corrector:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+# --- snapshot output and checkpoints (examples/common/vtk_writer.hpp:34) ---
+lib.gc_write_vtk.argtypes = [C.POINTER(gc_grid), C.c_int, C.c_void_p, C.c_char_p, C.c_char_p, C.c_int]
+lib.gc_write_checkpoint.argtypes = [C.POINTER(gc_grid), C.c_int, C.c_int32, C.c_void_p, C.c_char_p, C.c_char_p]
+lib.gc_checkpoint_info.argtypes = [C.c_char_p, C.POINTER(gc_grid), C.POINTER(C.c_int), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_size_t)]
+lib.gc_read_checkpoint.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t]
+lib.gc_load_checkpoint.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t]
+lib.gc_snapshotter_create.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]
+lib.gc_snapshot_vtk.argtypes = [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_void_p, C.c_char_p, C.c_char_p, C.c_int]
+lib.gc_snapshot_checkpoint.argtypes = [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_int32, C.c_void_p, C.c_char_p,
+                                       C.c_char_p]
+lib.gc_snapshotter_flush.argtypes = [C.c_void_p]
+lib.gc_snapshotter_destroy.argtypes = [C.c_void_p]
+for _f in ("gc_write_vtk", "gc_write_checkpoint", "gc_checkpoint_info", "gc_read_checkpoint", "gc_load_checkpoint",
+           "gc_snapshotter_create", "gc_snapshot_vtk", "gc_snapshot_checkpoint", "gc_snapshotter_flush",
+           "gc_snapshotter_destroy"):
+    getattr(lib, _f).restype = C.c_int
+
+
+def _host_array(field):
+    import numpy as np
+    a = field.detach().cpu().numpy() if hasattr(field, "detach") else np.asarray(field)
+    a = np.ascontiguousarray(a)
+    if a.dtype == np.float64:
+        return a, F64
+    if a.dtype == np.float32:
+        return a, F32
+    raise ValueError(f"gridcalc_b200: fields must be float64 or float32, got {a.dtype}")
+
+
+def _components(n: int, grid: Grid) -> int:
+    if n % grid.size:
+        raise ValueError(f"gridcalc_b200: field has {n} values, not a multiple of the grid's {grid.size}")
+    return n // grid.size
+
+
+def write_vtk(field, grid: Grid, path: str, name: str = "psi", binary: bool = False) -> None:
+    """gridcalc::examples::writeVtkStructuredPoints (examples/common/vtk_writer.hpp:34):
+    the reference's ASCII file byte for byte, or the same header with
+    big-endian doubles (binary=True).  field: numpy array or tensor."""
+    a, dt = _host_array(field)
+    if a.size != grid.size:
+        raise ValueError(f"gridcalc_b200: field has {a.size} values, grid needs {grid.size}")
+    _check(lib.gc_write_vtk(C.byref(grid.c()), dt, a.ctypes.data, os.fsencode(path), name.encode(), int(binary)))
+
+
+def save_checkpoint(field, grid: Grid, path: str, meta: dict | None = None) -> None:
+    """Writes a checkpoint (header, JSON metadata, the field's planes)."""
+    import json
+    a, dt = _host_array(field)
+    _check(lib.gc_write_checkpoint(C.byref(grid.c()), dt, _components(a.size, grid), a.ctypes.data,
+                                   os.fsencode(path), json.dumps(meta or {}).encode()))
+
+
+def checkpoint_info(path: str):
+    """(Grid, 'f64' | 'f32', components, metadata length) of a checkpoint."""
+    g, dt, comps, mlen = gc_grid(), C.c_int(), C.c_int32(), C.c_size_t()
+    _check(lib.gc_checkpoint_info(os.fsencode(path), C.byref(g), C.byref(dt), C.byref(comps), C.byref(mlen)))
+    return Grid(g.nx, g.ny, g.nz, g.hx, g.hy, g.hz), ("f64" if dt.value == F64 else "f32"), comps.value, mlen.value
+
+
+def load_checkpoint(path: str, device=None, ctx=None):
+    """Reads a checkpoint: (field, Grid, metadata dict).  device None: a numpy
+    array; a CUDA device: a tensor filled on the context's stream."""
+    import json
+    import numpy as np
+    grid, dts, comps, mlen = checkpoint_info(path)
+    shape = grid.shape if comps == 1 else (comps,) + grid.shape
+    meta = C.create_string_buffer(mlen + 1)
+    if device is None:
+        a = np.empty(shape, dtype=np.float64 if dts == "f64" else np.float32)
+        _check(lib.gc_read_checkpoint(os.fsencode(path), a.ctypes.data, a.nbytes, meta, mlen + 1))
+        return a, grid, json.loads(meta.value.decode() or "{}")
+    import torch
+    t = torch.empty(shape, dtype=torch.float64 if dts == "f64" else torch.float32, device=device)
+    _check(lib.gc_load_checkpoint(_ctx(ctx), os.fsencode(path), t.data_ptr(), t.numel() * t.element_size(), meta,
+                                  mlen + 1))
+    return t, grid, json.loads(meta.value.decode() or "{}")
+
+
+class Snapshotter:
+    """Snapshots of device fields that overlap the computation: each call
+    copies the field into a device slot on the context's stream and
+    returns; the slot reaches pinned host memory on a copy stream and a
+    writer thread writes the file.  ``flush()`` waits for every file."""
+
+    def __init__(self, depth: int = 2, ctx=None):
+        self._ctx = ctx or context()
+        self.handle = C.c_void_p()
+        _check(lib.gc_snapshotter_create(self._ctx.handle, depth, C.byref(self.handle)))
+
+    def vtk(self, field, grid: Grid, path: str, name: str = "psi", binary: bool = False) -> None:
+        _require(field, grid)
+        _check(lib.gc_snapshot_vtk(self.handle, C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                                   os.fsencode(path), name.encode(), int(binary)))
+
+    def checkpoint(self, field, grid: Grid, path: str, meta: dict | None = None) -> None:
+        import json
+        if not field.is_cuda or not field.is_contiguous():
+            raise ValueError("gridcalc_b200: snapshots take contiguous CUDA tensors")
+        _check(lib.gc_snapshot_checkpoint(self.handle, C.byref(grid.c()), _dtype_code(field),
+                                          _components(field.numel(), grid), field.data_ptr(), os.fsencode(path),
+                                          json.dumps(meta or {}).encode()))
+
+    def flush(self) -> None:
+        _check(lib.gc_snapshotter_flush(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            h, self.handle = self.handle, C.c_void_p()
+            _check(lib.gc_snapshotter_destroy(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib.gc_snapshotter_destroy(self.handle)
         except Exception:
             pass

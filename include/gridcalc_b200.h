@@ -395,6 +395,55 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
                                       int32_t n_coarse, const gc_corrector_policy* pol,
                                       gc_corrector_stats* stats);
 
+/* ---- snapshot output and checkpoint / resume ---------------------------- */
+
+typedef enum gc_vtk_encoding { GC_VTK_ASCII = 0, GC_VTK_BINARY = 1 } gc_vtk_encoding;
+
+/* gridcalc::examples::writeVtkStructuredPoints (examples/common/vtk_writer.hpp:34-66):
+ * legacy VTK 3.0 STRUCTURED_POINTS with one SCALARS array of doubles, i
+ * fastest.  GC_VTK_ASCII writes the reference's bytes exactly (17
+ * significant digits per value); GC_VTK_BINARY the same header with
+ * big-endian doubles.  host: the field in host memory (dt values, float
+ * written as double).  Needs no device. */
+GC_API gc_status gc_write_vtk(const gc_grid* g, gc_dtype dt, const void* host, const char* path,
+                              const char* field_name, gc_vtk_encoding enc);
+
+/* Checkpoint file: an 80-byte little-endian header (magic "GCB200CK",
+ * version 1, dtype, nx ny nz, components, hx hy hz, data bytes, metadata
+ * bytes, 64-bit checksum of the data), the metadata (e.g. JSON: step, time,
+ * parameters), then `components` planes of the field, i fastest.  Written
+ * under a temporary name and renamed.  Needs no device. */
+GC_API gc_status gc_write_checkpoint(const gc_grid* g, gc_dtype dt, int32_t components, const void* host,
+                                     const char* path, const char* meta_json);
+/* The header of a checkpoint: grid, dtype, components and metadata length. */
+GC_API gc_status gc_checkpoint_info(const char* path, gc_grid* g, gc_dtype* dt, int32_t* components,
+                                    size_t* meta_len);
+/* Reads the field into host memory (host_bytes >= its size) and the
+ * metadata into meta (NUL-terminated, at most meta_cap - 1 characters; may
+ * be NULL); a checksum mismatch is GC_ERR_INVALID_ARG. */
+GC_API gc_status gc_read_checkpoint(const char* path, void* host, size_t host_bytes, char* meta, size_t meta_cap);
+/* The same into a device buffer, ordered on the context's stream (returns
+ * after the copy). */
+GC_API gc_status gc_load_checkpoint(gc_context* ctx, const char* path, void* field, size_t field_bytes, char* meta,
+                                    size_t meta_cap);
+
+/* Snapshots of device fields that do not stall the computation: each call
+ * copies the field device-to-device on the context's stream into one of
+ * `depth` slots (so later work may overwrite the field at once), a copy
+ * stream moves the slot to pinned host memory while later work runs, and a
+ * writer thread writes the file.  A call waits only when all slots still
+ * hold unwritten snapshots.  One thread at a time per snapshotter. */
+typedef struct gc_snapshotter gc_snapshotter;
+GC_API gc_status gc_snapshotter_create(gc_context* ctx, int32_t depth, gc_snapshotter** out);
+GC_API gc_status gc_snapshot_vtk(gc_snapshotter* s, const gc_grid* g, gc_dtype dt, const void* field,
+                                 const char* path, const char* field_name, gc_vtk_encoding enc);
+GC_API gc_status gc_snapshot_checkpoint(gc_snapshotter* s, const gc_grid* g, gc_dtype dt, int32_t components,
+                                        const void* field, const char* path, const char* meta_json);
+/* Waits until every queued file is written; returns the first write error. */
+GC_API gc_status gc_snapshotter_flush(gc_snapshotter* s);
+/* Flushes, stops the writer thread and frees the slots. */
+GC_API gc_status gc_snapshotter_destroy(gc_snapshotter* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,7 @@
 #include <gridcalc/solve/Integrator.hpp>
 
 #include <common/cahn_hilliard.hpp>
+#include <common/vtk_writer.hpp>
 
 namespace {
 
@@ -319,6 +320,15 @@ int ref_evaluate_program(int components, int arity, int nx, int ny, int nz, doub
     } else {
       throw std::invalid_argument("ref: components must be 1 or 3");
     }
+  });
+}
+
+// examples/common/vtk_writer.hpp:34-66, the reference's snapshot writer.
+int ref_write_vtk(int nx, int ny, int nz, double hx, double hy, double hz, const double* f, const char* path,
+                  const char* name) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    gridcalc::examples::writeVtkStructuredPoints(load(g, f), path, name);
   });
 }
 

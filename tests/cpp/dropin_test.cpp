@@ -17,6 +17,8 @@
 #include <gridcalc/solve/Diffusion.hpp>
 #include <gridcalc/solve/Integrator.hpp>
 
+#include <common/vtk_writer.hpp>
+
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -171,6 +173,33 @@ int main() {
     const double tr = gridcalc::func::evaluate(u, [](const auto&, const auto& M) { return M.trace(); });
     const double dv = gridcalc::func::integrate(gridcalc::diff::divergence(u));
     require(fe == fe_dev && std::isfinite(b4) && tr == dv, "func::evaluate with recorded callables");
+  }
+  {  // examples/common/vtk_writer.hpp: header lines and 17-digit values
+    Grid g(3, 2, 1, Vec3d(0.5, 0.25, 1.0));
+    Field<double> f(g, [](double x, double y, double) { return x / 3.0 - y; });
+    const std::string path = "dropin_snapshot.vtk";
+    gridcalc::examples::writeVtkStructuredPoints(f, path, "psi");
+    std::FILE* in = std::fopen(path.c_str(), "r");
+    char line[128];
+    int lines = 0;
+    bool ok = in != nullptr;
+    std::string eleventh, spacing;
+    while (ok && std::fgets(line, sizeof line, in)) {
+      ++lines;
+      if (lines == 7) spacing = line;
+      if (lines == 11) eleventh = line;
+    }
+    if (in) std::fclose(in);
+    std::remove(path.c_str());
+    char want[64];
+    std::snprintf(want, sizeof want, "%.17g\n", f.data()[0]);
+    bool threw = false;
+    try {
+      gridcalc::examples::writeVtkStructuredPoints(f, "no/such/dir/x.vtk", "psi");
+    } catch (const std::runtime_error&) {
+      threw = true;
+    }
+    require(ok && lines == 16 && spacing == "SPACING 0.5 0.25 1\n" && eleventh == want && threw, "vtk writer");
   }
   std::printf("version %s\n", gridcalc::version());
   return 0;

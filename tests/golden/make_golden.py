@@ -101,6 +101,16 @@ def main() -> None:
         out[f"program/{cname}"] = integrand_cases.rows(prog)
         out[f"program/{cname}_shape"] = np.array([prog.components, prog.arity])
 
+    # A snapshot written by the reference's VTK writer, with values that pin
+    # its number formatting (signed zero, extremes, non-finite, inexact decimals).
+    vals = np.concatenate([rng.standard_normal(48),
+                           [-0.0, 0.0, 1e-300, -1e300, 0.1, 1.0 / 3.0, 2.0 ** -1074, np.inf, -np.inf, np.nan,
+                            123456789012345678.0, 5e-324]])
+    snap = vals.reshape(3, 4, 5)
+    out["vtk/values"] = snap
+    out["vtk/h"] = np.array([0.3, 0.25, 0.5])
+    ref.write_vtk(snap, os.path.join(HERE, "reference_snapshot.vtk"), "psi", (0.3, 0.25, 0.5))
+
     path = os.path.join(HERE, "reference_vectors.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path} ({os.path.getsize(path)} bytes, {len(out)} arrays)")

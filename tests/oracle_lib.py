@@ -194,6 +194,11 @@ class Reference(_Lib):
     def __init__(self):
         super().__init__(REF_SO, "ref_")
 
+    def write_vtk(self, f, path: str, name: str, h=(1.0, 1.0, 1.0)) -> None:
+        """examples/common/vtk_writer.hpp: the reference's ASCII snapshot file."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        self._rc(self.lib.ref_write_vtk(*self._g(f.shape, h), _ptr(f), path.encode(), name.encode()))
+
     def make_random_ic(self, shape, seed: int, amplitude: float, h=(1.0, 1.0, 1.0)):
         out = np.zeros(shape)
         self.lib.ref_make_random_ic(*self._g(shape, h), C.c_uint64(seed), _d(amplitude), _ptr(out))
