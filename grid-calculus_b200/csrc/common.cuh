@@ -80,6 +80,7 @@ enum ScratchSlot {
   kSlotIntegrand,
   kSlotFlags,
   kSlotMisc,
+  kSlotSpectral,
 };
 
 gc_status scratch_get(gc_context* ctx, int slot, size_t bytes, void** out);

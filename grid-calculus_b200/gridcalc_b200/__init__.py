@@ -30,6 +30,7 @@ __all__ = [
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
     "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct",
     "write_vtk", "save_checkpoint", "checkpoint_info", "load_checkpoint", "Snapshotter",
+    "spectral_partial", "spectral_laplacian", "spectral_biharmonic", "spectral_gradient",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -852,3 +853,51 @@ class Snapshotter:
                 lib.gc_snapshotter_destroy(self.handle)
         except Exception:
             pass
+
+
+# --- spectral derivatives (spectral/Derivatives.hpp) ----------------------
+for _f, _args in (("gc_spectral_partial", [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_void_p]),
+                  ("gc_spectral_laplacian", [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_void_p, C.c_void_p]),
+                  ("gc_spectral_biharmonic", [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_void_p, C.c_void_p]),
+                  ("gc_spectral_gradient", [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_void_p, C.c_void_p])):
+    getattr(lib, _f).argtypes = _args
+    getattr(lib, _f).restype = C.c_int
+
+
+def spectral_partial(field, grid: Grid, counts, out=None, ctx=None):
+    """spectral::partial<ax, ay, az> (spectral/Derivatives.hpp:78-134): the
+    FFT derivative d^(ax+ay+az) f / dx^ax dy^ay dz^az of a float64 field."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    ax, ay, az = counts
+    _check(lib.gc_spectral_partial(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), ax, ay, az, field.data_ptr(),
+                                   out.data_ptr()))
+    return out
+
+
+def spectral_laplacian(field, grid: Grid, out=None, ctx=None):
+    """spectral::laplacian (spectral/Derivatives.hpp:144-172)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    _check(lib.gc_spectral_laplacian(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                                     out.data_ptr()))
+    return out
+
+
+def spectral_biharmonic(field, grid: Grid, out=None, ctx=None):
+    """spectral::biharmonic (spectral/Derivatives.hpp:175-204)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid) if out is None else out
+    _check(lib.gc_spectral_biharmonic(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                                      out.data_ptr()))
+    return out
+
+
+def spectral_gradient(field, grid: Grid, out=None, ctx=None):
+    """spectral::gradient (spectral/Derivatives.hpp:207-240); out (3, nz, ny, nx)."""
+    _require(field, grid)
+    out = _empty_like_grid(field, grid, 3) if out is None else out
+    _check(lib.gc_spectral_gradient(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
+                                    out.data_ptr()))
+    return out

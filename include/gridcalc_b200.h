@@ -395,6 +395,22 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
                                       int32_t n_coarse, const gc_corrector_policy* pol,
                                       gc_corrector_stats* stats);
 
+/* ---- spectral derivatives (spectral/Derivatives.hpp, Wavenumbers.hpp) ----
+ * FFT-based derivatives of a periodic double field: forward real-to-complex
+ * transform, the derivative's multiplier on the half spectrum, inverse
+ * transform.  Wavenumbers k = 2 pi n / (N h); an odd derivative count along
+ * an axis of even extent zeroes that axis's Nyquist mode.  Double fields
+ * only; Nx = 1 with another axis longer than 1 is GC_ERR_UNSUPPORTED.
+ * Agrees with the reference's PocketFFT path to rounding. */
+/* spectral::partial<ax, ay, az> (spectral/Derivatives.hpp:78-134), counts 0..8. */
+GC_API gc_status gc_spectral_partial(gc_context* ctx, const gc_grid* g, gc_dtype dt, int ax, int ay, int az,
+                                     const void* in, void* out);
+/* spectral::laplacian (:144-172) and spectral::biharmonic (:175-204). */
+GC_API gc_status gc_spectral_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in, void* out);
+GC_API gc_status gc_spectral_biharmonic(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in, void* out);
+/* spectral::gradient (:207-240): three planes out. */
+GC_API gc_status gc_spectral_gradient(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* in, void* out3);
+
 /* ---- snapshot output and checkpoint / resume ---------------------------- */
 
 typedef enum gc_vtk_encoding { GC_VTK_ASCII = 0, GC_VTK_BINARY = 1 } gc_vtk_encoding;

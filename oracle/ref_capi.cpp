@@ -12,7 +12,9 @@
 // message available from ref_last_error().
 #include <algorithm>
 #include <cmath>
+#include <array>
 #include <cstdint>
+#include <utility>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -31,6 +33,7 @@
 #include <gridcalc/fvm/CellLaplacian.hpp>
 #include <gridcalc/solve/Diffusion.hpp>
 #include <gridcalc/solve/Integrator.hpp>
+#include <gridcalc/spectral/Derivatives.hpp>
 
 #include <common/cahn_hilliard.hpp>
 #include <common/vtk_writer.hpp>
@@ -44,6 +47,19 @@ using gridcalc::core::Vec3d;
 namespace ch = gridcalc::examples::cahn_hilliard;
 
 thread_local std::string g_err;
+
+// spectral::partial<A, B, C> for every count triple 0..4 (runtime dispatch).
+template <int A, int B, int C>
+void spectralPartial(const Field<double>& f, double* out) {
+  const Field<double> r = gridcalc::spectral::partial<A, B, C>(f);
+  std::memcpy(out, r.data(), sizeof(double) * r.getSize());
+}
+using SpectralFn = void (*)(const Field<double>&, double*);
+template <int... I>
+constexpr std::array<SpectralFn, sizeof...(I)> spectralTable(std::integer_sequence<int, I...>) {
+  return {&spectralPartial<I / 25, (I / 5) % 5, I % 5>...};
+}
+const std::array<SpectralFn, 125> kSpectral = spectralTable(std::make_integer_sequence<int, 125>{});
 
 // A straight-line register program standing in for a callable (the layout
 // of gc_instr / oc_instr): r[dst] = op(r[a], r[b]), a constant or input a.
@@ -329,6 +345,33 @@ int ref_write_vtk(int nx, int ny, int nz, double hx, double hy, double hz, const
   return guarded([&] {
     const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
     gridcalc::examples::writeVtkStructuredPoints(load(g, f), path, name);
+  });
+}
+
+// spectral/Derivatives.hpp: the reference's PocketFFT path.  op: 0 partial
+// (counts ax, ay, az in 0..4), 1 laplacian, 2 biharmonic, 3 gradient (out: 3 planes).
+int ref_spectral(int op, int ax, int ay, int az, int nx, int ny, int nz, double hx, double hy, double hz,
+                 const double* in, double* out) {
+  return guarded([&] {
+    const Grid g = makeGrid(nx, ny, nz, hx, hy, hz);
+    const Field<double> f = load(g, in);
+    if (op == 0) {
+      if (ax < 0 || ay < 0 || az < 0 || ax > 4 || ay > 4 || az > 4)
+        throw std::invalid_argument("ref: spectral counts must be 0..4");
+      kSpectral[static_cast<std::size_t>(25 * ax + 5 * ay + az)](f, out);
+    } else if (op == 1) {
+      store(gridcalc::spectral::laplacian(f), out);
+    } else if (op == 2) {
+      store(gridcalc::spectral::biharmonic(f), out);
+    } else {
+      const Field<Vec3d> r = gridcalc::spectral::gradient(f);
+      const std::size_t n = g.getSize();
+      for (std::size_t i = 0; i < n; ++i) {
+        out[i] = r.data()[i](0);
+        out[n + i] = r.data()[i](1);
+        out[2 * n + i] = r.data()[i](2);
+      }
+    }
   });
 }
 

@@ -12,6 +12,7 @@
 #include <gridcalc/diff/MixedPartial.hpp>
 #include <gridcalc/diff/ThirdOrder.hpp>
 #include <gridcalc/func/Functional.hpp>
+#include <gridcalc/spectral/Derivatives.hpp>
 #include <gridcalc/func/Integrate.hpp>
 #include <gridcalc/fvm/CellLaplacian.hpp>
 #include <gridcalc/solve/Diffusion.hpp>
@@ -200,6 +201,25 @@ int main() {
       threw = true;
     }
     require(ok && lines == 16 && spacing == "SPACING 0.5 0.25 1\n" && eleventh == want && threw, "vtk writer");
+  }
+  {  // spectral/Derivatives.hpp: exact on a band-limited field
+    const int N = 16;
+    const double h = 2 * kPi / N;
+    Grid g(N, N, N, Vec3d(h, h, h));
+    Field<double> f(g, [](double x, double y, double z) { return std::sin(x) * std::cos(2 * y) * std::sin(z); });
+    const auto lap = gridcalc::spectral::laplacian(f);
+    const auto fxy = gridcalc::spectral::partial<1, 1, 0>(f);
+    const auto grad = gridcalc::spectral::gradient(f);
+    double e1 = 0, e2 = 0, e3 = 0;
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const double x = i * h, y = j * h, z = k * h;
+          e1 = std::max(e1, std::abs(lap(i, j, k) + 6 * f(i, j, k)));
+          e2 = std::max(e2, std::abs(fxy(i, j, k) + 2 * std::cos(x) * std::sin(2 * y) * std::sin(z)));
+          e3 = std::max(e3, std::abs(grad(i, j, k)(2) - std::sin(x) * std::cos(2 * y) * std::cos(z)));
+        }
+    require(e1 < 1e-12 && e2 < 1e-12 && e3 < 1e-12, "spectral derivatives");
   }
   std::printf("version %s\n", gridcalc::version());
   return 0;

@@ -23,6 +23,10 @@ PARTIALS = oracle_lib.PARTIALS
 # Grids and orders the partials are stored for (all 31 each).
 PARTIAL_CASES = [("aniso3d", 4), ("flat2d", 2)]
 
+# Count triples the spectral partial is stored for.
+SPECTRAL_COUNTS = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (2, 1, 1), (0, 3, 0), (2, 2, 0), (1, 1, 1),
+                   (4, 0, 0), (0, 0, 3)]
+
 # (name, shape (nz, ny, nx), h)
 GRIDS = [
     ("aniso3d", (8, 10, 12), (0.3, 0.25, 0.5)),
@@ -68,6 +72,12 @@ def main() -> None:
             out[f"{name}/evaluate_{cname}"] = np.array(ref.evaluate_program(comps, prog.arity, prog.instr, src, h))
             out[f"{name}/evaluate_{cname}_kahan"] = np.array(
                 ref.evaluate_program(comps, prog.arity, prog.instr, src, h, kahan=True))
+        # The reference's spectral (PocketFFT) derivatives.
+        out[f"{name}/spectral_laplacian"] = ref.spectral("laplacian", f, h)
+        out[f"{name}/spectral_biharmonic"] = ref.spectral("biharmonic", f, h)
+        out[f"{name}/spectral_gradient"] = ref.spectral("gradient", f, h)
+        for c in SPECTRAL_COUNTS:
+            out[f"{name}/spectral_partial{c[0]}{c[1]}{c[2]}"] = ref.spectral("partial", f, h, c)
         for pname, porder in PARTIAL_CASES:
             if pname == name:
                 for c in PARTIALS:

@@ -194,6 +194,15 @@ class Reference(_Lib):
     def __init__(self):
         super().__init__(REF_SO, "ref_")
 
+    def spectral(self, op: str, f, h=(1.0, 1.0, 1.0), counts=(0, 0, 0)):
+        """spectral/Derivatives.hpp through PocketFFT: op 'partial' (counts
+        0..4 each), 'laplacian', 'biharmonic' or 'gradient' (3 planes)."""
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        code = {"partial": 0, "laplacian": 1, "biharmonic": 2, "gradient": 3}[op]
+        out = np.zeros(((3,) if op == "gradient" else ()) + f.shape)
+        self._rc(self.lib.ref_spectral(code, *counts, *self._g(f.shape, h), _ptr(f), _ptr(out)))
+        return out
+
     def write_vtk(self, f, path: str, name: str, h=(1.0, 1.0, 1.0)) -> None:
         """examples/common/vtk_writer.hpp: the reference's ASCII snapshot file."""
         f = np.ascontiguousarray(f, dtype=np.float64)

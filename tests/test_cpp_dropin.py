@@ -30,4 +30,4 @@ def test_dropin_runs_reference_style_checks(tmp_path):
     _compile(exe)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("PASS") == 12 and "FAIL" not in r.stdout, r.stdout
+    assert r.stdout.count("PASS") == 13 and "FAIL" not in r.stdout, r.stdout
