@@ -81,6 +81,7 @@ enum ScratchSlot {
   kSlotFlags,
   kSlotMisc,
   kSlotSpectral,
+  kSlotFaces,
 };
 
 gc_status scratch_get(gc_context* ctx, int slot, size_t bytes, void** out);
