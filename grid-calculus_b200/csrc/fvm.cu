@@ -14,6 +14,7 @@
 // RK4 then costs 13 field passes plus 4 x 3 face reads per step, and no
 // division.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "stepper.cuh"
@@ -350,9 +351,157 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_kernel(const FvmParams
   }
 }
 
+// Two-column float variant of the FVM z-march (even nx): a 32 x 8 CTA owns a
+// 64 x 8 column block, each thread two adjacent cells loaded and stored as
+// float2, so the per-plane index arithmetic, queue rotation and barriers are
+// paid once per two cells (the single-column float kernel was issue-bound).
+// Row layout in shared memory: halo column at 1, the block at 2 .. 65, halo
+// at 66, so each thread's pair sits on an 8-byte boundary.
+template <int MODE>
+__global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_x2_kernel(const FvmParams<float> p, int zc) {
+  constexpr int RW = 2 * FZ_X + 4;
+  __shared__ __align__(8) float sy[FZ_Y + 2][RW];
+  __shared__ __align__(8) float sd[FZ_Y + 2][RW];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  const int x0 = blockIdx.x * (2 * FZ_X), y0 = blockIdx.y * FZ_Y;
+  const int z0 = blockIdx.z * zc;
+  const int z1 = min(z0 + zc, nz);
+  const size_t plane = static_cast<size_t>(nx) * ny;
+  const int gx = wrap(x0 + 2 * tx, nx), gy = wrap(y0 + ty, ny);  // gx even (nx even)
+  const size_t col = static_cast<size_t>(gy) * nx + gx;
+  const bool active = x0 + 2 * tx < nx && y0 + ty < ny;
+  const bool hx = tx < 2;
+  const size_t hx_off = static_cast<size_t>(gy) * nx + wrap(tx == 0 ? x0 - 1 : x0 + 2 * FZ_X, nx);
+  const int hx_slot = tx == 0 ? 1 : 2 * FZ_X + 2;
+  const bool hy = ty < 2;
+  const size_t hy_off = static_cast<size_t>(wrap(ty == 0 ? y0 - 1 : y0 + FZ_Y, ny)) * nx + gx;
+  const int hy_slot = ty == 0 ? 0 : FZ_Y + 1;
+  const bool has_kin = p.kin != nullptr;
+  const int sc = 2 * tx + 2;  // this thread's first cell in a shared row
+
+  auto ld2 = [](const float* base, size_t gi) { return __ldg(reinterpret_cast<const float2*>(base + gi)); };
+  auto y2 = [&](float2 ps, float2 ks) {
+    return has_kin ? make_float2(ps.x + p.a * ks.x, ps.y + p.a * ks.y) : ps;
+  };
+  auto yval = [&](size_t gi) -> float {
+    float v = __ldg(p.psi + gi);
+    if (has_kin) v = v + p.a * __ldg(p.kin + gi);
+    return v;
+  };
+  auto qaddr = [&](int z) { return static_cast<size_t>(wrap(z, nz)) * plane + col; };
+
+  float2 qy[3], qd[3], qp[3], qk[3];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const size_t gi = qaddr(z0 - 1 + k);
+    qp[k + 1] = ld2(p.psi, gi);
+    qk[k + 1] = has_kin ? ld2(p.kin, gi) : make_float2(0.f, 0.f);
+    qy[k + 1] = y2(qp[k + 1], qk[k + 1]);
+    qd[k + 1] = ld2(p.D, gi);
+  }
+  float2 n_p = ld2(p.psi, qaddr(z0 + 1));
+  float2 n_k = has_kin ? ld2(p.kin, qaddr(z0 + 1)) : make_float2(0.f, 0.f);
+  float2 n_d = ld2(p.D, qaddr(z0 + 1));
+  float n_hxy = hx ? yval(static_cast<size_t>(z0) * plane + hx_off) : 0.f;
+  float n_hxd = hx ? __ldg(p.D + static_cast<size_t>(z0) * plane + hx_off) : 0.f;
+  float2 n_hyy = make_float2(0.f, 0.f), n_hyd = make_float2(0.f, 0.f);
+  if (hy) {
+    const size_t gi = static_cast<size_t>(z0) * plane + hy_off;
+    n_hyy = y2(ld2(p.psi, gi), has_kin ? ld2(p.kin, gi) : make_float2(0.f, 0.f));
+    n_hyd = ld2(p.D, gi);
+  }
+  float2 n_k1 = make_float2(0.f, 0.f), n_k2 = make_float2(0.f, 0.f);
+  if (MODE == MODE_RK4_FINAL && active) {
+    n_k1 = ld2(p.k1, static_cast<size_t>(z0) * plane + col);
+    n_k2 = ld2(p.k2, static_cast<size_t>(z0) * plane + col);
+  }
+
+  for (int z = z0; z < z1; ++z) {
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      qy[k] = qy[k + 1];
+      qd[k] = qd[k + 1];
+      qp[k] = qp[k + 1];
+      qk[k] = qk[k + 1];
+    }
+    qp[2] = n_p;
+    qk[2] = n_k;
+    qy[2] = y2(n_p, n_k);
+    qd[2] = n_d;
+    const float hxy = n_hxy, hxd = n_hxd;
+    const float2 hyy = n_hyy, hyd = n_hyd, k1c = n_k1, k2c = n_k2;
+    if (z + 1 < z1) {
+      const size_t zo = static_cast<size_t>(z + 1) * plane;
+      n_p = ld2(p.psi, qaddr(z + 2));
+      if (has_kin) n_k = ld2(p.kin, qaddr(z + 2));
+      n_d = ld2(p.D, qaddr(z + 2));
+      if (hx) {
+        n_hxy = yval(zo + hx_off);
+        n_hxd = __ldg(p.D + zo + hx_off);
+      }
+      if (hy) {
+        n_hyy = y2(ld2(p.psi, zo + hy_off), has_kin ? ld2(p.kin, zo + hy_off) : make_float2(0.f, 0.f));
+        n_hyd = ld2(p.D, zo + hy_off);
+      }
+      if (MODE == MODE_RK4_FINAL && active) {
+        n_k1 = ld2(p.k1, zo + col);
+        n_k2 = ld2(p.k2, zo + col);
+      }
+    }
+    *reinterpret_cast<float2*>(&sy[ty + 1][sc]) = qy[1];
+    *reinterpret_cast<float2*>(&sd[ty + 1][sc]) = qd[1];
+    if (hx) {
+      sy[ty + 1][hx_slot] = hxy;
+      sd[ty + 1][hx_slot] = hxd;
+    }
+    if (hy) {
+      *reinterpret_cast<float2*>(&sy[hy_slot][sc]) = hyy;
+      *reinterpret_cast<float2*>(&sd[hy_slot][sc]) = hyd;
+    }
+    __syncthreads();
+    if (active) {
+      float out[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int c = sc + q;
+        const float pc = q == 0 ? qy[1].x : qy[1].y;
+        const float dc = q == 0 ? qd[1].x : qd[1].y;
+        const float dzu = q == 0 ? qd[2].x : qd[2].y, dzd = q == 0 ? qd[0].x : qd[0].y;
+        const float yzu = q == 0 ? qy[2].x : qy[2].y, yzd = q == 0 ? qy[0].x : qy[0].y;
+        const float dxp = hmean(dc, sd[ty + 1][c + 1]), dxm = hmean(sd[ty + 1][c - 1], dc);
+        const float dyp = hmean(dc, sd[ty + 2][c]), dym = hmean(sd[ty][c], dc);
+        const float dzp = hmean(dc, dzu), dzm = hmean(dzd, dc);
+        const float rx = (dxp * (sy[ty + 1][c + 1] - pc) - dxm * (pc - sy[ty + 1][c - 1])) * p.ihx2;
+        const float ry = (dyp * (sy[ty + 2][c] - pc) - dym * (pc - sy[ty][c])) * p.ihy2;
+        const float rz = (dzp * (yzu - pc) - dzm * (pc - yzd)) * p.ihz2;
+        const float rhs = (rx + ry) + rz;
+        if constexpr (MODE == MODE_RHS) {
+          out[q] = rhs;
+        } else if constexpr (MODE == MODE_RK4_FINAL) {
+          const float s14 = (q == 0 ? k1c.x : k1c.y) + rhs;
+          const float s23 = (q == 0 ? k2c.x : k2c.y) + (q == 0 ? qk[1].x : qk[1].y);
+          out[q] = (q == 0 ? qp[1].x : qp[1].y) + (p.c6 * s14 + p.c3 * s23);
+        } else {
+          out[q] = pc + p.c6 * rhs;
+        }
+      }
+      const size_t gi = static_cast<size_t>(z) * plane + static_cast<size_t>(y0 + ty) * nx + (x0 + 2 * tx);
+      *reinterpret_cast<float2*>(p.out + gi) = make_float2(out[0], out[1]);
+    }
+    __syncthreads();
+  }
+}
+
 template <class T, int KIND, int MODE>
 gc_status launch_fvm_zmarch(gc_context* ctx, const FvmParams<T>& p) {
-  const int tiles_x = div_up(p.nx, FZ_X), tiles_y = div_up(p.ny, FZ_Y);
+  bool x2 = false;
+  if constexpr (std::is_same_v<T, float> && KIND == KIND_FVM)
+    x2 = !p.fx && p.nx % 2 == 0 &&
+         (reinterpret_cast<uintptr_t>(p.psi) | reinterpret_cast<uintptr_t>(p.kin) | reinterpret_cast<uintptr_t>(p.D) |
+          reinterpret_cast<uintptr_t>(p.out) | reinterpret_cast<uintptr_t>(p.k1) | reinterpret_cast<uintptr_t>(p.k2)) %
+                 8 == 0;
+  const int tiles_x = div_up(p.nx, x2 ? 2 * FZ_X : FZ_X), tiles_y = div_up(p.ny, FZ_Y);
   const long long tiles = static_cast<long long>(tiles_x) * tiles_y;
   const long long want = 16LL * ctx->num_sms;
   int chunks = static_cast<int>(std::min<long long>((want + tiles - 1) / tiles, std::max(1, p.nz / 16)));
@@ -360,6 +509,13 @@ gc_status launch_fvm_zmarch(gc_context* ctx, const FvmParams<T>& p) {
   const int zc = div_up(p.nz, chunks);
   chunks = div_up(p.nz, zc);
   dim3 grid(tiles_x, tiles_y, chunks), block(FZ_X, FZ_Y);
+  if constexpr (std::is_same_v<T, float> && KIND == KIND_FVM) {
+    if (x2) {
+      fvm_zmarch_x2_kernel<MODE><<<grid, block, 0, ctx->stream>>>(p, zc);
+      GC_CHECK_LAUNCH("fvm_zmarch_x2_kernel");
+      return GC_OK;
+    }
+  }
   if (KIND == KIND_FVM && p.fx)
     fvm_zmarch_kernel<T, KIND, MODE, true><<<grid, block, 0, ctx->stream>>>(p, zc);
   else
