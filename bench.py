@@ -186,6 +186,15 @@ def _cuda_time(fn, reps=5):
     return s.elapsed_time(e) / reps
 
 
+# FP64 operations per cell of the 3-D biharmonic as the kernels evaluate it
+# (unit-weight taps add without a multiply): axial fourth derivatives
+# 3 x (7, 13, 17), mixed second-derivative products 3 x (14, 50, 98) (every
+# tap added from 0, non-unit products multiplied first), and the
+# 15-operation combination (diff/Biharmonic.hpp:70-99).
+BIHARMONIC_FP64_OPS = {2: 3 * 7 + 3 * 14 + 15, 4: 3 * 13 + 3 * 50 + 15, 6: 3 * 17 + 3 * 98 + 15}
+FP64_NOMINAL_TOPS = 18.5
+
+
 def fourier_field(n, seed, device, dtype):
     """Sum of 64 modes a cos(2 pi k.x + phi) on the unit cube, |k| <= 16
     (integer k != 0 drawn uniformly), a ~ N(0, 1), phi ~ U[0, 2 pi); returns
@@ -261,14 +270,22 @@ def form_operators(gc, peak):
             es = f.element_size()
             res = {}
 
-            def rec(name, bytes_per_cell, fn, result, analytic):
+            def rec(name, bytes_per_cell, fn, result, analytic, fp64_ops=None):
                 ms = _cuda_time(fn)
                 gbs = bytes_per_cell * es * cells / ms / 1e6
                 res[name] = {"ms": ms, "GB/s": gbs, "frac": gbs / peak, "err_vs_analytic": rel(result, analytic)}
+                if fp64_ops and tag == "f64":
+                    # Exact (unfused) FP64: every add and multiply is one
+                    # instruction, against the nominal 18.5 T per second
+                    # (one FP64 lane-operation per clock on 64 lanes x 148 SMs).
+                    tops = fp64_ops * cells / ms / 1e9
+                    res[name].update({"fp64_ops_per_cell": fp64_ops, "fp64_Tops": tops,
+                                      "fp64_frac_of_nominal": tops / FP64_NOMINAL_TOPS})
 
             for order in (2, 4, 6):
                 rec(f"laplacian{order}", 2, lambda: gc.laplacian(f, g, order, o), o, lap_a)
-                rec(f"biharmonic{order}", 2, lambda: gc.biharmonic(f, g, order, o), o, bih_a)
+                rec(f"biharmonic{order}", 2, lambda: gc.biharmonic(f, g, order, o), o, bih_a,
+                    BIHARMONIC_FP64_OPS[order])
                 rec(f"gradient{order}", 4, lambda: gc.gradient(f, g, order, o3), o3, grad_a)
                 rec(f"divergence{order}", 4, lambda: gc.divergence(vec, g, order, o), o, div_a)
             # Mixed and higher partials (the named dxy, d3dxdydz, d4dx2dy2), checked
