@@ -64,7 +64,7 @@ def test_f32_ensemble_error_and_diagnostics(gc, oracle):
         assert l2 < 1e-4, (i, l2)
         f_ref = oracle.ch_free_energy(want, kap)
         v4 = nx * ny / 4.0
-        # BASELINE convention F + V/4 (f = (c^2 - 1)^2 / 4)
+        # double-well form F + V/4 (f = (c^2 - 1)^2 / 4)
         assert abs((energy[i] + v4) - (f_ref + v4)) / abs(f_ref + v4) < 1e-4, (i, energy[i], f_ref)
         m_ref = float(init[i].sum())
         assert abs(mass[i] - m_ref) < 1e-6 * nx * ny, (i, mass[i], m_ref)  # mean drift < 1e-6

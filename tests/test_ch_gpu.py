@@ -68,7 +68,7 @@ def test_trajectories_golden(gc):
 def test_plain_method_128_bit_exact(gc, oracle):
     """128 x 128, M = kappa = 1, order 2, dt = 0.01, 2000 RK4 steps, FP64:
     every 500 steps the state is bit-identical to the oracle, and so are the
-    free energy (BASELINE convention F_ref + V/4) and the mass."""
+    free energy in the double-well form F_ref + V/4 and the mass."""
     shape = (1, 128, 128)
     psi0 = uniform_ic(shape, 42)
     g = grid_of(gc, shape)
