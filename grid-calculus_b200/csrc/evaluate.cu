@@ -45,7 +45,7 @@ struct EvalGrid {
   const void* field;
   long long n;
   int nx, ny, nz;
-  int step_i, step_j, step_k;     // kEvalThreads cells as (di, dj, dk)
+  int step_i, step_j, step_k;     // 2 kEvalThreads cells (one chunk-walk iteration) as (di, dj, dk)
   int kstep_i, kstep_j, kstep_k;  // the compensated sum's stride as (di, dj, dk)
   int pad;
   double ihx, ihy, ihz;     // 1 / h
@@ -93,16 +93,10 @@ __device__ __forceinline__ int gc_off(int i, int o, int n) {
   return o + (t < 0 ? n : 0) - (t >= n ? n : 0);
 }
 
-__device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
-  const GC_T* __restrict__ p = (const GC_T*)g.field + c;
-  gc_i64 xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
-  const gc_i64 plane = (gc_i64)g.nx * g.ny;
-#pragma unroll
-  for (int m = 0; m <= 2 * GC_R; ++m) {
-    xo[m] = gc_off(i, m - GC_R, g.nx);
-    yo[m] = (gc_i64)gc_off(j, m - GC_R, g.ny) * g.nx;
-    zo[m] = (gc_i64)gc_off(k, m - GC_R, g.nz) * plane;
-  }
+// Inputs of the arity and the integrand at the cell p points to; xo / yo /
+// zo are the flat offsets of its x, y and z taps.
+__device__ __forceinline__ double gc_eval_at(const EvalGrid& g, const GC_T* __restrict__ p, const gc_i64* xo,
+                                             const gc_i64* yo, const gc_i64* zo) {
   auto v = [&](int comp, int ox, int oy, int oz) -> double {
     gc_i64 off = (gc_i64)comp * g.n;
     if (ox) off += xo[ox + GC_R];
@@ -175,6 +169,39 @@ __device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, in
   return gc_integrand(in);
 }
 
+__device__ __forceinline__ void gc_yz_offsets(const EvalGrid& g, int j, int k, gc_i64* yo, gc_i64* zo) {
+  const gc_i64 plane = (gc_i64)g.nx * g.ny;
+#pragma unroll
+  for (int m = 0; m <= 2 * GC_R; ++m) {
+    yo[m] = (gc_i64)gc_off(j, m - GC_R, g.ny) * g.nx;
+    zo[m] = (gc_i64)gc_off(k, m - GC_R, g.nz) * plane;
+  }
+}
+
+__device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
+  gc_i64 xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+#pragma unroll
+  for (int m = 0; m <= 2 * GC_R; ++m) xo[m] = gc_off(i, m - GC_R, g.nx);
+  gc_yz_offsets(g, j, k, yo, zo);
+  return gc_eval_at(g, (const GC_T*)g.field + c, xo, yo, zo);
+}
+
+// Cells (i, j, k) and (i + 1, j, k) of one row (i + 1 < nx): the y and z
+// offsets are formed once and the shared x taps are loaded once.
+__device__ __forceinline__ void gc_cell_pair(const EvalGrid& g, gc_i64 c, int i, int j, int k, double& a,
+                                             double& b) {
+  gc_i64 xa[2 * GC_R + 1], xb[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+#pragma unroll
+  for (int m = 0; m <= 2 * GC_R; ++m) {
+    xa[m] = gc_off(i, m - GC_R, g.nx);
+    xb[m] = gc_off(i + 1, m - GC_R, g.nx);
+  }
+  gc_yz_offsets(g, j, k, yo, zo);
+  const GC_T* p = (const GC_T*)g.field + c;
+  a = gc_eval_at(g, p, xa, yo, zo);
+  b = gc_eval_at(g, p + 1, xb, yo, zo);
+}
+
 // (i, j, k) += a step given as (di, dj, dk) with di < nx, dj < ny.
 __device__ __forceinline__ void gc_advance(int& i, int& j, int& k, int nx, int ny, int di, int dj, int dk) {
   i += di;
@@ -216,10 +243,29 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGri
     gc_i64 lo = 0, hi = g.n;
     gc_descend(lo, hi, c, depth);
     const int len = (int)(hi - lo);
+    // Two consecutive cells per thread and iteration.
     int i, j, k;
-    gc_locate(g, lo + threadIdx.x, i, j, k);
-    for (int e = threadIdx.x; e < len; e += 256) {
-      s[gc_padpos(e)] = gc_cell(g, lo + e, i, j, k);
+    gc_locate(g, lo + 2 * threadIdx.x, i, j, k);
+    for (int e = 2 * threadIdx.x; e < len; e += 512) {
+      if (e + 1 < len && i + 1 < g.nx) {
+        double a, b;
+        gc_cell_pair(g, lo + e, i, j, k, a, b);
+        s[gc_padpos(e)] = a;
+        s[gc_padpos(e + 1)] = b;
+      } else {
+        s[gc_padpos(e)] = gc_cell(g, lo + e, i, j, k);
+        if (e + 1 < len) {
+          int i1 = i + 1, j1 = j, k1 = k;
+          if (i1 == g.nx) {
+            i1 = 0;
+            if (++j1 == g.ny) {
+              j1 = 0;
+              ++k1;
+            }
+          }
+          s[gc_padpos(e + 1)] = gc_cell(g, lo + e + 1, i1, j1, k1);
+        }
+      }
       gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
     }
     int d2 = 0;
@@ -502,7 +548,7 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   a.field = field;
   a.n = n;
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-  split_step(kEvalThreads, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
+  split_step(2 * kEvalThreads, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
   split_step(static_cast<long long>(kKahanBlocks) * kKahanThreads, g->nx, g->ny, &a.kstep_i, &a.kstep_j, &a.kstep_k);
   a.ihx = 1.0 / g->hx; a.ihy = 1.0 / g->hy; a.ihz = 1.0 / g->hz;
   a.ihx2 = 1.0 / (g->hx * g->hx); a.ihy2 = 1.0 / (g->hy * g->hy); a.ihz2 = 1.0 / (g->hz * g->hz);
