@@ -37,6 +37,7 @@
 namespace gcb {
 namespace {
 
+constexpr int kChunkCells = 8192;   // pairwise chunk bound (pairwise.cuh kChunkMax)
 constexpr int kEvalThreads = 256;
 
 // Kernel argument; the device source declares the same layout.
@@ -44,9 +45,9 @@ struct EvalGrid {
   const void* field;
   long long n;
   int nx, ny, nz;
-  int step_i, step_j, step_k;     // 64 cells (one pass of a warp over a node) as (di, dj, dk)
+  int step_i, step_j, step_k;     // 2 kEvalThreads cells (one chunk-walk iteration) as (di, dj, dk)
   int kstep_i, kstep_j, kstep_k;  // the compensated sum's stride as (di, dj, dk)
-  float inv_nx, inv_ny;           // 1 / nx, 1 / ny (small-offset division)
+  int pad;
   double ihx, ihy, ihz;     // 1 / h
   double ihx2, ihy2, ihz2;  // 1 / h^2
   double ihx4, ihy4, ihz4;  // (1 / h^2)^2
@@ -64,7 +65,7 @@ struct EvalGrid {
   int nx, ny, nz;
   int step_i, step_j, step_k;
   int kstep_i, kstep_j, kstep_k;
-  float inv_nx, inv_ny;
+  int pad;
   double ihx, ihy, ihz, ihx2, ihy2, ihz2, ihx4, ihy4, ihz4;
 };
 
@@ -217,6 +218,8 @@ __device__ __forceinline__ void gc_locate(const EvalGrid& g, gc_i64 c, int& i, i
   k = (int)(rest / g.ny);
 }
 
+__device__ __forceinline__ int gc_padpos(int e) { return e + (e >> 6); }
+
 __device__ __forceinline__ void gc_descend(gc_i64& lo, gc_i64& hi, gc_i64 idx, int depth) {
   for (int b = depth - 1; b >= 0; --b) {
     const gc_i64 mid = lo + (hi - lo) / 2;
@@ -225,84 +228,62 @@ __device__ __forceinline__ void gc_descend(gc_i64& lo, gc_i64& hi, gc_i64 idx, i
   }
 }
 
-// floor(x / n) for 0 <= x < 2^20: the float product is within 1e-3 of the
-// quotient there, so one correction step makes it exact.
-__device__ __forceinline__ int gc_div_small(int x, int n, float inv) {
-  int q = (int)((float)x * inv);
-  const int r = x - q * n;
-  if (r < 0) --q;
-  else if (r >= n) ++q;
-  return q;
+__device__ __forceinline__ double gc_seq_sum(const double* s, int a, int b) {
+  double acc = 0.0;
+  for (int e = a; e < b; ++e) acc = __dadd_rn(acc, s[gc_padpos(e)]);
+  return acc;
 }
 
-// The pairwise chunk walk (pairwise_chunks) with the summands formed in
-// place.  A chunk's leaf nodes (contiguous ranges of <= 128 cells, summed
-// left to right; a node of 65..128 as its two halves) are spread over the
-// CTA's warps: the lanes form a node's integrands in pairs of consecutive
-// cells into the warp's own 128-value buffer, then one lane (or two, one per
-// half) sums them in order.  The node sums are combined up the chunk's
-// binary tree as the reference's recursion pairs them.
 extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
                                                                    double* __restrict__ partial) {
-  __shared__ double wbuf[8][128];
-  __shared__ double ns[64];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* wb = wbuf[warp];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = (double*)smem_raw;
+  double* ns = s + gc_padpos(8192) + 8;
   for (gc_i64 c = blockIdx.x; c < nchunks; c += gridDim.x) {
     gc_i64 lo = 0, hi = g.n;
     gc_descend(lo, hi, c, depth);
     const int len = (int)(hi - lo);
+    // Two consecutive cells per thread and iteration.
+    int i, j, k;
+    gc_locate(g, lo + 2 * threadIdx.x, i, j, k);
+    for (int e = 2 * threadIdx.x; e < len; e += 512) {
+      if (e + 1 < len && i + 1 < g.nx) {
+        double a, b;
+        gc_cell_pair(g, lo + e, i, j, k, a, b);
+        s[gc_padpos(e)] = a;
+        s[gc_padpos(e + 1)] = b;
+      } else {
+        s[gc_padpos(e)] = gc_cell(g, lo + e, i, j, k);
+        if (e + 1 < len) {
+          int i1 = i + 1, j1 = j, k1 = k;
+          if (i1 == g.nx) {
+            i1 = 0;
+            if (++j1 == g.ny) {
+              j1 = 0;
+              ++k1;
+            }
+          }
+          s[gc_padpos(e + 1)] = gc_cell(g, lo + e + 1, i1, j1, k1);
+        }
+      }
+      gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
+    }
     int d2 = 0;
     while (((len + (1 << d2) - 1) >> d2) > 128) ++d2;
     const int nodes = 1 << d2;
-    int ci, cj, ck;
-    gc_locate(g, lo, ci, cj, ck);
-    for (int node = warp; node < nodes; node += 8) {
-      gc_i64 na = 0, nb = len;
-      gc_descend(na, nb, node, d2);
-      const int m = (int)(nb - na);
-      // This lane's first cell: chunk start + na + 2 lane.
-      int i = ci, j = cj, k = ck;
-      {
-        const int d = (int)na + 2 * lane;
-        const int rows = gc_div_small(d, g.nx, g.inv_nx);
-        const int planes = gc_div_small(rows, g.ny, g.inv_ny);
-        gc_advance(i, j, k, g.nx, g.ny, d - rows * g.nx, rows - planes * g.ny, planes);
+    __syncthreads();
+    if (threadIdx.x < nodes) {
+      gc_i64 a = 0, b = len;
+      gc_descend(a, b, threadIdx.x, d2);
+      const int m = (int)(b - a);
+      double v;
+      if (m <= 64) {
+        v = gc_seq_sum(s, (int)a, (int)b);
+      } else {
+        const int h = m / 2;
+        v = __dadd_rn(gc_seq_sum(s, (int)a, (int)a + h), gc_seq_sum(s, (int)a + h, (int)b));
       }
-      for (int e = 2 * lane; e < m; e += 64) {
-        const gc_i64 cell = lo + na + e;
-        if (e + 1 < m && i + 1 < g.nx) {
-          double a, b;
-          gc_cell_pair(g, cell, i, j, k, a, b);
-          wb[e] = a;
-          wb[e + 1] = b;
-        } else {
-          wb[e] = gc_cell(g, cell, i, j, k);
-          if (e + 1 < m) {
-            int i1 = i + 1, j1 = j, k1 = k;
-            if (i1 == g.nx) {
-              i1 = 0;
-              if (++j1 == g.ny) {
-                j1 = 0;
-                ++k1;
-              }
-            }
-            wb[e + 1] = gc_cell(g, cell + 1, i1, j1, k1);
-          }
-        }
-        gc_advance(i, j, k, g.nx, g.ny, g.step_i, g.step_j, g.step_k);
-      }
-      __syncwarp();
-      const int h = m <= 64 ? m : m / 2;
-      double part = 0.0;
-      if (lane == 0) {
-        for (int e = 0; e < h; ++e) part = __dadd_rn(part, wb[e]);
-      } else if (lane == 1 && m > 64) {
-        for (int e = h; e < m; ++e) part = __dadd_rn(part, wb[e]);
-      }
-      const double other = __shfl_down_sync(0xffffffffu, part, 1);
-      if (lane == 0) ns[node] = m <= 64 ? part : __dadd_rn(part, other);
-      __syncwarp();
+      ns[threadIdx.x] = v;
     }
     __syncthreads();
     for (int w = nodes >> 1; w >= 1; w >>= 1) {
@@ -455,6 +436,7 @@ std::string program_source(const gc_program* f, gc_dtype dt) {
 struct Driver {
   PFN_cuModuleLoadData load = nullptr;
   PFN_cuModuleGetFunction get = nullptr;
+  PFN_cuFuncSetAttribute attr = nullptr;
   PFN_cuLaunchKernel launch = nullptr;
 };
 
@@ -477,6 +459,7 @@ gc_status driver(Driver* d) {
     };
     if (!get("cuModuleLoadData", reinterpret_cast<void**>(&drv.load)) ||
         !get("cuModuleGetFunction", reinterpret_cast<void**>(&drv.get)) ||
+        !get("cuFuncSetAttribute", reinterpret_cast<void**>(&drv.attr)) ||
         !get("cuLaunchKernel", reinterpret_cast<void**>(&drv.launch)))
       return fail(GC_ERR_CUDA, "gc_evaluate_program: CUDA driver entry points unavailable");
     ok = true;
@@ -519,6 +502,9 @@ gc_status compile(gc_context* ctx, const std::string& src, Compiled* out) {
   if (drv.load(&mod, cubin.data()) != CUDA_SUCCESS || drv.get(&c.pairwise, mod, "gc_eval_pairwise") != CUDA_SUCCESS ||
       drv.get(&c.kahan, mod, "gc_eval_kahan") != CUDA_SUCCESS)
     return fail(GC_ERR_CUDA, "gc_evaluate_program: loading the compiled integrand failed");
+  const int smem = static_cast<int>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+  if (drv.attr(c.pairwise, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS)
+    return fail(GC_ERR_CUDA, "gc_evaluate_program: shared-memory attribute refused");
   g_jit.emplace(key, c);
   *out = c;
   return GC_OK;
@@ -562,9 +548,7 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   a.field = field;
   a.n = n;
   a.nx = g->nx; a.ny = g->ny; a.nz = g->nz;
-  split_step(64, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
-  a.inv_nx = 1.0f / static_cast<float>(g->nx);
-  a.inv_ny = 1.0f / static_cast<float>(g->ny);
+  split_step(2 * kEvalThreads, g->nx, g->ny, &a.step_i, &a.step_j, &a.step_k);
   split_step(static_cast<long long>(kKahanBlocks) * kKahanThreads, g->nx, g->ny, &a.kstep_i, &a.kstep_j, &a.kstep_k);
   a.ihx = 1.0 / g->hx; a.ihy = 1.0 / g->hy; a.ihz = 1.0 / g->hz;
   a.ihx2 = 1.0 / (g->hx * g->hx); a.ihy2 = 1.0 / (g->hy * g->hy); a.ihz2 = 1.0 / (g->hz * g->hz);
@@ -586,9 +570,9 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
     int depth = plan.depth;
     long long nchunks = plan.nchunks;
     void* args[] = {&a, &depth, &nchunks, &partial};
-    // 8.7 KB of shared memory per CTA: several CTAs per SM.
-    const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 8));
-    if (drv.launch(k.pairwise, grid, 1, 1, kEvalThreads, 1, 1, 0, ctx->stream, args, nullptr) != CUDA_SUCCESS)
+    const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3));
+    const unsigned smem = static_cast<unsigned>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+    if (drv.launch(k.pairwise, grid, 1, 1, kEvalThreads, 1, 1, smem, ctx->stream, args, nullptr) != CUDA_SUCCESS)
       return fail(GC_ERR_CUDA, "gc_evaluate_program: launch failed");
     if ((s = pairwise_finish(ctx, partial, nchunks, &total)) != GC_OK) return s;
   }
