@@ -755,6 +755,7 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt, const
 GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
                                  const gc_ch_params* cp, void* psi, double dt_step, int n_steps,
                                  gc_integrator integ) {
+  NvtxScope nvtx("gc_ch_integrate");
   Call call(ctx);
   if (call.st != GC_OK) return call.st;
   gc_status s = check_ch(ctx, g, dt, cp);

@@ -511,6 +511,7 @@ GC_API gc_status gc_ch_batch_state(gc_ch_batch* b, void** dev) {
 }
 
 GC_API gc_status gc_ch_batch_run(gc_ch_batch* b, int32_t n_steps) {
+  NvtxScope nvtx("gc_ch_batch_run");
   if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_run: null batch");
   Call call(b->ctx);
   if (call.st != GC_OK) return call.st;

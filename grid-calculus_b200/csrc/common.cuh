@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <cstring>
@@ -127,6 +128,16 @@ gc_status kahan_finish(gc_context* ctx, double* part, double* result);
 // reference's pairwise tree (GC_SUM_PAIRWISE) or the deterministic
 // compensated sum (GC_SUM_KAHAN); synchronises and returns it on the host.
 gc_status sum_any(gc_context* ctx, gc_dtype dt, const void* x, long long n, gc_sum sum, double* result);
+
+// A named NVTX range for the duration of a scope: the long-running entry
+// points show up by name on an Nsight Systems / NVTX timeline (no cost when
+// no tool is attached).
+struct NvtxScope {
+  explicit NvtxScope(const char* name) { nvtxRangePushA(name); }
+  ~NvtxScope() { nvtxRangePop(); }
+  NvtxScope(const NvtxScope&) = delete;
+  NvtxScope& operator=(const NvtxScope&) = delete;
+};
 
 // Scope of one API call: validates the context, orders the context stream
 // after the caller's stream on entry and the caller's stream after the

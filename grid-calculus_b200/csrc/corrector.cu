@@ -1089,6 +1089,7 @@ GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, gc_dtype 
 // One Adam step on the training loss (inputs and targets on the device).
 GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
                                          const void* target, float lr, double* loss) {
+  NvtxScope nvtx("gc_corrector_train_step");
   if (!c || !cin || !target) return fail(GC_ERR_INVALID_ARG, "gc_corrector_train_step: null pointer");
   Call call(c->ctx);
   if (call.st != GC_OK) return call.st;
@@ -1118,6 +1119,7 @@ GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtyp
 GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const gc_ch_params* cp, double* psi,
                                       int32_t n_coarse, const gc_corrector_policy* pol,
                                       gc_corrector_stats* stats) {
+  NvtxScope nvtx("gc_corrector_advance");
   if (!c || !g || !cp || !psi || !pol) return fail(GC_ERR_INVALID_ARG, "gc_corrector_advance: null pointer");
   Call call(c->ctx);
   if (call.st != GC_OK) return call.st;

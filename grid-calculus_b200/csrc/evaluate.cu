@@ -527,6 +527,7 @@ extern "C" {
 
 GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field,
                                      const gc_program* f, gc_sum sum, double* result) {
+  NvtxScope nvtx("gc_evaluate_program");
   Call call(ctx);
   gc_status s = call.st;
   if (s != GC_OK) return s;

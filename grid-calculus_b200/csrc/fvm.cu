@@ -685,6 +685,7 @@ GC_API gc_status gc_cell_laplacian(gc_context* ctx, const gc_grid* g, gc_dtype d
 
 GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi, double D,
                             double dt_step, int n_steps, gc_integrator integ) {
+  NvtxScope nvtx("gc_diffuse");
   Call call(ctx);
   gc_status s = call.st;
   if (s != GC_OK) return s;
@@ -705,6 +706,7 @@ GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void
 
 GC_API gc_status gc_diffuse_fvm(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi, const void* D,
                                 double dt_step, int n_steps, gc_integrator integ, int64_t* bad_index) {
+  NvtxScope nvtx("gc_diffuse_fvm");
   Call call(ctx);
   gc_status s = call.st;
   if (s != GC_OK) return s;

@@ -164,6 +164,18 @@ __global__ void first_nonpositive_kernel(const T* __restrict__ D, long long n,
   }
 }
 
+// First flat index holding a NaN or an infinity.
+template <class T>
+__global__ void first_nonfinite_kernel(const T* __restrict__ x, long long n, unsigned long long* __restrict__ first) {
+  for (long long c = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
+       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+    if (!isfinite(static_cast<double>(x[c]))) {
+      atomicMin(first, static_cast<unsigned long long>(c));
+      return;
+    }
+  }
+}
+
 }  // namespace
 
 PairwisePlan pairwise_plan(long long n) {
@@ -339,6 +351,48 @@ GC_API gc_status gc_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, co
   if (s != GC_OK) return s;
   *result = (g->hx * g->hy * g->hz) * total;
   return GC_OK;
+}
+
+GC_API gc_status gc_check_finite(gc_context* ctx, const gc_grid* g, gc_dtype dt, int32_t components,
+                                 const void* field, int64_t* first_bad) {
+  Call call(ctx);
+  gc_status s = call.st;
+  if (s != GC_OK) return s;
+  if ((s = check_grid(g)) != GC_OK) return s;
+  if (!field) return fail(GC_ERR_INVALID_ARG, "gc_check_finite: null field pointer");
+  if (dt != GC_F64 && dt != GC_F32) return fail(GC_ERR_INVALID_ARG, "gc_check_finite: unknown dtype");
+  if (components < 1) return fail(GC_ERR_INVALID_ARG, "gc_check_finite: components must be >= 1");
+  void* buf = nullptr;
+  if ((s = scratch_get(ctx, kSlotFlags, 64, &buf)) != GC_OK) return s;
+  unsigned long long* word = static_cast<unsigned long long*>(buf) + 2;
+  GC_CUDA(cudaMemsetAsync(word, 0xff, sizeof(unsigned long long), ctx->stream));
+  const long long n = static_cast<long long>(cells(g)) * components;
+  const int blocks = ctx->num_sms * 8;
+  if (dt == GC_F64)
+    first_nonfinite_kernel<double><<<blocks, 256, 0, ctx->stream>>>(static_cast<const double*>(field), n, word);
+  else
+    first_nonfinite_kernel<float><<<blocks, 256, 0, ctx->stream>>>(static_cast<const float*>(field), n, word);
+  GC_CHECK_LAUNCH("first_nonfinite_kernel");
+  unsigned long long* host = static_cast<unsigned long long*>(ctx->host_pinned) + 2;
+  GC_CUDA(cudaMemcpyAsync(host, word, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  GC_CUDA(cudaStreamSynchronize(ctx->stream));
+  const long long first = host[0] == ~0ULL ? -1 : static_cast<long long>(host[0]);
+  if (first_bad) *first_bad = first;
+  if (first < 0) return GC_OK;
+  double v = 0.0;
+  if (dt == GC_F64) {
+    GC_CUDA(cudaMemcpy(&v, static_cast<const double*>(field) + first, sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    float f = 0.f;
+    GC_CUDA(cudaMemcpy(&f, static_cast<const float*>(field) + first, sizeof(float), cudaMemcpyDeviceToHost));
+    v = f;
+  }
+  const long long nc = static_cast<long long>(cells(g));
+  const long long cell = first % nc;
+  const long long i = cell % g->nx, j = (cell / g->nx) % g->ny, k = cell / (static_cast<long long>(g->nx) * g->ny);
+  return fail(GC_ERR_NONFINITE, "gc_check_finite: non-finite value " + std::to_string(v) + " at flat index " +
+                                    std::to_string(first) + " (component " + std::to_string(first / nc) + ", cell (" +
+                                    std::to_string(i) + ", " + std::to_string(j) + ", " + std::to_string(k) + "))");
 }
 
 GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,

@@ -30,7 +30,7 @@ __all__ = [
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
     "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct",
     "write_vtk", "save_checkpoint", "checkpoint_info", "load_checkpoint", "Snapshotter",
-    "spectral_partial", "spectral_laplacian", "spectral_biharmonic", "spectral_gradient",
+    "spectral_partial", "spectral_laplacian", "spectral_biharmonic", "spectral_gradient", "check_finite",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -654,6 +654,8 @@ class Corrector:
         self.handle = h
         self.n_params = lib.gc_corrector_num_params()
         self.s_out = 0.05
+        self._base = None       # (mobility, kappa, order, dt_coarse, stages) of set_base
+        self._normalized = None  # set_loss
 
     def set_params(self, params, s_out: float = 0.05) -> None:
         import numpy as np
@@ -674,11 +676,36 @@ class Corrector:
         None turns the base step off (coarse step c + delta)."""
         _check(lib.gc_corrector_set_base(self.handle, C.byref(rhs.c()) if rhs is not None else None,
                                          dt_coarse, stages))
+        self._base = None if rhs is None else (rhs.mobility, rhs.kappa, rhs.order, dt_coarse, stages)
 
     def set_loss(self, normalized: bool) -> None:
         """normalized: weight each training sample by 1 / mean((target - s)^2),
         s = B(c) with a base step else c."""
         _check(lib.gc_corrector_set_loss(self.handle, 1 if normalized else 0))
+        self._normalized = bool(normalized)
+
+    def save(self, path: str, meta: dict | None = None) -> None:
+        """Writes the FP32 master parameters (the BF16 tensor-core copies are
+        derived from them) as a checkpoint file, with s_out, the base step and
+        the loss setting in its metadata."""
+        info = dict(meta or {})
+        info.update({"kind": "corrector", "n_params": self.n_params, "s_out": self.s_out,
+                     "base": list(self._base) if self._base else None, "normalized_loss": self._normalized})
+        save_checkpoint(self.get_params(), Grid(self.n_params, 1, 1), path, info)
+
+    def load(self, path: str) -> dict:
+        """Restores parameters (and the base step / loss setting when the file
+        records them) written by save(); returns the file's metadata."""
+        params, _, meta = load_checkpoint(path)
+        if meta.get("kind") != "corrector" or meta.get("n_params") != self.n_params:
+            raise ValueError(f"gridcalc_b200: {path} does not hold parameters of this corrector")
+        self.set_params(params.reshape(-1), s_out=meta["s_out"])
+        if meta.get("base"):
+            m, k, o, dt_c, st = meta["base"]
+            self.set_base(CahnHilliardRhs(m, k, int(o)), dt_c, int(st))
+        if meta.get("normalized_loss") is not None:
+            self.set_loss(meta["normalized_loss"])
+        return meta
 
     def forward(self, c):
         """Coarse-step increment (B(c) - c + delta with a base step, else the
@@ -901,3 +928,19 @@ def spectral_gradient(field, grid: Grid, out=None, ctx=None):
     _check(lib.gc_spectral_gradient(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), field.data_ptr(),
                                     out.data_ptr()))
     return out
+
+
+# --- non-finite detection ----------------------------------------------------
+lib.gc_check_finite.argtypes = [C.c_void_p, C.POINTER(gc_grid), C.c_int, C.c_int32, C.c_void_p,
+                                C.POINTER(C.c_int64)]
+lib.gc_check_finite.restype = C.c_int
+
+
+def check_finite(field, grid: Grid, ctx=None) -> None:
+    """Raises GcError (status GC_ERR_NONFINITE, the message naming the value
+    and its cell) when the device field holds a NaN or an infinity."""
+    if not field.is_cuda or not field.is_contiguous():
+        raise ValueError("gridcalc_b200: fields must be contiguous CUDA tensors")
+    first = C.c_int64(-1)
+    _check(lib.gc_check_finite(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), _components(field.numel(), grid),
+                               field.data_ptr(), C.byref(first)))

@@ -249,6 +249,15 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
  * program).  Each distinct source is compiled once per process and device. */
 GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap);
 
+/* Non-finite detection (no counterpart in the reference, which has no such
+ * check): scans `components` planes of a device field for a NaN or an
+ * infinity.  All finite: GC_OK and *first_bad = -1.  Otherwise
+ * GC_ERR_NONFINITE, *first_bad = the first flat index, and the message names
+ * the value, its component and its cell.  Run it after a batch of steps or
+ * before a snapshot to catch a blown-up trajectory. */
+GC_API gc_status gc_check_finite(gc_context* ctx, const gc_grid* g, gc_dtype dt, int32_t components,
+                                 const void* field, int64_t* first_bad);
+
 /* ---- time integration (solve::) ----------------------------------------- */
 
 /* Cahn-Hilliard right-hand side M lap(-psi + psi^3 - kappa lap psi)

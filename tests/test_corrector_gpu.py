@@ -174,3 +174,28 @@ def test_rejected_steps_fall_back_to_plain_rk4_exactly(gc, oracle):
     want = oracle.ch_integrate(2, 1.0, 1.0, psi0, 0.01, 80)
     assert np.array_equal(t.cpu().numpy(), want[0])
     net.close()
+
+
+def test_parameters_save_and_load(gc, tmp_path):
+    """Corrector.save / load: FP32 master parameters, s_out, the base step and
+    the loss setting survive a round trip through the checkpoint format; the
+    restored network gives the same increment."""
+    import torch
+    net = gc.Corrector(32, 32, max_batch=1)
+    net.set_params(gc.corrector_init_params(seed=4, last_scale=0.5, inputs=3), s_out=0.7)
+    net.set_base(gc.CahnHilliardRhs(1.0, 0.8, 2), 0.16, 6)
+    net.set_loss(True)
+    path = str(tmp_path / "net.gcb")
+    net.save(path, {"trained_on": "unit test"})
+    c = (0.1 * torch.rand((1, 32, 32), device="cuda", dtype=torch.float64)).contiguous()
+    want = net.forward(c)
+    other = gc.Corrector(32, 32, max_batch=1)
+    meta = other.load(path)
+    assert meta["trained_on"] == "unit test" and meta["s_out"] == 0.7
+    assert np.array_equal(other.get_params(), net.get_params())
+    assert torch.equal(other.forward(c), want)
+    with pytest.raises(ValueError, match="does not hold"):
+        gc.save_checkpoint(np.zeros(10, dtype=np.float32), gc.Grid(10, 1, 1), str(tmp_path / "x.gcb"))
+        other.load(str(tmp_path / "x.gcb"))
+    net.close()
+    other.close()
