@@ -127,6 +127,7 @@ GC_API const char* gc_status_string(gc_status s) {
     case GC_ERR_TIMEOUT: return "GC_ERR_TIMEOUT";
     case GC_ERR_NONFINITE: return "GC_ERR_NONFINITE";
     case GC_ERR_UNSUPPORTED: return "GC_ERR_UNSUPPORTED";
+    case GC_ERR_IO: return "GC_ERR_IO";
   }
   return "GC_ERR_UNKNOWN";
 }

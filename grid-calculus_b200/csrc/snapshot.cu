@@ -81,7 +81,7 @@ inline double value_at(const void* host, gc_dtype dt, size_t i) {
 gc_status write_vtk_file(const gc_grid* g, gc_dtype dt, const void* host, const std::string& path,
                          const std::string& name, gc_vtk_encoding enc) {
   std::FILE* out = std::fopen(path.c_str(), "wb");
-  if (!out) return fail(GC_ERR_INVALID_ARG, "writeVtkStructuredPoints: cannot open '" + path + "' for writing");
+  if (!out) return fail(GC_ERR_IO, "writeVtkStructuredPoints: cannot open '" + path + "' for writing");
   const size_t n = cells(g);
   std::string head = "# vtk DataFile Version 3.0\n";
   head += "gridcalc field: " + name + "\n";
@@ -140,7 +140,7 @@ gc_status write_vtk_file(const gc_grid* g, gc_dtype dt, const void* host, const 
     }
   }
   ok = (std::fclose(out) == 0) && ok;
-  if (!ok) return fail(GC_ERR_INVALID_ARG, "writeVtkStructuredPoints: write to '" + path + "' failed");
+  if (!ok) return fail(GC_ERR_IO, "writeVtkStructuredPoints: write to '" + path + "' failed");
   return GC_OK;
 }
 
@@ -159,48 +159,48 @@ gc_status write_ckpt_file(const gc_grid* g, gc_dtype dt, int comps, const void* 
   // truncated file under the final name.
   const std::string tmp = path + ".part";
   std::FILE* out = std::fopen(tmp.c_str(), "wb");
-  if (!out) return fail(GC_ERR_INVALID_ARG, "checkpoint: cannot open '" + tmp + "' for writing");
+  if (!out) return fail(GC_ERR_IO, "checkpoint: cannot open '" + tmp + "' for writing");
   bool ok = std::fwrite(&h, sizeof h, 1, out) == 1;
   ok = ok && (meta.empty() || std::fwrite(meta.data(), 1, meta.size(), out) == meta.size());
   ok = ok && (h.data_bytes == 0 || std::fwrite(host, 1, h.data_bytes, out) == h.data_bytes);
   ok = (std::fclose(out) == 0) && ok;
   if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) {
     std::remove(tmp.c_str());
-    return fail(GC_ERR_INVALID_ARG, "checkpoint: write to '" + path + "' failed");
+    return fail(GC_ERR_IO, "checkpoint: write to '" + path + "' failed");
   }
   return GC_OK;
 }
 
 gc_status read_ckpt_header(std::FILE* in, const std::string& path, CkptHeader* h) {
   if (std::fread(h, sizeof *h, 1, in) != 1 || std::memcmp(h->magic, kCkptMagic, 8) != 0)
-    return fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' is not a gridcalc_b200 checkpoint");
+    return fail(GC_ERR_IO, "checkpoint: '" + path + "' is not a gridcalc_b200 checkpoint");
   if (h->version != kCkptVersion)
     return fail(GC_ERR_UNSUPPORTED, "checkpoint: '" + path + "' has version " + std::to_string(h->version));
   if ((h->dtype != GC_F64 && h->dtype != GC_F32) || h->nx <= 0 || h->ny <= 0 || h->nz <= 0 || h->components <= 0 ||
       h->data_bytes != static_cast<uint64_t>(h->nx) * h->ny * h->nz * h->components * (h->dtype == GC_F64 ? 8 : 4))
-    return fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' has an inconsistent header");
+    return fail(GC_ERR_IO, "checkpoint: '" + path + "' has an inconsistent header");
   return GC_OK;
 }
 
 gc_status read_ckpt(const std::string& path, CkptHeader* h, std::string* meta, void* host, size_t host_bytes) {
   std::FILE* in = std::fopen(path.c_str(), "rb");
-  if (!in) return fail(GC_ERR_INVALID_ARG, "checkpoint: cannot open '" + path + "'");
+  if (!in) return fail(GC_ERR_IO, "checkpoint: cannot open '" + path + "'");
   gc_status s = read_ckpt_header(in, path, h);
   if (s == GC_OK && meta) {
     meta->assign(static_cast<size_t>(h->meta_len), '\0');
     if (h->meta_len && std::fread(&(*meta)[0], 1, static_cast<size_t>(h->meta_len), in) != h->meta_len)
-      s = fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' is truncated");
+      s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
   }
   if (s == GC_OK && host) {
     if (host_bytes < h->data_bytes) {
       s = fail(GC_ERR_INVALID_ARG, "checkpoint: buffer of " + std::to_string(host_bytes) + " bytes, field has " +
                                        std::to_string(h->data_bytes));
     } else if (!meta && std::fseek(in, static_cast<long>(sizeof *h + h->meta_len), SEEK_SET) != 0) {
-      s = fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' is truncated");
+      s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
     } else if (h->data_bytes && std::fread(host, 1, h->data_bytes, in) != h->data_bytes) {
-      s = fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' is truncated");
+      s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
     } else if (checksum64(host, h->data_bytes) != h->checksum) {
-      s = fail(GC_ERR_INVALID_ARG, "checkpoint: '" + path + "' fails its checksum");
+      s = fail(GC_ERR_IO, "checkpoint: '" + path + "' fails its checksum");
     }
   }
   std::fclose(in);
@@ -292,7 +292,7 @@ gc_status enqueue(gc_snapshotter* s, const gc_grid* g, gc_dtype dt, int comps, c
     index = s->next;
     slot = &s->slots[index];
     s->cv.wait(lock, [&] { return !slot->busy; });
-    if (!s->error.empty()) return fail(GC_ERR_INVALID_ARG, s->error);
+    if (!s->error.empty()) return fail(GC_ERR_IO, s->error);
   }
   s->next = (s->next + 1) % static_cast<int>(s->slots.size());
   if (slot->cap < bytes) {
@@ -349,7 +349,7 @@ GC_API gc_status gc_checkpoint_info(const char* path, gc_grid* g, gc_dtype* dt, 
                                     size_t* meta_len) {
   if (!path) return fail(GC_ERR_INVALID_ARG, "checkpoint: null path");
   std::FILE* in = std::fopen(path, "rb");
-  if (!in) return fail(GC_ERR_INVALID_ARG, std::string("checkpoint: cannot open '") + path + "'");
+  if (!in) return fail(GC_ERR_IO, std::string("checkpoint: cannot open '") + path + "'");
   CkptHeader h;
   const gc_status s = read_ckpt_header(in, path, &h);
   std::fclose(in);
@@ -443,7 +443,7 @@ GC_API gc_status gc_snapshotter_flush(gc_snapshotter* s) {
   if (!s->error.empty()) {
     const std::string e = s->error;
     s->error.clear();
-    return fail(GC_ERR_INVALID_ARG, e);
+    return fail(GC_ERR_IO, e);
   }
   return GC_OK;
 }

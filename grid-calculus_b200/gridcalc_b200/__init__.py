@@ -48,7 +48,7 @@ GC_OK = 0
 STATUS = {
     0: "GC_OK", 1: "GC_ERR_INVALID_ARG", 2: "GC_ERR_AXIS_EXTENT", 3: "GC_ERR_GRID_MISMATCH",
     4: "GC_ERR_NONPOSITIVE_D", 5: "GC_ERR_CFL", 6: "GC_ERR_CUDA", 7: "GC_ERR_TIMEOUT",
-    8: "GC_ERR_NONFINITE", 9: "GC_ERR_UNSUPPORTED",
+    8: "GC_ERR_NONFINITE", 9: "GC_ERR_UNSUPPORTED", 10: "GC_ERR_IO",
 }
 
 

@@ -56,7 +56,8 @@ typedef enum gc_status {
   GC_ERR_CUDA = 6,          /* a CUDA runtime call failed */
   GC_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
   GC_ERR_NONFINITE = 8,     /* a non-finite value was detected in the state */
-  GC_ERR_UNSUPPORTED = 9    /* (order, dtype, shape) combination not built */
+  GC_ERR_UNSUPPORTED = 9,   /* (order, dtype, shape) combination not built */
+  GC_ERR_IO = 10            /* a file could not be opened, read or written, or failed its checks */
 } gc_status;
 
 typedef enum gc_dtype { GC_F64 = 0, GC_F32 = 1 } gc_dtype;
@@ -445,7 +446,8 @@ GC_API gc_status gc_checkpoint_info(const char* path, gc_grid* g, gc_dtype* dt, 
                                     size_t* meta_len);
 /* Reads the field into host memory (host_bytes >= its size) and the
  * metadata into meta (NUL-terminated, at most meta_cap - 1 characters; may
- * be NULL); a checksum mismatch is GC_ERR_INVALID_ARG. */
+ * be NULL).  A missing, truncated or corrupt file (bad magic, inconsistent
+ * header, checksum mismatch) is GC_ERR_IO. */
 GC_API gc_status gc_read_checkpoint(const char* path, void* host, size_t host_bytes, char* meta, size_t meta_cap);
 /* The same into a device buffer, ordered on the context's stream (returns
  * after the copy). */

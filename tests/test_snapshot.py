@@ -64,8 +64,9 @@ def test_vtk_binary_and_float_fields(gcm, tmp_path):
 
 def test_vtk_open_failure_message(gcm, tmp_path):
     g = gcm.Grid(2, 2, 1)
-    with pytest.raises(ValueError, match="cannot open"):
+    with pytest.raises(ValueError, match="cannot open") as ei:
         gcm.write_vtk(np.zeros((1, 2, 2)), g, str(tmp_path / "no" / "such" / "dir.vtk"))
+    assert ei.value.status == "GC_ERR_IO"
 
 
 @pytest.mark.parametrize("dtype,comps", [(np.float64, 1), (np.float32, 1), (np.float64, 3)])
@@ -99,8 +100,9 @@ def test_checkpoint_integrity_checks(gcm, tmp_path):
     raw2 = bytearray(raw)
     raw2[-9] ^= 0x01                       # one bit of the data
     bad.write_bytes(bytes(raw2))
-    with pytest.raises(ValueError, match="checksum"):
+    with pytest.raises(ValueError, match="checksum") as ei:
         gcm.load_checkpoint(str(bad))
+    assert ei.value.status == "GC_ERR_IO"
     (tmp_path / "short.gcb").write_bytes(bytes(raw[:-8]))
     with pytest.raises(ValueError, match="truncated"):
         gcm.load_checkpoint(str(tmp_path / "short.gcb"))
