@@ -42,7 +42,10 @@ __device__ __forceinline__ void cp_async_bytes(void* smem, const void* gmem, int
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
 }
 
-template <class T>
+// WX: the x extent of the tap table (2 rx + 1), a compile-time constant so
+// that the innermost loop unrolls (shared-memory offsets and coefficient
+// indices become immediates); the y and z extents stay runtime values.
+template <class T, int WX>
 __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ PartialParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);  // [NB][PH][PW]
@@ -72,7 +75,8 @@ __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ Par
   for (int z = z0 - rz; z < z0 + rz + kPRing; ++z) issue(z);
   const int gx = x0 + tx, gy = y0 + ty;
   const bool active = gx < nx && gy < ny;
-  const int wx = 2 * rx + 1, wy = 2 * ry + 1, wz = 2 * rz + 1;
+  constexpr int wx = WX;
+  const int wy = 2 * ry + 1, wz = 2 * rz + 1;
   for (int z = z0; z < z1; ++z) {
     asm volatile("cp.async.wait_group %0;" ::"n"(kPRing - 1) : "memory");  // plane z + rz landed
     __syncthreads();
@@ -83,6 +87,7 @@ __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ Par
         for (int my = 0; my < wy; ++my) {
           const T* row = pl + (ty + R + my - ry) * PW + tx + R - rx;
           const double* cr = p.coef + (mz * wy + my) * wx;
+#pragma unroll
           for (int mx = 0; mx < wx; ++mx) {
             const double c = cr[mx];
             if (c != 0.0) sum = Ar<T>::add(sum, Ar<T>::mul(static_cast<T>(c), row[mx]));
@@ -135,11 +140,18 @@ gc_status launch_partial(gc_context* ctx, PartialParams& p) {
   p.zc = div_up(p.nz, chunks);
   chunks = div_up(p.nz, p.zc);
   const size_t smem = sizeof(T) * static_cast<size_t>(2 * p.rz + 1 + kPRing) * (PX + 2 * p.R) * (PY + 2 * p.R);
-  auto kern = partial_kernel<T>;
-  static bool attr = false;
-  if (!attr) {
+  void (*kern)(const PartialParams);
+  switch (2 * p.rx + 1) {
+    case 1: kern = partial_kernel<T, 1>; break;
+    case 3: kern = partial_kernel<T, 3>; break;
+    case 5: kern = partial_kernel<T, 5>; break;
+    case 7: kern = partial_kernel<T, 7>; break;
+    default: kern = partial_kernel<T, 9>; break;  // rx <= 4 (checked by axis_table)
+  }
+  static bool attr[5] = {false, false, false, false, false};
+  if (!attr[p.rx]) {
     GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
-    attr = true;
+    attr[p.rx] = true;
   }
   kern<<<dim3(tiles_x, tiles_y, chunks), dim3(PX, PY), smem, ctx->stream>>>(p);
   GC_CHECK_LAUNCH("partial_kernel");
