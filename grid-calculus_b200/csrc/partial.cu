@@ -42,10 +42,11 @@ __device__ __forceinline__ void cp_async_bytes(void* smem, const void* gmem, int
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
 }
 
-// WX: the x extent of the tap table (2 rx + 1), a compile-time constant so
-// that the innermost loop unrolls (shared-memory offsets and coefficient
-// indices become immediates); the y and z extents stay runtime values.
-template <class T, int WX>
+// WX, WY: the x and y extents of the tap table (2 rx + 1, 2 ry + 1),
+// compile-time constants so that the two inner loops unroll (shared-memory
+// offsets and coefficient indices become immediates); the z extent stays a
+// runtime value.
+template <class T, int WX, int WY>
 __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ PartialParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ring = reinterpret_cast<T*>(smem_raw);  // [NB][PH][PW]
@@ -75,8 +76,8 @@ __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ Par
   for (int z = z0 - rz; z < z0 + rz + kPRing; ++z) issue(z);
   const int gx = x0 + tx, gy = y0 + ty;
   const bool active = gx < nx && gy < ny;
-  constexpr int wx = WX;
-  const int wy = 2 * ry + 1, wz = 2 * rz + 1;
+  constexpr int wx = WX, wy = WY;
+  const int wz = 2 * rz + 1;
   for (int z = z0; z < z1; ++z) {
     asm volatile("cp.async.wait_group %0;" ::"n"(kPRing - 1) : "memory");  // plane z + rz landed
     __syncthreads();
@@ -84,6 +85,7 @@ __global__ void __launch_bounds__(PT) partial_kernel(const __grid_constant__ Par
       T sum = T(0);
       for (int mz = 0; mz < wz; ++mz) {
         const T* pl = ring + static_cast<size_t>(slot_of(z + mz - rz)) * PS;
+#pragma unroll
         for (int my = 0; my < wy; ++my) {
           const T* row = pl + (ty + R + my - ry) * PW + tx + R - rx;
           const double* cr = p.coef + (mz * wy + my) * wx;
@@ -130,6 +132,28 @@ int axis_table(int count, int order, double* w) {
   return -1;
 }
 
+template <class T, int WX>
+auto kernel_for_y(int ry) -> void (*)(const PartialParams) {
+  switch (ry) {
+    case 0: return partial_kernel<T, WX, 1>;
+    case 1: return partial_kernel<T, WX, 3>;
+    case 2: return partial_kernel<T, WX, 5>;
+    case 3: return partial_kernel<T, WX, 7>;
+    default: return partial_kernel<T, WX, 9>;
+  }
+}
+
+template <class T>
+auto kernel_for(int rx, int ry) -> void (*)(const PartialParams) {
+  switch (rx) {
+    case 0: return kernel_for_y<T, 1>(ry);
+    case 1: return kernel_for_y<T, 3>(ry);
+    case 2: return kernel_for_y<T, 5>(ry);
+    case 3: return kernel_for_y<T, 7>(ry);
+    default: return kernel_for_y<T, 9>(ry);
+  }
+}
+
 template <class T>
 gc_status launch_partial(gc_context* ctx, PartialParams& p) {
   const int tiles_x = div_up(p.nx, PX), tiles_y = div_up(p.ny, PY);
@@ -140,18 +164,12 @@ gc_status launch_partial(gc_context* ctx, PartialParams& p) {
   p.zc = div_up(p.nz, chunks);
   chunks = div_up(p.nz, p.zc);
   const size_t smem = sizeof(T) * static_cast<size_t>(2 * p.rz + 1 + kPRing) * (PX + 2 * p.R) * (PY + 2 * p.R);
-  void (*kern)(const PartialParams);
-  switch (2 * p.rx + 1) {
-    case 1: kern = partial_kernel<T, 1>; break;
-    case 3: kern = partial_kernel<T, 3>; break;
-    case 5: kern = partial_kernel<T, 5>; break;
-    case 7: kern = partial_kernel<T, 7>; break;
-    default: kern = partial_kernel<T, 9>; break;  // rx <= 4 (checked by axis_table)
-  }
-  static bool attr[5] = {false, false, false, false, false};
-  if (!attr[p.rx]) {
+  // rx, ry <= 4 (axis_table): one instantiation per (WX, WY).
+  void (*kern)(const PartialParams) = kernel_for<T>(p.rx, p.ry);
+  static bool attr[5][5] = {};
+  if (!attr[p.rx][p.ry]) {
     GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
-    attr[p.rx] = true;
+    attr[p.rx][p.ry] = true;
   }
   kern<<<dim3(tiles_x, tiles_y, chunks), dim3(PX, PY), smem, ctx->stream>>>(p);
   GC_CHECK_LAUNCH("partial_kernel");
