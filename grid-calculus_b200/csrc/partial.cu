@@ -12,7 +12,9 @@
 // order (zero products are skipped: that changes only the sign of an exact
 // zero).  Kernel: a 32 x 8 CTA marches up a chunk of z planes through a ring
 // of staged planes (periodic x/y halo of max(rx, ry)) filled by cp.async
-// several planes ahead; radii are runtime values.
+// several planes ahead.  The x and y table widths are template parameters
+// (one instantiation per pair, so both tap loops unroll); the z radius stays
+// a runtime value.
 #include <algorithm>
 
 #include "common.cuh"
