@@ -411,6 +411,312 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
   return GC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Two-column variant of the TMA stage kernel for double grids of even
+// width: the RHS stages (RK4 stages 1-3) and the explicit-Euler step.
+// 64 x 4 threads over a 128-column mu region; a thread owns a pair of
+// adjacent columns in every phase, so shared-memory reads, the in-place y
+// pass and the global stores move 16 bytes per instruction, the address
+// arithmetic of a row is shared by two cells, and each thread carries two
+// independent tap-sum chains.  The single-column kernel is issue-bound, not
+// bandwidth-bound, in these stages.  Cell arithmetic is that of
+// ch_tma_kernel operation for operation, so results are bit-identical.
+//
+// Alignment: tile widths (128 - 2R) and tile origins are even, the staged
+// rows are YX = 128 + 2R doubles (a multiple of 16 bytes), so the x-tap span
+// of a pair (columns 2t .. 2t + 2R + 1 of the y or mu region) and every
+// pair store start on 16-byte boundaries.  The centre pair of a y or mu row
+// (columns 2t + R, 2t + R + 1) is 16-byte aligned only for even R; for
+// R = 1 the whole span (4 doubles) is kept per window row instead.
+constexpr int kX2DT = 64;  // threads in x: column pairs of the mu region
+
+// The x-tap span of pair t in a row: sp[j] = row[2 t + j], j < 2R + 2.
+template <int R>
+__device__ __forceinline__ void x2_span(const double* row, int t, double (&sp)[2 * R + 2]) {
+#pragma unroll
+  for (int j = 0; j < R + 1; ++j) {
+    const double2 v = *reinterpret_cast<const double2*>(row + 2 * t + 2 * j);
+    sp[2 * j] = v.x;
+    sp[2 * j + 1] = v.y;
+  }
+}
+
+// The centre pair of pair t in a row (columns 2t + R, 2t + R + 1).
+template <int R>
+__device__ __forceinline__ double2 x2_centre(const double* row, int t) {
+  if constexpr (R % 2 == 0) {
+    return *reinterpret_cast<const double2*>(row + 2 * t + R);
+  } else {
+    return make_double2(row[2 * t + R], row[2 * t + R + 1]);
+  }
+}
+
+// Laplacian of a pair: x taps from its span, y taps from ya(o), yb(o),
+// o = -R .. R; the axes and the 1-cell z axis combined as in ch_tma_kernel.
+template <int ORDER, class GA, class GB>
+__device__ __forceinline__ void x2_lap_pair(const StageParams<double>& p, const double (&sp)[2 * W<2, ORDER>::R + 2],
+                                            GA ya, GB yb, double& la, double& lb) {
+  using T = double;
+  constexpr int R = W<2, ORDER>::R;
+  const T axa = tap_sum<T, 2, ORDER>([&](int o) { return sp[R + o]; });
+  const T axb = tap_sum<T, 2, ORDER>([&](int o) { return sp[R + 1 + o]; });
+  const T aya = tap_sum<T, 2, ORDER>(ya);
+  const T ayb = tap_sum<T, 2, ORDER>(yb);
+  la = lap_xy(p, axa, aya);
+  lb = lap_xy(p, axb, ayb);
+  if constexpr (ORDER != 2) {
+    const T ca = sp[R], cb = sp[R + 1];
+    la = lap_z(p, la, tap_sum<T, 2, ORDER>([&](int) { return ca; }));
+    lb = lap_z(p, lb, tap_sum<T, 2, ORDER>([&](int) { return cb; }));
+  }
+}
+
+// Runs pair t's window down rows [r0, r1) (at most `count`) of a region
+// with row stride `stride`: row r takes rows r .. r + 2R as its y taps and
+// row r + R's span as its x taps; emit(r, la, lb, ca, cb) receives the two
+// Laplacians and the two centre values.  For R = 1 the window keeps each
+// row's whole span (two 16-byte loads per row and pair, nothing else).
+template <int ORDER, int COUNT, class Emit>
+__device__ __forceinline__ void x2_sweep(const StageParams<double>& p, const double* src, int stride, int t, int r0,
+                                         int r1, Emit emit) {
+  using T = double;
+  constexpr int R = W<2, ORDER>::R;
+  constexpr int NS = 2 * R + 2, NW = 2 * R + 1;
+  if constexpr (R == 1) {
+    T sw[3][NS];
+    x2_span<R>(src + r0 * stride, t, sw[1]);
+    x2_span<R>(src + (r0 + 1) * stride, t, sw[2]);
+#pragma unroll
+    for (int k = 0; k < COUNT; ++k) {
+      const int r = r0 + k;
+      if (r >= r1) break;
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        sw[0][j] = sw[1][j];
+        sw[1][j] = sw[2][j];
+      }
+      x2_span<R>(src + (r + 2) * stride, t, sw[2]);
+      T la, lb;
+      x2_lap_pair<ORDER>(p, sw[1], [&](int o) { return sw[1 + o][1]; }, [&](int o) { return sw[1 + o][2]; }, la, lb);
+      emit(r, la, lb, sw[1][1], sw[1][2]);
+    }
+  } else {
+    double2 win[NW];
+#pragma unroll
+    for (int q = 0; q < 2 * R; ++q) win[q + 1] = x2_centre<R>(src + (r0 + q) * stride, t);
+#pragma unroll
+    for (int k = 0; k < COUNT; ++k) {
+      const int r = r0 + k;
+      if (r >= r1) break;
+#pragma unroll
+      for (int q = 0; q + 1 < NW; ++q) win[q] = win[q + 1];
+      win[NW - 1] = x2_centre<R>(src + (r + 2 * R) * stride, t);
+      T sp[NS];
+      x2_span<R>(src + (r + R) * stride, t, sp);
+      T la, lb;
+      x2_lap_pair<ORDER>(p, sp, [&](int o) { return win[R + o].x; }, [&](int o) { return win[R + o].y; }, la, lb);
+      emit(r, la, lb, win[R].x, win[R].y);
+    }
+  }
+}
+
+template <int ORDER, bool KIN>
+struct TmaX2Layout {
+  static constexpr int R = W<2, ORDER>::R;
+  static constexpr int MX = 2 * kX2DT, TX = MX - 2 * R, TY = kT2Y;
+  static constexpr int YX = TX + 4 * R, YY = TY + 4 * R, MY = TY + 2 * R;
+  static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
+  static constexpr size_t YB = al(sizeof(double) * YX * YY);
+  static constexpr size_t BUF = YB * (KIN ? 2 : 1);
+  static constexpr size_t OFF_BUF = 128;
+  static constexpr size_t MSB = al(sizeof(double) * MX * MY);
+  // Input buffers: two (the next tile's TMA lands while this one computes)
+  // when two such CTAs fit in an SM's 228 KB of shared memory (each also
+  // holds 1 KB reserved by the hardware); otherwise one, where the next
+  // tile's TMA is issued once the y region is consumed (after phase 2) and
+  // an L2 prefetch of that tile at the start of this one covers its
+  // latency.  Order 2 with k_prev: two buffers, 100 KB, two CTAs per SM;
+  // order 4 with k_prev: one buffer, 71 KB, three CTAs per SM instead of one.
+  static constexpr int NB = 2 * (OFF_BUF + 2 * BUF + MSB + 128 + 1024) <= 228 * 1024 ? 2 : 1;
+  static constexpr size_t OFF_MS = OFF_BUF + NB * BUF;
+  static constexpr size_t BYTES = OFF_MS + MSB + 128;
+  static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(double) * YX * YY * (KIN ? 2 : 1));
+  static_assert(YX % 2 == 0 && TX % 2 == 0 && (YX * YY) % 2 == 0, "pairs must stay 16-byte aligned");
+};
+
+template <int ORDER, int MODE, bool KIN>
+__global__ void __launch_bounds__(kX2DT * kT2TY) ch_tma_x2_kernel(
+    const StageParams<double> p, const __grid_constant__ CUtensorMap m_psi,
+    const __grid_constant__ CUtensorMap m_kin, const int tiles_x, const int tiles_y, int* status) {
+  using T = double;
+  using L = TmaX2Layout<ORDER, KIN>;
+  static_assert(MODE == MODE_RHS || L::NB == 2, "a single input buffer holds psi only until phase 2");
+  constexpr int R = L::R, TX = L::TX, TY = L::TY, YX = L::YX, YY = L::YY, MX = L::MX, MY = L::MY;
+  constexpr int NT = kX2DT * kT2TY;
+  constexpr int NB = L::NB;
+  constexpr int MS = (MY + kT2TY - 1) / kT2TY;
+  constexpr int OS = TY / kT2TY;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+  int* s_abort = reinterpret_cast<int*>(base + 64);
+  auto buf_psi = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF); };
+  auto buf_kin = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + L::YB); };
+  T* ms = reinterpret_cast<T*>(base + L::OFF_MS);
+
+  const int nx = p.nx, ny = p.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kX2DT + tx;
+  const int ntiles = tiles_x * tiles_y;
+
+  auto tile_origin = [&](int tl, int& x0, int& y0) {
+    x0 = (tl % tiles_x) * TX;
+    y0 = (tl / tiles_x) * TY;
+  };
+  auto interior = [&](int x0, int y0) {
+    return x0 - 2 * R >= 0 && x0 - 2 * R + YX <= nx && y0 - 2 * R >= 0 && y0 - 2 * R + YY <= ny;
+  };
+  auto issue = [&](int tl, int b) {  // one thread
+    int x0, y0;
+    tile_origin(tl, x0, y0);
+    if (interior(x0, y0)) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&bar[b], L::TX_BYTES);
+      tma_load_2d(buf_psi(b), &m_psi, x0 - 2 * R, y0 - 2 * R, &bar[b]);
+      if constexpr (KIN) tma_load_2d(buf_kin(b), &m_kin, x0 - 2 * R, y0 - 2 * R, &bar[b]);
+    } else {
+      mbar_arrive(&bar[b]);
+    }
+  };
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    *s_abort = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+
+  int i = 0;
+  for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x, ++i) {
+    const int b = NB == 2 ? (i & 1) : 0;
+    const uint32_t parity = NB == 2 ? (i >> 1) & 1 : i & 1;
+    const int next = tl + static_cast<int>(gridDim.x);
+    if (tid == 0 && next < ntiles) {
+      if constexpr (NB == 2) {
+        issue(next, b ^ 1);
+      } else {
+        int nx0, ny0;
+        tile_origin(next, nx0, ny0);
+        if (interior(nx0, ny0)) {
+          tma_prefetch_2d(&m_psi, nx0 - 2 * R, ny0 - 2 * R);
+          tma_prefetch_2d(&m_kin, nx0 - 2 * R, ny0 - 2 * R);
+        }
+      }
+    }
+    int x0, y0;
+    tile_origin(tl, x0, y0);
+    const long long t_start = clock64();
+    while (!mbar_try_wait(&bar[b], parity)) {
+      if (clock64() - t_start > kWaitBudgetCycles) {
+        *s_abort = 1;
+        atomicExch(status, static_cast<int>(GC_ERR_TIMEOUT));
+        break;
+      }
+    }
+    T* ps = buf_psi(b);
+    if (!interior(x0, y0)) {
+      T* ks = buf_kin(b);
+      for (int e = tid; e < YX * YY; e += NT) {
+        const int r = e / YX, cc = e - r * YX;
+        const size_t gi = static_cast<size_t>(wrap(y0 - 2 * R + r, ny)) * nx + wrap(x0 - 2 * R + cc, nx);
+        ps[e] = p.psi[gi];
+        if constexpr (KIN) ks[e] = p.kin[gi];
+      }
+    }
+    __syncthreads();
+    if (*s_abort) {
+      if (NB == 2 && tid == 0 && next < ntiles) {
+        const long long t_drain = clock64();
+        while (!mbar_try_wait(&bar[b ^ 1], ((i + 1) >> 1) & 1) && clock64() - t_drain < kWaitBudgetCycles) {
+        }
+      }
+      break;
+    }
+
+    // y = psi + a k_prev, in place over k_prev, a pair per thread and step.
+    const T* ys = ps;
+    if constexpr (KIN) {
+      double2* k2 = reinterpret_cast<double2*>(buf_kin(b));
+      const double2* p2 = reinterpret_cast<const double2*>(ps);
+      for (int e = tid; e < YX * YY / 2; e += NT) {
+        const double2 v = p2[e];
+        double2 w = k2[e];
+        w.x = Ar<T>::add(v.x, Ar<T>::mul(p.a, w.x));
+        w.y = Ar<T>::add(v.y, Ar<T>::mul(p.a, w.y));
+        k2[e] = w;
+      }
+      __syncthreads();
+      ys = buf_kin(b);
+    }
+
+    // Phase 2: mu on mu columns 2 tx, 2 tx + 1 of the mu-row strip.
+    {
+      const int m0 = ty * MS;
+      x2_sweep<ORDER, MS>(p, ys, YX, tx, m0, min(m0 + MS, MY), [&](int m, T la, T lb, T ya, T yb) {
+        *reinterpret_cast<double2*>(ms + m * MX + 2 * tx) = make_double2(chem_pot(p, ya, la), chem_pot(p, yb, lb));
+      });
+    }
+    __syncthreads();
+    // One buffer: the y region is consumed, the next tile may land in it.
+    if (NB == 1 && tid == 0 && next < ntiles) issue(next, 0);
+
+    // Phase 3: output pair (2 tx, 2 tx + 1) of each of this thread's rows.
+    if (2 * tx < TX && x0 + 2 * tx < nx) {
+      const int o0 = ty * OS;
+      const int o1 = min(o0 + OS, ny - y0);
+      x2_sweep<ORDER, OS>(p, ms, MX, tx, o0, o1, [&](int oy, T la, T lb, T, T) {
+        const double2 rhs = make_double2(mobility(p, la), mobility(p, lb));
+        const size_t gi = static_cast<size_t>(y0 + oy) * nx + (x0 + 2 * tx);
+        double2* out = reinterpret_cast<double2*>(p.out + gi);
+        if constexpr (MODE == MODE_RHS) {
+          *out = rhs;
+        } else {  // MODE_EULER_FINAL
+          const double2 pc = *reinterpret_cast<const double2*>(ps + (oy + 2 * R) * YX + 2 * tx + 2 * R);
+          *out = make_double2(Ar<T>::add(pc.x, Ar<T>::mul(p.c6, rhs.x)), Ar<T>::add(pc.y, Ar<T>::mul(p.c6, rhs.y)));
+        }
+      });
+    }
+    __syncthreads();
+  }
+}
+
+// Launches the two-column kernel when its rules hold (even width, 16-byte
+// aligned output, the staged region fits the grid); GC_ERR_UNSUPPORTED
+// (nothing launched) otherwise.
+template <int ORDER, int MODE, bool KIN>
+gc_status launch_tma_x2(gc_context* ctx, const StageParams<double>& p) {
+  using L = TmaX2Layout<ORDER, KIN>;
+  if (p.nx % 2 != 0 || p.nx < L::YX || p.ny < L::YY || reinterpret_cast<uintptr_t>(p.out) % 16 != 0) {
+    return GC_ERR_UNSUPPORTED;
+  }
+  CUtensorMap mpsi{}, mkin{};
+  if (!make_tensor_map_2d(&mpsi, p.psi, p.nx, p.ny, 8, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
+  if (KIN && !make_tensor_map_2d(&mkin, p.kin, p.nx, p.ny, 8, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
+  auto kern = ch_tma_x2_kernel<ORDER, MODE, KIN>;
+  static int ctas_per_sm = 0;  // one instantiation per template argument set
+  if (ctas_per_sm == 0) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::BYTES)));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kX2DT * kT2TY, L::BYTES));
+    if (ctas_per_sm < 1) ctas_per_sm = 1;
+  }
+  const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
+  const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
+  const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
+  kern<<<grid, dim3(kX2DT, kT2TY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, tiles_x, tiles_y, ctx->device_status);
+  GC_CHECK_LAUNCH("ch_tma_x2_kernel");
+  return GC_OK;
+}
+
 // Single-grid work source for the cp.async-pipelined persistent loop.
 template <class T>
 struct GridSource {
@@ -488,6 +794,17 @@ gc_status launch_pipe_x2(gc_context* ctx, const StageParams<float>& p) {
 // float on even widths).
 template <class T, int ORDER, int MODE>
 gc_status launch_2d(gc_context* ctx, const StageParams<T>& p) {
+  if constexpr (sizeof(T) == 8 && (MODE == MODE_RHS || MODE == MODE_EULER_FINAL)) {
+    gc_status s = GC_ERR_UNSUPPORTED;
+    if constexpr (ORDER != 6) {  // order 6: 118 registers in two columns, slower than one
+      if (!p.kin) {
+        s = launch_tma_x2<ORDER, MODE, false>(ctx, p);
+      } else if constexpr (MODE == MODE_RHS) {
+        s = launch_tma_x2<ORDER, MODE, true>(ctx, p);
+      }
+    }
+    if (s != GC_ERR_UNSUPPORTED) return s;
+  }
   if constexpr (sizeof(T) == 8 && MODE != MODE_RKC_FIRST && MODE != MODE_RKC) {
     gc_status s;
     if constexpr (MODE == MODE_RHS) {

@@ -67,6 +67,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Prefetch of the same box into L2 (no shared memory, no barrier); the
+// alignment rule on x is that of tma_load_2d.
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y)
+               : "memory");
+}
+
 // Host: builds a 2-D tensor map over a row-major nx x ny field of elem_bytes
 // values with a box of box_x x box_y.  False when the driver entry point is
 // missing or the layout breaks a TMA rule (base 16-byte aligned, row pitch a
