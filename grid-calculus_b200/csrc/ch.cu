@@ -414,7 +414,8 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
 // ---------------------------------------------------------------------------
 // Two-column variant of the TMA stage kernel for double grids of even
 // width: the RHS stages (RK4 stages 1-3) and the explicit-Euler step.
-// 64 x 4 threads over a 128-column mu region; a thread owns a pair of
+// 64 threads in x over a 128-column mu region (8 thread rows over 32-row
+// tiles at order 2, 4 over 16 rows at order 4); a thread owns a pair of
 // adjacent columns in every phase, so shared-memory reads, the in-place y
 // pass and the global stores move 16 bytes per instruction, the address
 // arithmetic of a row is shared by two cells, and each thread carries two
@@ -482,6 +483,7 @@ __device__ __forceinline__ void x2_sweep(const StageParams<double>& p, const dou
   using T = double;
   constexpr int R = W<2, ORDER>::R;
   constexpr int NS = 2 * R + 2, NW = 2 * R + 1;
+  if (r0 >= r1) return;  // an idle thread row: not even the window's first rows
   if constexpr (R == 1) {
     T sw[3][NS];
     x2_span<R>(src + r0 * stride, t, sw[1]);
@@ -523,7 +525,11 @@ __device__ __forceinline__ void x2_sweep(const StageParams<double>& p, const dou
 template <int ORDER, bool KIN>
 struct TmaX2Layout {
   static constexpr int R = W<2, ORDER>::R;
-  static constexpr int MX = 2 * kX2DT, TX = MX - 2 * R, TY = kT2Y;
+  // Order 2: 64 x 8 threads over 32-row tiles (32 warps per SM in both
+  // stage kinds, 36 staged rows per 32 output rows); wider stencils keep
+  // 64 x 4 threads over 16 rows, whose staged regions fit three CTAs per SM.
+  static constexpr int NTY = ORDER == 2 ? 8 : kT2TY;
+  static constexpr int MX = 2 * kX2DT, TX = MX - 2 * R, TY = ORDER == 2 ? 32 : kT2Y;
   static constexpr int YX = TX + 4 * R, YY = TY + 4 * R, MY = TY + 2 * R;
   static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
   static constexpr size_t YB = al(sizeof(double) * YX * YY);
@@ -535,8 +541,9 @@ struct TmaX2Layout {
   // holds 1 KB reserved by the hardware); otherwise one, where the next
   // tile's TMA is issued once the y region is consumed (after phase 2) and
   // an L2 prefetch of that tile at the start of this one covers its
-  // latency.  Order 2 with k_prev: two buffers, 100 KB, two CTAs per SM;
-  // order 4 with k_prev: one buffer, 71 KB, three CTAs per SM instead of one.
+  // latency.  Order 2: two buffers without k_prev and one with it, 108 KB
+  // and two 512-thread CTAs per SM either way; order 4 with k_prev: one
+  // buffer, 71 KB, three CTAs per SM instead of one.
   static constexpr int NB = 2 * (OFF_BUF + 2 * BUF + MSB + 128 + 1024) <= 228 * 1024 ? 2 : 1;
   static constexpr size_t OFF_MS = OFF_BUF + NB * BUF;
   static constexpr size_t BYTES = OFF_MS + MSB + 128;
@@ -545,17 +552,18 @@ struct TmaX2Layout {
 };
 
 template <int ORDER, int MODE, bool KIN>
-__global__ void __launch_bounds__(kX2DT * kT2TY) ch_tma_x2_kernel(
+__global__ void __launch_bounds__(kX2DT * TmaX2Layout<ORDER, KIN>::NTY) ch_tma_x2_kernel(
     const StageParams<double> p, const __grid_constant__ CUtensorMap m_psi,
     const __grid_constant__ CUtensorMap m_kin, const int tiles_x, const int tiles_y, int* status) {
   using T = double;
   using L = TmaX2Layout<ORDER, KIN>;
   static_assert(MODE == MODE_RHS || L::NB == 2, "a single input buffer holds psi only until phase 2");
   constexpr int R = L::R, TX = L::TX, TY = L::TY, YX = L::YX, YY = L::YY, MX = L::MX, MY = L::MY;
-  constexpr int NT = kX2DT * kT2TY;
+  constexpr int NTY = L::NTY, NT = kX2DT * NTY;
   constexpr int NB = L::NB;
-  constexpr int MS = (MY + kT2TY - 1) / kT2TY;
-  constexpr int OS = TY / kT2TY;
+  constexpr int MS = (MY + NTY - 1) / NTY;
+  constexpr int OS = TY / NTY;
+  static_assert(TY % NTY == 0, "output rows split evenly over thread rows");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   uint64_t* bar = reinterpret_cast<uint64_t*>(base);
@@ -706,13 +714,13 @@ gc_status launch_tma_x2(gc_context* ctx, const StageParams<double>& p) {
   static int ctas_per_sm = 0;  // one instantiation per template argument set
   if (ctas_per_sm == 0) {
     GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::BYTES)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kX2DT * kT2TY, L::BYTES));
+    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kX2DT * L::NTY, L::BYTES));
     if (ctas_per_sm < 1) ctas_per_sm = 1;
   }
   const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
   const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
   const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
-  kern<<<grid, dim3(kX2DT, kT2TY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, tiles_x, tiles_y, ctx->device_status);
+  kern<<<grid, dim3(kX2DT, L::NTY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, tiles_x, tiles_y, ctx->device_status);
   GC_CHECK_LAUNCH("ch_tma_x2_kernel");
   return GC_OK;
 }
