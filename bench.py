@@ -49,9 +49,9 @@ DT = 0.01
 # k_prev and write k_s, stage 4 reads psi, k1, k2, k3 and writes psi').
 BYTES_PER_CELL_STEP = 13 * 8
 # DRAM bytes (read + write) per RK4 step per cell measured by ncu for the
-# four stage kernels (profiles/ch_rk4_fp64_tma_4096.md: 1630.6 MB per step on
-# 4096^2, both sizes beyond L2, so it scales with the cell count).
-NCU_TRAFFIC_PER_CELL_STEP = 97.2
+# four stage kernels (one full capture on 4096^2: 1648.0 MB per step for
+# 16.8 M cells; both sizes are beyond L2, so it scales with the cell count).
+NCU_TRAFFIC_PER_CELL_STEP = 98.2
 
 
 def peaks():
@@ -695,7 +695,8 @@ def run_ours(args, rank: int, world: int, local: int):
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "ch_tma_kernel (4 launches per step, 104 B/cell-step algorithmic)",
+                         "kernel": "ch_tma_x2_kernel (RK4 stages 1-3) + ch_tma_kernel (stage 4): "
+                                   "4 launches per step, 104 B/cell-step algorithmic",
                          "traffic_unit": "bytes per launch (average of the 4 stage launches)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": cells * 8 / chunk,
