@@ -118,6 +118,41 @@ def test_2d_tma_tiles_interior_edge_partial(gc, oracle, shape, order):
     gc.context().synchronize()  # reports a timed-out device wait, if any
 
 
+@pytest.mark.parametrize("shape", [(1, 36, 260), (1, 37, 130), (1, 70, 132), (1, 41, 382)])
+@pytest.mark.parametrize("order", [2, 4])
+def test_2d_two_column_edges_non_unit(gc, oracle, shape, order):
+    """The two-column kernel's limits: a height equal to its staged rows (36
+    at order 2: no tile is interior in y), a width equal to its staged
+    columns (130 / 132), widths that leave a narrow last tile, and anisotropic
+    spacing with M, kappa != 1 (no unit shortcuts); RK4 and Euler."""
+    h = (0.9, 1.2, 1.0)
+    psi0 = uniform_ic(shape, 11 * order + shape[1])
+    dt = {2: 0.004, 4: 0.002}[order]
+    rhs = gc.CahnHilliardRhs(0.8, 1.3, order)
+    g = grid_of(gc, shape, h)
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt, 12, gc.RK4)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.3, psi0, dt, 12, h=h))
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt, 4, gc.ExplicitEuler)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.3, psi0, dt, 4, rk4=False, h=h))
+
+
+def test_2d_state_buffer_off_16_byte_boundary(gc, oracle):
+    """A state field starting 8 bytes past a 16-byte boundary cannot be a TMA
+    source or a 16-byte store target: the stage launches take the plain
+    kernels for it, and the result is the same bits."""
+    import torch
+    shape = (1, 96, 260)
+    psi0 = uniform_ic(shape, 5)
+    flat = torch.empty(psi0.size + 1, dtype=torch.float64, device="cuda")
+    t = flat[1:].view(shape)
+    assert t.data_ptr() % 16 == 8
+    t.copy_(dev(psi0))
+    gc.ch_integrate(t, grid_of(gc, shape), gc.CahnHilliardRhs(1.0, 1.0, 2), 0.01, 10, gc.RK4)
+    assert np.array_equal(host(t), oracle.ch_integrate(2, 1.0, 1.0, psi0, 0.01, 10))
+
+
 def test_3d_and_anisotropic(gc, oracle):
     shape = (12, 10, 14)
     h = (0.9, 1.1, 1.3)
