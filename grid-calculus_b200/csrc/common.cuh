@@ -78,7 +78,6 @@ enum ScratchSlot {
   kSlotK3,
   kSlotPsiB,
   kSlotReduce,
-  kSlotIntegrand,
   kSlotFlags,
   kSlotMisc,
   kSlotSpectral,
@@ -128,6 +127,13 @@ gc_status kahan_finish(gc_context* ctx, double* part, double* result);
 // reference's pairwise tree (GC_SUM_PAIRWISE) or the deterministic
 // compensated sum (GC_SUM_KAHAN); synchronises and returns it on the host.
 gc_status sum_any(gc_context* ctx, gc_dtype dt, const void* x, long long n, gc_sum sum, double* result);
+
+// func::evaluate of a checked integrand program over a field whose axis
+// extents were checked: the NVRTC-compiled chunk walk forms the integrand
+// from the field and its neighbours and reduces it (no integrand field in
+// HBM); returns volume x sum on the host.
+gc_status run_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field, const gc_program* f,
+                      gc_sum sum, double* result);
 
 // A named NVTX range for the duration of a scope: the long-running entry
 // points show up by name on an Nsight Systems / NVTX timeline (no cost when

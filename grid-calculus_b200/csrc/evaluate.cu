@@ -539,6 +539,27 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   // gradient (radius 1), Laplacian (radius 1), biharmonic (radius 2).
   if (f->arity >= 2 && (s = require_axes(g, 1)) != GC_OK) return s;
   if (f->components == 1 && f->arity >= 4 && (s = require_axes(g, 2)) != GC_OK) return s;
+  return run_program(ctx, g, dt, field, f, sum, result);
+}
+
+GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap) {
+  if (!f || check_program(f) != GC_OK) return 0;
+  const std::string src = program_source(f, dt);
+  if (buf && cap) {
+    const size_t n = std::min(cap - 1, src.size());
+    std::memcpy(buf, src.data(), n);
+    buf[n] = '\0';
+  }
+  return src.size() + 1;
+}
+
+}  // extern "C"
+
+namespace gcb {
+
+gc_status run_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field, const gc_program* f,
+                      gc_sum sum, double* result) {
+  gc_status s;
   Compiled k;
   if ((s = compile(ctx, program_source(f, dt), &k)) != GC_OK) return s;
   Driver drv;
@@ -581,15 +602,4 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
   return GC_OK;
 }
 
-GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap) {
-  if (!f || check_program(f) != GC_OK) return 0;
-  const std::string src = program_source(f, dt);
-  if (buf && cap) {
-    const size_t n = std::min(cap - 1, src.size());
-    std::memcpy(buf, src.data(), n);
-    buf[n] = '\0';
-  }
-  return src.size() + 1;
-}
-
-}  // extern "C"
+}  // namespace gcb

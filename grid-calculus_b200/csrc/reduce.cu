@@ -81,49 +81,6 @@ __global__ void __launch_bounds__(1024) kahan_final(const double* __restrict__ i
   if (threadIdx.x == 0) out[0] = __dadd_rn(sh[0].s, sh[0].c);
 }
 
-// ---- integrands (func/Functional.hpp:88-148 over cahn_hilliard.hpp:64-77) --
-template <class T>
-__global__ void integrand_kernel(const T* __restrict__ psi, int nx, int ny, int nz, double ihx,
-                                 double ihy, double ihz, int kind, double kappa,
-                                 double* __restrict__ out) {
-  const size_t n = static_cast<size_t>(nx) * ny * nz;
-  for (size_t c = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < n;
-       c += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const double p = static_cast<double>(psi[c]);
-    double f;
-    if (kind == GC_INTEGRAND_PSI) {
-      f = p;
-    } else if (kind == GC_INTEGRAND_PSI_SQUARED) {
-      f = __dmul_rn(p, p);
-    } else {
-      const int i = static_cast<int>(c % nx);
-      const size_t rest = c / nx;
-      const int j = static_cast<int>(rest % ny);
-      const int k = static_cast<int>(rest / ny);
-      const size_t row = static_cast<size_t>(nx);
-      const size_t plane = static_cast<size_t>(nx) * ny;
-      auto val = [&](int ii, int jj, int kk) {
-        return static_cast<double>(psi[static_cast<size_t>(wrap(kk, nz)) * plane +
-                                       static_cast<size_t>(wrap(jj, ny)) * row + wrap(ii, nx)]);
-      };
-      // Order-2 gradient, the reference's default (diff/Gradient.hpp:59-69).
-      const double dx = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i - 1, j, k)), __dmul_rn(0.5, val(i + 1, j, k))), ihx);
-      const double dy = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i, j - 1, k)), __dmul_rn(0.5, val(i, j + 1, k))), ihy);
-      const double dz = __dmul_rn(__dadd_rn(__dmul_rn(-0.5, val(i, j, k - 1)), __dmul_rn(0.5, val(i, j, k + 1))), ihz);
-      const double sq = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-      if (kind == GC_INTEGRAND_GRAD_SQUARED) {
-        f = sq;
-      } else {
-        const double t1 = __dmul_rn(__dmul_rn(-0.5, p), p);
-        const double t2 = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.25, p), p), p), p);
-        const double t3 = __dmul_rn(__dmul_rn(0.5, kappa), sq);
-        f = __dadd_rn(__dadd_rn(t1, t2), t3);
-      }
-    }
-    out[c] = f;
-  }
-}
-
 // ---- largest harmonic face D (solve/Diffusion.hpp:187-207) -----------------
 template <class T>
 __global__ void d_max_face_kernel(const T* __restrict__ D, int nx, int ny, int nz,
@@ -304,32 +261,73 @@ gc_status first_nonpositive(gc_context* ctx, const gc_grid* g, gc_dtype dt, cons
   return GC_OK;
 }
 
+// The hot-path integrands (cahn_hilliard.hpp:64-77, heterogeneous_diffusion.hpp:82)
+// as integrand programs: the operations of the reference's expressions in
+// its order, so the fused evaluation gives its values bit for bit.
+// -psi^2/2 + psi^4/4 + kappa/2 |grad psi|^2 is ((-0.5 p) p + (((0.25 p) p) p) p)
+// + (0.5 kappa) ((gx gx + gy gy) + gz gz).
+gc_program fixed_program(int kind, double kappa) {
+  gc_program f{};
+  f.components = 1;
+  auto op = [&](int code, int dst, int a, int b, double v = 0.0) {
+    f.instr[f.n_instr++] = gc_instr{static_cast<int16_t>(code), static_cast<int16_t>(dst), static_cast<int16_t>(a),
+                                    static_cast<int16_t>(b), v};
+  };
+  auto grad_squared = [&](int into) {  // registers 1..3 hold the gradient; result in `into`
+    op(GC_OPC_MUL, 1, 1, 1);
+    op(GC_OPC_MUL, 2, 2, 2);
+    op(GC_OPC_ADD, 1, 1, 2);
+    op(GC_OPC_MUL, 3, 3, 3);
+    op(GC_OPC_ADD, into, 1, 3);
+  };
+  switch (kind) {
+    case GC_INTEGRAND_PSI:
+      f.arity = 1;
+      op(GC_OPC_INPUT, 0, GC_IN_PSI, 0);
+      break;
+    case GC_INTEGRAND_PSI_SQUARED:
+      f.arity = 1;
+      op(GC_OPC_INPUT, 0, GC_IN_PSI, 0);
+      op(GC_OPC_MUL, 0, 0, 0);
+      break;
+    case GC_INTEGRAND_GRAD_SQUARED:
+      f.arity = 2;
+      op(GC_OPC_INPUT, 1, GC_IN_GRAD_X, 0);
+      op(GC_OPC_INPUT, 2, GC_IN_GRAD_Y, 0);
+      op(GC_OPC_INPUT, 3, GC_IN_GRAD_Z, 0);
+      grad_squared(0);
+      break;
+    default:  // GC_INTEGRAND_CH_FREE_ENERGY
+      f.arity = 2;
+      op(GC_OPC_INPUT, 0, GC_IN_PSI, 0);
+      op(GC_OPC_INPUT, 1, GC_IN_GRAD_X, 0);
+      op(GC_OPC_INPUT, 2, GC_IN_GRAD_Y, 0);
+      op(GC_OPC_INPUT, 3, GC_IN_GRAD_Z, 0);
+      op(GC_OPC_CONST, 4, 0, 0, -0.5);
+      op(GC_OPC_MUL, 4, 4, 0);
+      op(GC_OPC_MUL, 4, 4, 0);
+      op(GC_OPC_CONST, 5, 0, 0, 0.25);
+      for (int q = 0; q < 4; ++q) op(GC_OPC_MUL, 5, 5, 0);
+      op(GC_OPC_ADD, 5, 4, 5);
+      grad_squared(3);
+      op(GC_OPC_CONST, 1, 0, 0, 0.5 * kappa);
+      op(GC_OPC_MUL, 1, 1, 3);
+      op(GC_OPC_ADD, 5, 5, 1);
+      break;
+  }
+  return f;
+}
+
 gc_status evaluate_any(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
                        const gc_integrand* f, gc_sum sum, double* result) {
-  const long long n = static_cast<long long>(cells(g));
-  const double vol = g->hx * g->hy * g->hz;
-  if (f->kind == GC_INTEGRAND_PSI && dt == GC_F64) {
+  if (f->kind == GC_INTEGRAND_PSI && dt == GC_F64) {  // the field itself: a plain sum
     double s = 0.0;
-    gc_status st = sum_any(ctx, dt, psi, n, sum, &s);
-    *result = vol * s;
+    const gc_status st = sum_any(ctx, dt, psi, static_cast<long long>(cells(g)), sum, &s);
+    *result = g->hx * g->hy * g->hz * s;
     return st;
   }
-  void* buf = nullptr;
-  gc_status st = scratch_get(ctx, kSlotIntegrand, sizeof(double) * static_cast<size_t>(n), &buf);
-  if (st != GC_OK) return st;
-  double* integrand = static_cast<double*>(buf);
-  const int blocks = ctx->num_sms * 8;
-  if (dt == GC_F64)
-    integrand_kernel<double><<<blocks, 256, 0, ctx->stream>>>(static_cast<const double*>(psi), g->nx, g->ny, g->nz,
-                                                              1.0 / g->hx, 1.0 / g->hy, 1.0 / g->hz, f->kind, f->kappa, integrand);
-  else
-    integrand_kernel<float><<<blocks, 256, 0, ctx->stream>>>(static_cast<const float*>(psi), g->nx, g->ny, g->nz,
-                                                             1.0 / g->hx, 1.0 / g->hy, 1.0 / g->hz, f->kind, f->kappa, integrand);
-  GC_CHECK_LAUNCH("integrand_kernel");
-  double s = 0.0;
-  st = sum_any(ctx, GC_F64, integrand, n, sum, &s);
-  *result = vol * s;
-  return st;
+  const gc_program prog = fixed_program(f->kind, f->kappa);
+  return run_program(ctx, g, dt, psi, &prog, sum, result);
 }
 
 }  // namespace gcb

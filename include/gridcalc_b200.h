@@ -184,7 +184,10 @@ typedef struct gc_integrand {
 } gc_integrand;
 
 /* func::evaluate(psi, f, tag): the integrand is formed on the device from
- * psi and its order-2 gradient (the reference's default) and reduced in FP64. */
+ * psi and its order-2 gradient (the reference's default) and reduced in FP64,
+ * in one pass over psi (the integrand runs as a built-in program of
+ * gc_evaluate_program below, with the reference expression's operations in
+ * its order). */
 GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,
                              const gc_integrand* f, gc_sum sum, double* result);
 
