@@ -430,6 +430,7 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
 // (columns 2t + R, 2t + R + 1) is 16-byte aligned only for even R; for
 // R = 1 the whole span (4 doubles) is kept per window row instead.
 constexpr int kX2DT = 64;  // threads in x: column pairs of the mu region
+constexpr long long kX2MinRounds = 10;  // tiles per persistent CTA for the two-column kernel
 
 // The x-tap span of pair t in a row: sp[j] = row[2 t + j], j < 2R + 2.
 template <int R>
@@ -699,8 +700,9 @@ __global__ void __launch_bounds__(kX2DT * TmaX2Layout<ORDER, KIN>::NTY) ch_tma_x
 }
 
 // Launches the two-column kernel when its rules hold (even width, 16-byte
-// aligned output, the staged region fits the grid); GC_ERR_UNSUPPORTED
-// (nothing launched) otherwise.
+// aligned output, the staged region fits the grid, enough tiles to fill
+// ten rounds of persistent CTAs); GC_ERR_UNSUPPORTED (nothing launched)
+// otherwise, and the caller uses ch_tma_kernel.
 template <int ORDER, int MODE, bool KIN>
 gc_status launch_tma_x2(gc_context* ctx, const StageParams<double>& p) {
   using L = TmaX2Layout<ORDER, KIN>;
@@ -719,7 +721,15 @@ gc_status launch_tma_x2(gc_context* ctx, const StageParams<double>& p) {
   }
   const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
   const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
-  const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
+  const long long slots = static_cast<long long>(ctas_per_sm) * ctx->num_sms;
+  // The two-column tiles hold 4x (order 2) or 2x (order 4) the cells of the
+  // one-column kernel's: with fewer than ten rounds of them per persistent
+  // CTA, idle SMs and the partly filled last round cost more than the two
+  // columns save (measured on B200, RK4 per step at order 2: 512^2 31 vs 24 us,
+  // 3072^2 273 vs 240 us, 4096^2 424 vs 430 us, 8192^2 1.54 vs 1.70 ms; order 4:
+  // 2048^2 equal, 3072^2 370 vs 389 us).
+  if (ntiles < kX2MinRounds * slots) return GC_ERR_UNSUPPORTED;
+  const int grid = static_cast<int>(std::min<long long>(ntiles, slots));
   kern<<<grid, dim3(kX2DT, L::NTY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, tiles_x, tiles_y, ctx->device_status);
   GC_CHECK_LAUNCH("ch_tma_x2_kernel");
   return GC_OK;

@@ -120,10 +120,9 @@ def test_2d_tma_tiles_interior_edge_partial(gc, oracle, shape, order):
 
 @pytest.mark.parametrize("shape", [(1, 36, 260), (1, 37, 130), (1, 70, 132), (1, 41, 382)])
 @pytest.mark.parametrize("order", [2, 4])
-def test_2d_two_column_edges_non_unit(gc, oracle, shape, order):
-    """The two-column kernel's limits: a height equal to its staged rows (36
-    at order 2: no tile is interior in y), a width equal to its staged
-    columns (130 / 132), widths that leave a narrow last tile, and anisotropic
+def test_2d_edges_non_unit(gc, oracle, shape, order):
+    """Small even-width grids (the one-column TMA kernel): heights and widths
+    at or just above a staged region's, a narrow last tile, and anisotropic
     spacing with M, kappa != 1 (no unit shortcuts); RK4 and Euler."""
     h = (0.9, 1.2, 1.0)
     psi0 = uniform_ic(shape, 11 * order + shape[1])
@@ -136,6 +135,33 @@ def test_2d_two_column_edges_non_unit(gc, oracle, shape, order):
     t = dev(psi0)
     gc.ch_integrate(t, g, rhs, dt, 4, gc.ExplicitEuler)
     assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.3, psi0, dt, 4, rk4=False, h=h))
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_2d_two_column_large_grid(gc, oracle, order):
+    """Grids large enough for the two-column kernel (at least ten rounds of
+    its tiles per persistent CTA: 126 x 32 tiles in two 512-thread CTAs per
+    SM at order 2, 124 x 16 in three 256-thread CTAs at order 4), with a
+    partial last tile in x and in y and non-unit h, M, kappa; RK4 (its three
+    RHS stages) and Euler, bit-identical to the oracle."""
+    import math
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    nx = 4094                                   # even; last tile 62 (order 2) / 2 (order 4) columns
+    tx, ty, slots = (126, 32, 2 * sms) if order == 2 else (124, 16, 3 * sms)
+    rows = math.ceil(10 * slots / math.ceil(nx / tx))
+    shape = (1, (rows - 1) * ty + ty // 2 + 1, nx)   # last tile row partly filled
+    h = (0.9, 1.2, 1.0)
+    psi0 = uniform_ic(shape, 3 + order)
+    dt = {2: 0.004, 4: 0.002}[order]
+    rhs = gc.CahnHilliardRhs(0.8, 1.3, order)
+    g = grid_of(gc, shape, h)
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt, 2, gc.RK4)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.3, psi0, dt, 2, h=h))
+    t = dev(psi0)
+    gc.ch_integrate(t, g, rhs, dt, 1, gc.ExplicitEuler)
+    assert np.array_equal(host(t), oracle.ch_integrate(order, 0.8, 1.3, psi0, dt, 1, rk4=False, h=h))
 
 
 def test_2d_state_buffer_off_16_byte_boundary(gc, oracle):
