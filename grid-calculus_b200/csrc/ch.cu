@@ -166,26 +166,22 @@ struct TmaLayout {
   static constexpr int YX = TX + 4 * R, YY = TY + 4 * R;
   static constexpr int MX = kT2W, MY = TY + 2 * R;
   // k1, k2 of the last RK4 stage are read once per output cell, so they are
-  // fetched into registers rather than staged (keeps three CTAs per SM).
-  static constexpr bool K12 = false;
+  // fetched into registers rather than staged.
   static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
   static constexpr size_t YB = al(sizeof(T) * YX * YY);   // one y-region field
-  static constexpr size_t OB = al(sizeof(T) * TX * TY);   // one output-tile field
-  static constexpr size_t BUF = YB + (KIN ? YB : 0) + (K12 ? 2 * OB : 0);
+  static constexpr size_t BUF = YB + (KIN ? YB : 0);
   static constexpr size_t OFF_BUF = 128;                  // after the barriers
   // y = psi + a k_prev is formed in place in the k_prev buffer (no separate
   // y region), which keeps four CTAs per SM in double precision.
   static constexpr size_t OFF_MS = OFF_BUF + 2 * BUF;
   static constexpr size_t BYTES = OFF_MS + al(sizeof(T) * MX * MY) + 128;  // + alignment slack
-  static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(T) * YX * YY * (KIN ? 2 : 1) +
-                                                             (K12 ? 2 * sizeof(T) * TX * TY : 0));
+  static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(T) * YX * YY * (KIN ? 2 : 1));
 };
 
 template <class T, int ORDER, int MODE, bool KIN>
 __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
     const StageParams<T> p, const __grid_constant__ CUtensorMap m_psi, const __grid_constant__ CUtensorMap m_kin,
-    const __grid_constant__ CUtensorMap m_k1, const __grid_constant__ CUtensorMap m_k2, const int tiles_x,
-    const int tiles_y, int* status) {
+    const int tiles_x, const int tiles_y, int* status) {
   using L = TmaLayout<T, ORDER, MODE, KIN>;
   constexpr int R = L::R, TX = L::TX, TY = L::TY, YX = L::YX, YY = L::YY, MX = L::MX, MY = L::MY;
   constexpr int NW = 2 * R + 1;
@@ -197,8 +193,6 @@ __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
   int* s_abort = reinterpret_cast<int*>(base + 64);
   auto buf_psi = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF); };
   auto buf_kin = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + L::YB); };
-  auto buf_k1 = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + (KIN ? 2 : 1) * L::YB); };
-  auto buf_k2 = [&](int b) { return reinterpret_cast<T*>(base + L::OFF_BUF + b * L::BUF + (KIN ? 2 : 1) * L::YB + L::OB); };
   T* ms = reinterpret_cast<T*>(base + L::OFF_MS);
 
   const int nx = p.nx, ny = p.ny;
@@ -220,10 +214,6 @@ __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
       mbar_arrive_expect_tx(&bar[b], L::TX_BYTES);
       tma_load_2d(buf_psi(b), &m_psi, x0 - 2 * R, y0 - 2 * R, &bar[b]);
       if constexpr (KIN) tma_load_2d(buf_kin(b), &m_kin, x0 - 2 * R, y0 - 2 * R, &bar[b]);
-      if constexpr (L::K12) {
-        tma_load_2d(buf_k1(b), &m_k1, x0, y0, &bar[b]);
-        tma_load_2d(buf_k2(b), &m_k2, x0, y0, &bar[b]);
-      }
     } else {
       mbar_arrive(&bar[b]);
     }
@@ -267,24 +257,13 @@ __global__ void __launch_bounds__(kTmaThreads) ch_tma_kernel(
     }
     T* ps = buf_psi(b);
     if (!interior(x0, y0)) {
-      // Wrapped y region (and output tile) with ordinary loads.
+      // Wrapped y region with ordinary loads.
       T* ks = buf_kin(b);
       for (int e = tid; e < YX * YY; e += kTmaThreads) {
         const int r = e / YX, cc = e - r * YX;
         const size_t gi = static_cast<size_t>(wrap(y0 - 2 * R + r, ny)) * nx + wrap(x0 - 2 * R + cc, nx);
         ps[e] = p.psi[gi];
         if constexpr (KIN) ks[e] = p.kin[gi];
-      }
-      if constexpr (L::K12) {
-        T* a1 = buf_k1(b);
-        T* a2 = buf_k2(b);
-        for (int e = tid; e < TX * TY; e += kTmaThreads) {
-          const int r = e / TX, cc = e - r * TX;
-          const bool in = x0 + cc < nx && y0 + r < ny;
-          const size_t gi = in ? static_cast<size_t>(y0 + r) * nx + (x0 + cc) : 0;
-          a1[e] = in ? p.k1[gi] : T(0);
-          a2[e] = in ? p.k2[gi] : T(0);
-        }
       }
     }
     __syncthreads();
@@ -387,14 +366,10 @@ template <class T, int ORDER, int MODE, bool KIN>
 gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
   using L = TmaLayout<T, ORDER, MODE, KIN>;
   if (p.nx < L::YX || p.ny < L::YY) return GC_ERR_UNSUPPORTED;
-  CUtensorMap mpsi{}, mkin{}, mk1{}, mk2{};
+  CUtensorMap mpsi{}, mkin{};
   const int eb = static_cast<int>(sizeof(T));
   if (!make_tensor_map_2d(&mpsi, p.psi, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
   if (KIN && !make_tensor_map_2d(&mkin, p.kin, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
-  if (L::K12) {
-    if (!make_tensor_map_2d(&mk1, p.k1, p.nx, p.ny, eb, L::TX, L::TY)) return GC_ERR_UNSUPPORTED;
-    if (!make_tensor_map_2d(&mk2, p.k2, p.nx, p.ny, eb, L::TX, L::TY)) return GC_ERR_UNSUPPORTED;
-  }
   auto kern = ch_tma_kernel<T, ORDER, MODE, KIN>;
   static int ctas_per_sm = 0;  // one instantiation per template argument set
   if (ctas_per_sm == 0) {
@@ -405,8 +380,7 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
   const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
   const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
   const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
-  kern<<<grid, dim3(kT2W, kT2TY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, mk1, mk2, tiles_x, tiles_y,
-                                                           ctx->device_status);
+  kern<<<grid, dim3(kT2W, kT2TY), L::BYTES, ctx->stream>>>(p, mpsi, mkin, tiles_x, tiles_y, ctx->device_status);
   GC_CHECK_LAUNCH("ch_tma_kernel");
   return GC_OK;
 }
