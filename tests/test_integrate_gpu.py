@@ -90,6 +90,30 @@ def test_energies_bit_exact_golden(gc):
         assert gc.evaluate(t, g, "psi") / vol_total == float(golden[f"{name}/mean"])
 
 
+def test_fixed_integrands_psi_squared_and_float(gc, oracle):
+    """The remaining hot-path integrands of func::evaluate: psi^2
+    (heterogeneous_diffusion.hpp:82) is the pairwise integral of the rounded
+    squares; float fields are promoted to double per cell, so 'psi' and
+    'psi_squared' on a float field are the oracle's values on the promoted
+    values; the Kahan tag agrees to a few ulps and is deterministic."""
+    import torch
+    rng = np.random.default_rng(23)
+    shape, h = (7, 33, 65), (0.5, 0.25, 2.0)
+    f = rng.standard_normal(shape)
+    g = gc.Grid(shape[2], shape[1], shape[0], *h)
+    assert gc.evaluate(dev(f), g, "psi_squared") == oracle.integrate(f * f, h)
+    f32 = f.astype(np.float32)
+    p32 = f32.astype(np.float64)
+    t32 = dev(f32, torch.float32)
+    assert gc.evaluate(t32, g, "psi") == oracle.integrate(p32, h)
+    assert gc.evaluate(t32, g, "psi_squared") == oracle.integrate(p32 * p32, h)
+    for name in ("psi_squared", "ch_free_energy", "grad_squared"):
+        a = gc.evaluate(dev(f), g, name, kappa=0.6, tag=gc.Kahan)
+        b = gc.evaluate(dev(f), g, name, kappa=0.6)
+        assert a == gc.evaluate(dev(f), g, name, kappa=0.6, tag=gc.Kahan)
+        assert abs(a - b) <= 1e-13 * abs(b), name
+
+
 def test_energies_bit_exact_large(gc, oracle):
     rng = np.random.default_rng(21)
     f = 0.3 * rng.standard_normal((1, 512, 384))
