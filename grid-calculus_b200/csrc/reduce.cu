@@ -273,13 +273,6 @@ gc_program fixed_program(int kind, double kappa) {
     f.instr[f.n_instr++] = gc_instr{static_cast<int16_t>(code), static_cast<int16_t>(dst), static_cast<int16_t>(a),
                                     static_cast<int16_t>(b), v};
   };
-  auto grad_squared = [&](int into) {  // registers 1..3 hold the gradient; result in `into`
-    op(GC_OPC_MUL, 1, 1, 1);
-    op(GC_OPC_MUL, 2, 2, 2);
-    op(GC_OPC_ADD, 1, 1, 2);
-    op(GC_OPC_MUL, 3, 3, 3);
-    op(GC_OPC_ADD, into, 1, 3);
-  };
   switch (kind) {
     case GC_INTEGRAND_PSI:
       f.arity = 1;
@@ -290,12 +283,16 @@ gc_program fixed_program(int kind, double kappa) {
       op(GC_OPC_INPUT, 0, GC_IN_PSI, 0);
       op(GC_OPC_MUL, 0, 0, 0);
       break;
-    case GC_INTEGRAND_GRAD_SQUARED:
+    case GC_INTEGRAND_GRAD_SQUARED:  // (gx gx + gy gy) + gz gz in r0..r2, as the recorder lays it out
       f.arity = 2;
-      op(GC_OPC_INPUT, 1, GC_IN_GRAD_X, 0);
-      op(GC_OPC_INPUT, 2, GC_IN_GRAD_Y, 0);
-      op(GC_OPC_INPUT, 3, GC_IN_GRAD_Z, 0);
-      grad_squared(0);
+      op(GC_OPC_INPUT, 0, GC_IN_GRAD_X, 0);
+      op(GC_OPC_INPUT, 1, GC_IN_GRAD_Y, 0);
+      op(GC_OPC_INPUT, 2, GC_IN_GRAD_Z, 0);
+      op(GC_OPC_MUL, 0, 0, 0);
+      op(GC_OPC_MUL, 1, 1, 1);
+      op(GC_OPC_ADD, 1, 0, 1);
+      op(GC_OPC_MUL, 2, 2, 2);
+      op(GC_OPC_ADD, 2, 1, 2);
       break;
     default:  // GC_INTEGRAND_CH_FREE_ENERGY
       f.arity = 2;
@@ -309,7 +306,11 @@ gc_program fixed_program(int kind, double kappa) {
       op(GC_OPC_CONST, 5, 0, 0, 0.25);
       for (int q = 0; q < 4; ++q) op(GC_OPC_MUL, 5, 5, 0);
       op(GC_OPC_ADD, 5, 4, 5);
-      grad_squared(3);
+      op(GC_OPC_MUL, 1, 1, 1);  // |grad psi|^2 = (gx gx + gy gy) + gz gz into r3
+      op(GC_OPC_MUL, 2, 2, 2);
+      op(GC_OPC_ADD, 1, 1, 2);
+      op(GC_OPC_MUL, 3, 3, 3);
+      op(GC_OPC_ADD, 3, 1, 3);
       op(GC_OPC_CONST, 1, 0, 0, 0.5 * kappa);
       op(GC_OPC_MUL, 1, 1, 3);
       op(GC_OPC_ADD, 5, 5, 1);
@@ -391,6 +392,14 @@ GC_API gc_status gc_check_finite(gc_context* ctx, const gc_grid* g, gc_dtype dt,
   return fail(GC_ERR_NONFINITE, "gc_check_finite: non-finite value " + std::to_string(v) + " at flat index " +
                                     std::to_string(first) + " (component " + std::to_string(first / nc) + ", cell (" +
                                     std::to_string(i) + ", " + std::to_string(j) + ", " + std::to_string(k) + "))");
+}
+
+GC_API gc_status gc_integrand_program(const gc_integrand* f, gc_program* out) {
+  if (!f || !out) return fail(GC_ERR_INVALID_ARG, "gc_integrand_program: null pointer");
+  if (f->kind < GC_INTEGRAND_PSI || f->kind > GC_INTEGRAND_GRAD_SQUARED)
+    return fail(GC_ERR_INVALID_ARG, "gc_integrand_program: unknown integrand kind");
+  *out = fixed_program(f->kind, f->kappa);
+  return GC_OK;
 }
 
 GC_API gc_status gc_evaluate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* psi,

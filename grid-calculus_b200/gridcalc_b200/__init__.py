@@ -28,7 +28,7 @@ __all__ = [
     "laplacian", "gradient", "divergence", "biharmonic", "d4", "cell_laplacian",
     "integrate", "evaluate", "ch_rhs", "ch_integrate", "diffuse", "diffuse_fvm",
     "d_max_face", "version", "ChBatch", "Corrector", "corrector_init_params", "ch_rkc",
-    "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct",
+    "rkc_stability_bound", "partial", "PARTIALS", "sqrt", "minimum", "maximum", "program_struct", "integrand_program",
     "write_vtk", "save_checkpoint", "checkpoint_info", "load_checkpoint", "Snapshotter",
     "spectral_partial", "spectral_laplacian", "spectral_biharmonic", "spectral_gradient", "check_finite",
 ]
@@ -411,6 +411,19 @@ class gc_program(C.Structure):
 
 lib.gc_evaluate_program.argtypes = [_vp, _gp, _i32, _vp, C.POINTER(gc_program), _i32, C.POINTER(C.c_double)]
 lib.gc_evaluate_program.restype = C.c_int
+
+
+lib.gc_integrand_program.argtypes = [C.POINTER(gc_integrand), C.POINTER(gc_program)]
+lib.gc_integrand_program.restype = C.c_int
+
+
+def integrand_program(name: str, kappa: float = 0.0) -> "_integrand.Program":
+    """The program evaluate(field, grid, name) runs for a named hot-path
+    integrand, as an integrand.Program (no GPU work)."""
+    out = gc_program()
+    _check(lib.gc_integrand_program(C.byref(gc_integrand(INTEGRANDS[name], kappa)), C.byref(out)))
+    rows = [(int(i.op), int(i.dst), int(i.a), int(i.b), float(i.value)) for i in out.instr[:out.n_instr]]
+    return _integrand.Program(out.components, out.arity, rows)
 
 
 def program_struct(prog: "_integrand.Program") -> gc_program:

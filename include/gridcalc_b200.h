@@ -252,6 +252,10 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
  * buf and returns the full size including the NUL (0 for a malformed
  * program).  Each distinct source is compiled once per process and device. */
 GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap);
+/* The program gc_evaluate runs for a named integrand (the reference
+ * expression's operations in its order; kappa enters as the constant
+ * 0.5 * kappa).  No counterpart in the reference; no GPU work. */
+GC_API gc_status gc_integrand_program(const gc_integrand* f, gc_program* out);
 
 /* Non-finite detection (no counterpart in the reference, which has no such
  * check): scans `components` planes of a device field for a NaN or an

@@ -173,3 +173,29 @@ def test_generated_sources_compile_for_sm100a():
     bad = gc.gc_program(1, 1, 1, 0)
     bad.instr[0] = gc.gc_instr(2, 0, 0, 0, 0.0)   # reads a register never written
     assert gc.lib.gc_program_source(C.byref(bad), gc.F64, None, 0) == 0
+
+
+def test_named_integrands_are_the_reference_expressions(oracle, golden):
+    """gc_evaluate runs its named integrands as built-in programs
+    (gc_integrand_program).  They are instruction for instruction what the
+    recorder makes of the reference's expressions (cahn_hilliard.hpp:64-77,
+    heterogeneous_diffusion.hpp:82), and the oracle running them gives the
+    reference's golden energies; no GPU is needed."""
+    import gridcalc_b200 as gc
+    for kappa in (0.8, 1.0, 0.35):
+        assert gc.integrand_program("ch_free_energy", kappa).instr == I.trace(
+            lambda p, g: -0.5 * p * p + 0.25 * p * p * p * p + (0.5 * kappa) * g.squaredNorm()).instr
+    assert gc.integrand_program("grad_squared").instr == I.trace(lambda p, g: g.squaredNorm()).instr
+    assert gc.integrand_program("psi_squared").instr == I.trace(lambda p: p * p).instr
+    assert gc.integrand_program("psi").instr == I.trace(lambda p: p).instr
+    for g in ("aniso3d", "cube7"):
+        f, h = golden[f"{g}/f"], tuple(golden[f"{g}/h"])
+        fe = gc.integrand_program("ch_free_energy", 0.8)
+        assert oracle.evaluate_program(1, fe.arity, fe.instr, f, h) == float(golden[f"{g}/free_energy"])
+        ge = gc.integrand_program("grad_squared")
+        assert oracle.evaluate_program(1, ge.arity, ge.instr, f, h) == float(golden[f"{g}/gradient_energy"])
+    with pytest.raises(KeyError):
+        gc.integrand_program("elastic")
+    bad = gc.gc_program()
+    assert gc.STATUS[gc.lib.gc_integrand_program(gc.C.byref(gc.gc_integrand(7, 0.0)), gc.C.byref(bad))] == \
+        "GC_ERR_INVALID_ARG"
