@@ -40,3 +40,50 @@ def rows(prog):
     """The program as an (n, 5) array of (op, dst, a, b, value)."""
     import numpy as np
     return np.array(prog.instr, dtype=np.float64).reshape(-1, 5)
+
+
+# --- random expression trees for the property tests ---------------------------
+_UNARY = ("neg", "abs", "sqrt")
+_BINARY = ("add", "sub", "mul", "div", "min", "max")
+
+
+def random_tree(n_inputs):
+    """A hypothesis strategy: expression trees over inputs 0..n_inputs-1 and
+    non-zero constants, with every unary and binary opcode."""
+    from hypothesis import strategies as st
+    leaf = st.one_of(st.tuples(st.just("in"), st.integers(0, n_inputs - 1)),
+                     st.tuples(st.just("c"), st.floats(-4.0, 4.0, allow_nan=False).filter(lambda v: v != 0.0)))
+    return st.recursive(leaf, lambda kids: st.one_of(
+        st.tuples(st.sampled_from(_UNARY), kids),
+        st.tuples(st.sampled_from(_BINARY), kids, kids)), max_leaves=12)
+
+
+def eval_tree(node, ins):
+    """The expression over scalars, Sym values or arrays alike: the same
+    Python callable is recorded and run directly."""
+    kind = node[0]
+    if kind == "in":
+        return ins[node[1]]
+    if kind == "c":
+        return node[1]
+    a = eval_tree(node[1], ins)
+    if kind == "neg":
+        return -a
+    if kind == "abs":
+        return abs(a)
+    if kind == "sqrt":
+        return sqrt(abs(a))
+    b = eval_tree(node[2], ins)
+    return {"add": lambda: a + b, "sub": lambda: a - b, "mul": lambda: a * b, "div": lambda: a / b,
+            "min": lambda: minimum(a, b), "max": lambda: maximum(a, b)}[kind]()
+
+
+def tree_callable(tree, arity):
+    """The tree as a callable of the given arity (psi, grad, lap, bih)."""
+    if arity == 1:
+        return lambda p: eval_tree(tree, [p])
+    if arity == 2:
+        return lambda p, g: eval_tree(tree, [p, g[0], g[1], g[2]])
+    if arity == 3:
+        return lambda p, g, lap: eval_tree(tree, [p, g[0], g[1], g[2], lap])
+    return lambda p, g, lap, bih: eval_tree(tree, [p, g[0], g[1], g[2], lap, bih])

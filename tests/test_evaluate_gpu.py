@@ -152,3 +152,29 @@ def test_non_finite_values_propagate_like_the_reference(gc, oracle):
     got = gc.evaluate(_dev(f), g, grad_only)
     assert math.isnan(want) and math.isnan(got)
     assert gc.evaluate(_dev(f), g, lambda p: p) == oracle.evaluate_program(1, 1, IC.integrand.trace(lambda p: p).instr, f, h) == math.inf
+
+
+from hypothesis import HealthCheck, assume, given, settings  # noqa: E402
+from hypothesis import strategies as st  # noqa: E402
+
+
+@settings(max_examples=20, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(data=st.data(), arity=st.integers(1, 4))
+def test_random_integrands_bit_exact_vs_oracle(gc, oracle, data, arity):
+    """Random expressions over every opcode and input (each a new NVRTC
+    compile): the device result is the oracle's, bit for bit, non-finite
+    field values included."""
+    tree = data.draw(IC.random_tree({1: 1, 2: 4, 3: 5, 4: 6}[arity]))
+    fn = IC.tree_callable(tree, arity)
+    try:
+        prog = IC.integrand.trace(fn)
+    except (ZeroDivisionError, ValueError):
+        assume(False)
+    rng = np.random.default_rng(len(prog.instr) + 17 * arity)
+    shape, h = (9, 11, 13), (0.5, 0.75, 1.25)
+    field = rng.standard_normal(shape)
+    if data.draw(st.integers(0, 4)) == 0:
+        field[4, 5, 6] = data.draw(st.sampled_from([np.inf, -np.inf, np.nan]))
+    want = oracle.evaluate_program(1, prog.arity, prog.instr, field, h)
+    got = gc.evaluate(_dev(field), _grid(gc, shape, h), prog)
+    assert got == want or (np.isnan(got) and np.isnan(want)), (prog.instr, got, want)

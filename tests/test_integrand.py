@@ -199,3 +199,43 @@ def test_named_integrands_are_the_reference_expressions(oracle, golden):
     bad = gc.gc_program()
     assert gc.STATUS[gc.lib.gc_integrand_program(gc.C.byref(gc.gc_integrand(7, 0.0)), gc.C.byref(bad))] == \
         "GC_ERR_INVALID_ARG"
+
+
+# --- random integrands (property test) --------------------------------------
+from hypothesis import HealthCheck, assume, given, settings  # noqa: E402
+from hypothesis import strategies as st  # noqa: E402
+
+
+@settings(max_examples=250, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(data=st.data(), arity=st.integers(1, 4))
+def test_random_integrands_record_exactly(oracle, data, arity):
+    """Random expressions over every opcode and every input of the arity:
+    the recorded program computes exactly what the Python callable computes
+    on the same arrays (bit for bit, non-finite values included), and the
+    oracle's func::evaluate of the program is the integral of those values."""
+    n_inputs = {1: 1, 2: 4, 3: 5, 4: 6}[arity]
+    tree = data.draw(IC.random_tree(n_inputs))
+    fn = IC.tree_callable(tree, arity)
+    try:
+        prog = I.trace(fn)
+    except (ZeroDivisionError, ValueError):   # a constant subexpression divides by zero / too large
+        assume(False)
+    rng = np.random.default_rng(len(prog.instr))
+    shape, h = (5, 6, 7), (0.5, 0.75, 1.25)
+    field = rng.standard_normal(shape)
+    if data.draw(st.integers(0, 4)) == 0:
+        field[2, 3, 4] = data.draw(st.sampled_from([np.inf, -np.inf, np.nan]))
+    ins = [field]
+    if arity >= 2:
+        ins += list(oracle.op("gradient", 2, field, h))
+    if arity >= 3:
+        ins.append(oracle.op("laplacian", 2, field, h))
+    if arity >= 4:
+        ins.append(oracle.op("biharmonic", 2, field, h))
+    with np.errstate(all="ignore"):
+        direct = np.asarray(fn(*([ins[0], I.SymVec3(ins[1:4]), *(ins[4:])][:arity])), dtype=np.float64) * np.ones(shape)
+        via = np.asarray(I.interpret(prog, ins), dtype=np.float64) * np.ones(shape)
+    assert np.array_equal(direct.view(np.uint64), via.view(np.uint64))
+    got = oracle.evaluate_program(1, prog.arity, prog.instr, field, h)
+    want = oracle.integrate(direct, h)
+    assert got == want or (np.isnan(got) and np.isnan(want))
