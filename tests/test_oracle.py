@@ -191,3 +191,69 @@ def test_order6_convergence_slope(oracle, op, expect):
         errs.append(np.abs(got - ref).max())
     slope = math.log(errs[0] / errs[1]) / math.log(ns[1] / ns[0])
     assert abs(slope - expect) < 0.5, (errs, slope)
+
+
+# --- 2b. live reference, random cases -----------------------------------------
+from hypothesis import HealthCheck, given, settings  # noqa: E402
+from hypothesis import strategies as st  # noqa: E402
+
+_AXIS = st.one_of(st.just(1), st.integers(7, 11))   # valid for every stencil radius up to 3
+_H = st.floats(0.3, 2.0, allow_nan=False)
+_OPS = ["laplacian", "gradient", "divergence", "biharmonic", "gradient_vec", "divergence_mat", "mixed",
+        "cell_laplacian", "ch_rhs", "ch_rk4", "ch_euler", "diffuse_const", "diffuse_fvm", "integrate"]
+
+
+@pytest.mark.skipif(not oracle_lib.reference_available(), reason="reference build (oracle/_ref) absent")
+@settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(data=st.data(), name=st.sampled_from(_OPS), order=st.sampled_from([2, 4]))
+def test_oracle_matches_live_reference_random(oracle, data, name, order):
+    """Random grids (degenerate and regular axes), spacings, orders and
+    coefficients: every path function of the oracle gives the reference's
+    own result (compiled from its headers) bit for bit."""
+    ref = oracle_lib.reference()
+    shape = (data.draw(_AXIS), data.draw(_AXIS), data.draw(_AXIS))
+    h = (data.draw(_H), data.draw(_H), data.draw(_H))
+    rng = np.random.default_rng(data.draw(st.integers(0, 2 ** 32 - 1)))
+    f = rng.standard_normal(shape)
+
+    def same(a, b):
+        assert np.array_equal(a, b, equal_nan=True), (name, order, shape, h)
+
+    if name in ("laplacian", "gradient", "biharmonic"):
+        same(oracle.op(name, order, f, h), ref.op(name, order, f, h))
+    elif name in ("divergence", "gradient_vec"):
+        v = rng.standard_normal((3,) + shape)
+        same(oracle.op(name, order, v, h), ref.op(name, order, v, h))
+    elif name == "divergence_mat":
+        m = rng.standard_normal((3, 3) + shape)
+        same(oracle.op(name, order, m, h), ref.op(name, order, m, h))
+    elif name == "mixed":
+        counts = data.draw(st.tuples(st.integers(0, 4), st.integers(0, 4), st.integers(0, 4))
+                           .filter(lambda c: 2 <= sum(c) <= 4))
+        same(oracle.mixed(counts, order, f, h), ref.mixed(counts, order, f, h))
+    elif name == "cell_laplacian":
+        D = np.exp(rng.standard_normal(shape))
+        same(oracle.cell_laplacian(f, D, h), ref.cell_laplacian(f, D, h))
+    elif name == "ch_rhs":
+        M, kappa = data.draw(_H), data.draw(_H)
+        same(oracle.ch_rhs(order, M, kappa, 0.1 * f, h), ref.ch_rhs(order, M, kappa, 0.1 * f, h))
+    elif name in ("ch_rk4", "ch_euler"):
+        M, kappa = data.draw(_H), data.draw(_H)
+        dt = 1e-3 * min(h) ** 4
+        rk4 = name == "ch_rk4"
+        same(oracle.ch_integrate(order, M, kappa, 0.1 * f, dt, 3, rk4=rk4, h=h),
+             ref.ch_integrate(order, M, kappa, 0.1 * f, dt, 3, rk4=rk4, h=h))
+    elif name == "diffuse_const":
+        D = data.draw(_H)
+        dt = 0.05 * min(h) ** 2 / D
+        rk4 = data.draw(st.booleans())
+        same(oracle.diffuse_const(f, D, dt, 3, rk4=rk4, h=h), ref.diffuse_const(f, D, dt, 3, rk4=rk4, h=h))
+    elif name == "diffuse_fvm":
+        D = np.exp(0.5 * rng.standard_normal(shape))
+        dt = 0.05 * min(h) ** 2 / float(D.max())
+        rk4 = data.draw(st.booleans())
+        same(oracle.diffuse_fvm(f, D, dt, 3, rk4=rk4, h=h), ref.diffuse_fvm(f, D, dt, 3, rk4=rk4, h=h))
+    else:
+        x = rng.standard_normal(data.draw(st.integers(1, 5000))).reshape(1, 1, -1)
+        assert oracle.integrate(x, h) == ref.integrate(x, h)
+        assert oracle.integrate(x, h, kahan=True) == ref.integrate(x, h, kahan=True)
