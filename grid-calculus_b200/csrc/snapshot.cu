@@ -5,7 +5,7 @@
 //   ASCII form (17 significant digits, i fastest), plus a BINARY form of the
 //   same header with big-endian doubles.
 // * Checkpoints: a fixed little-endian header (magic, version, dtype, grid,
-//   components, sizes, a 64-bit checksum of the data), a JSON metadata
+//   components, sizes, a 64-bit checksum of the whole file), a JSON metadata
 //   string, then the raw field planes.  Loading one and continuing a
 //   trajectory gives the bit-identical state of an uninterrupted run.
 // * gc_snapshotter: snapshots of device fields that do not stall the
@@ -31,7 +31,9 @@ namespace gcb {
 namespace {
 
 constexpr char kCkptMagic[8] = {'G', 'C', 'B', '2', '0', '0', 'C', 'K'};
-constexpr uint32_t kCkptVersion = 1;
+// Version 2: the checksum covers the header, the metadata and the data.
+// Version 1 files (checksum of the data only) are still read.
+constexpr uint32_t kCkptVersion = 2;
 
 struct CkptHeader {
   char magic[8];
@@ -66,6 +68,18 @@ uint64_t checksum64(const void* data, uint64_t bytes) {
   h ^= h >> 33;
   h *= 0xC4CEB9FE1A85EC53ull;
   return h ^ (h >> 29);
+}
+
+// Checksum of a version-2 file: the header with its checksum field zero,
+// the metadata and the data are each hashed and the three hashes hashed
+// together, so a changed bit anywhere in the file fails the check (every
+// step of checksum64 is a bijection of its state for a given length).
+uint64_t file_checksum(const CkptHeader& h, const std::string& meta, const void* data) {
+  CkptHeader z = h;
+  z.checksum = 0;
+  const uint64_t parts[3] = {checksum64(&z, sizeof z), checksum64(meta.data(), meta.size()),
+                             checksum64(data, h.data_bytes)};
+  return checksum64(parts, sizeof parts);
 }
 
 std::string g17(double v) {
@@ -154,7 +168,7 @@ gc_status write_ckpt_file(const gc_grid* g, gc_dtype dt, int comps, const void* 
   h.hx = g->hx; h.hy = g->hy; h.hz = g->hz;
   h.data_bytes = static_cast<uint64_t>(cells(g)) * comps * dtype_size(dt);
   h.meta_len = meta.size();
-  h.checksum = checksum64(host, h.data_bytes);
+  h.checksum = file_checksum(h, meta, host);
   // Written to a temporary name and renamed, so a crash never leaves a
   // truncated file under the final name.
   const std::string tmp = path + ".part";
@@ -174,7 +188,7 @@ gc_status write_ckpt_file(const gc_grid* g, gc_dtype dt, int comps, const void* 
 gc_status read_ckpt_header(std::FILE* in, const std::string& path, CkptHeader* h) {
   if (std::fread(h, sizeof *h, 1, in) != 1 || std::memcmp(h->magic, kCkptMagic, 8) != 0)
     return fail(GC_ERR_IO, "checkpoint: '" + path + "' is not a gridcalc_b200 checkpoint");
-  if (h->version != kCkptVersion)
+  if (h->version != 1 && h->version != kCkptVersion)
     return fail(GC_ERR_UNSUPPORTED, "checkpoint: '" + path + "' has version " + std::to_string(h->version));
   if ((h->dtype != GC_F64 && h->dtype != GC_F32) || h->nx <= 0 || h->ny <= 0 || h->nz <= 0 || h->components <= 0 ||
       h->data_bytes != static_cast<uint64_t>(h->nx) * h->ny * h->nz * h->components * (h->dtype == GC_F64 ? 8 : 4))
@@ -186,20 +200,21 @@ gc_status read_ckpt(const std::string& path, CkptHeader* h, std::string* meta, v
   std::FILE* in = std::fopen(path.c_str(), "rb");
   if (!in) return fail(GC_ERR_IO, "checkpoint: cannot open '" + path + "'");
   gc_status s = read_ckpt_header(in, path, h);
-  if (s == GC_OK && meta) {
-    meta->assign(static_cast<size_t>(h->meta_len), '\0');
-    if (h->meta_len && std::fread(&(*meta)[0], 1, static_cast<size_t>(h->meta_len), in) != h->meta_len)
+  // The metadata is read whenever the data is (a version-2 checksum covers it).
+  std::string local;
+  std::string* m = meta ? meta : (host ? &local : nullptr);
+  if (s == GC_OK && m) {
+    m->assign(static_cast<size_t>(h->meta_len), '\0');
+    if (h->meta_len && std::fread(&(*m)[0], 1, static_cast<size_t>(h->meta_len), in) != h->meta_len)
       s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
   }
   if (s == GC_OK && host) {
     if (host_bytes < h->data_bytes) {
       s = fail(GC_ERR_INVALID_ARG, "checkpoint: buffer of " + std::to_string(host_bytes) + " bytes, field has " +
                                        std::to_string(h->data_bytes));
-    } else if (!meta && std::fseek(in, static_cast<long>(sizeof *h + h->meta_len), SEEK_SET) != 0) {
-      s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
     } else if (h->data_bytes && std::fread(host, 1, h->data_bytes, in) != h->data_bytes) {
       s = fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
-    } else if (checksum64(host, h->data_bytes) != h->checksum) {
+    } else if ((h->version == 1 ? checksum64(host, h->data_bytes) : file_checksum(*h, *m, host)) != h->checksum) {
       s = fail(GC_ERR_IO, "checkpoint: '" + path + "' fails its checksum");
     }
   }

@@ -85,6 +85,7 @@ def test_checkpoint_round_trip(gcm, tmp_path, dtype, comps):
     assert meta2 == meta and grid2 == g
     raw = open(path, "rb").read()
     assert raw[:8] == b"GCB200CK" and len(raw) == 80 + mlen + f.nbytes
+    assert struct.unpack_from("<I", raw, 8) == (2,)          # version 2: whole-file checksum
     assert struct.unpack_from("<4i", raw, 16) == (9, 8, 7, comps)
     assert json.loads(raw[80:80 + mlen].decode()) == meta
     assert not os.path.exists(path + ".part")
@@ -116,3 +117,74 @@ def test_checkpoint_integrity_checks(gcm, tmp_path):
         gcm.checkpoint_info(str(tmp_path / "hdr.gcb"))
     with pytest.raises(ValueError, match="cannot open"):
         gcm.checkpoint_info(str(tmp_path / "missing.gcb"))
+
+
+# --- checkpoint integrity, random cases ----------------------------------------
+from hypothesis import HealthCheck, given, settings  # noqa: E402
+from hypothesis import strategies as st  # noqa: E402
+
+_M64 = (1 << 64) - 1
+
+
+def _checksum64(data: bytes) -> int:
+    """The format's 64-bit multiply-rotate checksum, restated (test only)."""
+    h = 0x9E3779B97F4A7C15 ^ len(data)
+    for i in range(0, len(data), 8):
+        w = int.from_bytes(data[i:i + 8].ljust(8, b"\0"), "little")
+        h ^= (w * 0xFF51AFD7ED558CCD) & _M64
+        h = ((((h << 27) | (h >> 37)) & _M64) * 0x9E3779B97F4A7C15 + 0x52DCE729) & _M64
+    h ^= h >> 33
+    h = (h * 0xC4CEB9FE1A85EC53) & _M64
+    return h ^ (h >> 29)
+
+
+_META = st.dictionaries(st.text(min_size=1, max_size=8), st.one_of(
+    st.integers(-10 ** 12, 10 ** 12), st.floats(allow_nan=False, allow_infinity=False), st.text(max_size=12)),
+    max_size=4)
+
+
+@settings(max_examples=80, deadline=None, suppress_health_check=[HealthCheck.too_slow,
+                                                                   HealthCheck.function_scoped_fixture])
+@given(data=st.data(), dtype=st.sampled_from([np.float64, np.float32]), comps=st.sampled_from([1, 3]),
+       meta=_META)
+def test_checkpoint_random_round_trip_and_any_bit_flip(gcm, tmp_path, data, dtype, comps, meta):
+    """Any grid, dtype, component count and JSON metadata round-trips
+    exactly; a single flipped bit anywhere in the file (header, metadata or
+    data) makes the load fail instead of returning altered values."""
+    n = [data.draw(st.integers(1, 6)) for _ in range(3)]
+    h = [data.draw(st.floats(1e-3, 1e3)) for _ in range(3)]
+    g = gcm.Grid(n[0], n[1], n[2], *h)
+    shape = g.shape if comps == 1 else (comps,) + g.shape
+    f = np.random.default_rng(sum(n)).standard_normal(shape).astype(dtype)
+    path = str(tmp_path / "r.gcb")
+    gcm.save_checkpoint(f, g, path, meta)
+    back, g2, m2 = gcm.load_checkpoint(path)
+    assert np.array_equal(back, f) and g2 == g and m2 == meta
+    raw = bytearray(open(path, "rb").read())
+    bit = data.draw(st.integers(0, 8 * len(raw) - 1))
+    raw[bit // 8] ^= 1 << (bit % 8)
+    bad = tmp_path / "flipped.gcb"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(ValueError):
+        gcm.load_checkpoint(str(bad))
+
+
+def test_checkpoint_version_1_still_read(gcm, tmp_path):
+    """A version-1 file (its checksum covers the data only) loads unchanged."""
+    g = gcm.Grid(5, 4, 3, 0.5, 0.25, 2.0)
+    f = np.random.default_rng(3).standard_normal(g.shape)
+    path = tmp_path / "v2.gcb"
+    gcm.save_checkpoint(f, g, str(path), {"step": 7})
+    raw = bytearray(path.read_bytes())
+    mlen = struct.unpack_from("<Q", raw, 64)[0]
+    struct.pack_into("<I", raw, 8, 1)
+    struct.pack_into("<Q", raw, 72, _checksum64(bytes(raw[80 + mlen:])))
+    old = tmp_path / "v1.gcb"
+    old.write_bytes(bytes(raw))
+    back, g2, meta = gcm.load_checkpoint(str(old))
+    assert np.array_equal(back, f) and g2 == g and meta == {"step": 7}
+    raw[-1] ^= 0x80                           # its data checksum still guards the data
+    old.write_bytes(bytes(raw))
+    with pytest.raises(ValueError, match="checksum"):
+        gcm.load_checkpoint(str(old))
+
