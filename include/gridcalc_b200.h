@@ -442,10 +442,11 @@ GC_API gc_status gc_write_vtk(const gc_grid* g, gc_dtype dt, const void* host, c
                               const char* field_name, gc_vtk_encoding enc);
 
 /* Checkpoint file: an 80-byte little-endian header (magic "GCB200CK",
- * version 1, dtype, nx ny nz, components, hx hy hz, data bytes, metadata
- * bytes, 64-bit checksum of the data), the metadata (e.g. JSON: step, time,
- * parameters), then `components` planes of the field, i fastest.  Written
- * under a temporary name and renamed.  Needs no device. */
+ * version 2, dtype, nx ny nz, components, hx hy hz, data bytes, metadata
+ * bytes, 64-bit checksum of the header, the metadata and the data), the
+ * metadata (e.g. JSON: step, time, parameters), then `components` planes of
+ * the field, i fastest.  Written under a temporary name and renamed.  Version
+ * 1 files (checksum of the data only) are read as well.  Needs no device. */
 GC_API gc_status gc_write_checkpoint(const gc_grid* g, gc_dtype dt, int32_t components, const void* host,
                                      const char* path, const char* meta_json);
 /* The header of a checkpoint: grid, dtype, components and metadata length. */
