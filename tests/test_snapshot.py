@@ -8,6 +8,8 @@ import struct
 
 import numpy as np
 import pytest
+from hypothesis import HealthCheck, given, settings
+from hypothesis import strategies as st
 
 import oracle_lib
 
@@ -41,6 +43,26 @@ def test_vtk_ascii_matches_live_reference(gcm, tmp_path):
         ref.write_vtk(f, str(tmp_path / "ref.vtk"), name, h)
         gcm.write_vtk(f, gcm.Grid(shape[2], shape[1], shape[0], *h), str(tmp_path / "ours.vtk"), name)
         assert (tmp_path / "ours.vtk").read_bytes() == (tmp_path / "ref.vtk").read_bytes()
+
+
+@pytest.mark.skipif(not oracle_lib.reference_available(), reason="reference build (oracle/_ref) absent")
+@settings(max_examples=200, deadline=None, suppress_health_check=[HealthCheck.too_slow,
+                                                                   HealthCheck.function_scoped_fixture])
+@given(data=st.data())
+def test_vtk_ascii_matches_live_reference_random(gcm, tmp_path, data):
+    """Any double (signed zeros, subnormals, infinities, NaNs of either sign,
+    extreme exponents), any spacing and field name: the same bytes as the
+    reference writer."""
+    ref = oracle_lib.reference()
+    shape = tuple(data.draw(st.integers(1, 5)) for _ in range(3))
+    h = tuple(data.draw(st.floats(1e-9, 1e9)) for _ in range(3))
+    name = data.draw(st.text(alphabet="abcdefghijklmnopqrstuvwxyz_0123456789", min_size=1, max_size=10))
+    vals = data.draw(st.lists(st.floats(allow_nan=True, allow_infinity=True, width=64),
+                              min_size=int(np.prod(shape)), max_size=int(np.prod(shape))))
+    f = np.array(vals, dtype=np.float64).reshape(shape)
+    ref.write_vtk(f, str(tmp_path / "ref.vtk"), name, h)
+    gcm.write_vtk(f, gcm.Grid(shape[2], shape[1], shape[0], *h), str(tmp_path / "ours.vtk"), name)
+    assert (tmp_path / "ours.vtk").read_bytes() == (tmp_path / "ref.vtk").read_bytes()
 
 
 def test_vtk_binary_and_float_fields(gcm, tmp_path):
@@ -120,8 +142,6 @@ def test_checkpoint_integrity_checks(gcm, tmp_path):
 
 
 # --- checkpoint integrity, random cases ----------------------------------------
-from hypothesis import HealthCheck, given, settings  # noqa: E402
-from hypothesis import strategies as st  # noqa: E402
 
 _M64 = (1 << 64) - 1
 
