@@ -193,6 +193,16 @@ gc_status read_ckpt_header(std::FILE* in, const std::string& path, CkptHeader* h
   if ((h->dtype != GC_F64 && h->dtype != GC_F32) || h->nx <= 0 || h->ny <= 0 || h->nz <= 0 || h->components <= 0 ||
       h->data_bytes != static_cast<uint64_t>(h->nx) * h->ny * h->nz * h->components * (h->dtype == GC_F64 ? 8 : 4))
     return fail(GC_ERR_IO, "checkpoint: '" + path + "' has an inconsistent header");
+  // The sizes must add up to the file's, before anyone sizes a buffer by them.
+  const off_t at = ftello(in);
+  if (at < 0 || fseeko(in, 0, SEEK_END) != 0) return fail(GC_ERR_IO, "checkpoint: cannot read '" + path + "'");
+  const off_t end = ftello(in);
+  if (end < 0 || fseeko(in, at, SEEK_SET) != 0) return fail(GC_ERR_IO, "checkpoint: cannot read '" + path + "'");
+  const uint64_t size = static_cast<uint64_t>(end), body = size - sizeof *h;
+  if (h->meta_len > body || h->data_bytes > body - h->meta_len)
+    return fail(GC_ERR_IO, "checkpoint: '" + path + "' is truncated");
+  if (h->meta_len + h->data_bytes != body)
+    return fail(GC_ERR_IO, "checkpoint: '" + path + "' has an inconsistent header");
   return GC_OK;
 }
 
