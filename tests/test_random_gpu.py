@@ -26,7 +26,7 @@ def _host(t):
     return t.cpu().numpy()
 
 
-@settings(max_examples=40, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=40, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(data=st.data(), name=st.sampled_from(_OPS), order=st.sampled_from([2, 4, 6]))
 def test_random_operators(gc, oracle, data, name, order):
     shape = (data.draw(_AXIS), data.draw(_AXIS), data.draw(_AXIS))
@@ -57,7 +57,7 @@ def test_random_operators(gc, oracle, data, name, order):
     assert np.array_equal(got, want), (name, order, shape, h)
 
 
-@settings(max_examples=25, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=25, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(data=st.data(), order=st.sampled_from([2, 4, 6]), rk4=st.booleans())
 def test_random_cahn_hilliard(gc, oracle, data, order, rk4):
     """2-D grids of random (odd and even) widths, so that the strip, the
