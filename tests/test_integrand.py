@@ -206,7 +206,7 @@ from hypothesis import HealthCheck, assume, given, settings  # noqa: E402
 from hypothesis import strategies as st  # noqa: E402
 
 
-@settings(max_examples=250, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@settings(max_examples=250, deadline=None, derandomize=True, suppress_health_check=[HealthCheck.too_slow])
 @given(data=st.data(), arity=st.integers(1, 4))
 def test_random_integrands_record_exactly(oracle, data, arity):
     """Random expressions over every opcode and every input of the arity:
