@@ -1,5 +1,6 @@
 """The C-ABI library loads on a machine without a GPU and exports every entry
-point that include/gridcalc_b200.h declares (no compute calls here)."""
+point that include/gridcalc_b200.h declares; a plain C program uses the
+entry points that need no device (no compute calls here)."""
 import ctypes
 import os
 import re
@@ -46,3 +47,18 @@ def test_python_mirror_imports():
         assert "extents" in str(e)
     else:
         raise AssertionError("Grid(0, 1, 1) accepted")
+
+
+def test_c_program_uses_the_abi_without_gpu(tmp_path):
+    """tests/c/abi_c_test.c: the header compiles as strict C99 and a C
+    program linked against the library runs the device-free entry points."""
+    import subprocess
+    libdir = os.path.dirname(LIB)
+    exe = str(tmp_path / "abi_c_test")
+    cmd = ["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", os.path.join(ROOT, "tests", "c", "abi_c_test.c"),
+           "-I", os.path.join(ROOT, "include"), "-L", libdir, "-lgridcalc_b200", f"-Wl,-rpath,{libdir}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe, str(tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "FAIL" not in r.stdout, r.stdout + r.stderr
+    assert r.stdout.count("PASS") == 9, r.stdout
