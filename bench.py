@@ -8,29 +8,39 @@ One "step" is one RK4 step (four fused stage kernels).  Metric: Mcell-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The timed region is made of blocks of exactly K steps, each bracketed by a
+barrier and a device synchronize; blocks repeat until --min-seconds of device
+time have passed (so the clock sampler sees the load) and the value is the
+median block.
+
 Multi-GPU (torchrun, one rank per GPU): every rank advances its own replica
 (the method has no data-path exchange at this size: replicas only, weak
 scaling); the time is the max over ranks.
 
-Besides the headline line's `value`, the default single-GPU run measures the
-other forms under "forms" (each outside the headline's timed region, with a
-bounded budget stated in its entry): the operator sweep on 256^3 / 512^3
-Fourier-mode fields with errors against the analytic derivatives, the FVM
-heterogeneous diffusion on 384^3 (FP32, FP64 mass), the batched ensemble of
-256 members (FP32, order 4) with its speedup over the plain path and its
-error against the FP64 oracle, and the learned corrector (training and
-held-out evaluation).  `--forms headline` skips them.
+Besides the headline, the default single-GPU run measures the other forms,
+each outside the headline's timed region and printed as its own JSON line
+({"form": name, ...}) before the headline: the configured 128 x 128 plain run
+from the reference's mt19937_64 initial condition (config1), the operator
+sweep on 256^3 / 512^3 Fourier-mode fields with errors against the analytic
+derivatives, the FVM heterogeneous diffusion on 384^3 (FP32, FP64 mass), the
+batched ensemble of 256 members (FP32, order 4) with its speedup over the
+plain path and its per-member error on 16 members across the size range,
+and the learned corrector (training and held-out evaluation).  The headline
+line, printed last, carries a short summary of each under "forms".
+`--forms headline` skips them.
 
 The reference arm (--impl reference) times the reference's own CPU code
-(the reference headers compiled into oracle/_ref/libgcref.so; the C oracle
-port if that build is absent) on the box's host cores: independent replicas
-of a bounded 1024 x 1024 sample, one per host thread, each step one RK4 step.
+(the reference headers compiled into oracle/_ref; the release build for the
+host's x86-64 level where present) on the box's host cores: independent
+replicas of a bounded 1024 x 1024 sample, one per host thread, each step one
+RK4 step.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -52,6 +62,8 @@ BYTES_PER_CELL_STEP = 13 * 8
 # four stage kernels (one full capture on 4096^2: 1648.0 MB per step for
 # 16.8 M cells; both sizes are beyond L2, so it scales with the cell count).
 NCU_TRAFFIC_PER_CELL_STEP = 98.2
+# Forms the default run measures after the headline (each its own JSON line).
+DEFAULT_FORMS = ["config1", "operators", "fvm", "batched", "learned"]
 
 
 def peaks():
@@ -122,14 +134,12 @@ def dist_setup(n_gpus: int):
 
 
 def cpu_sample(threads: int, n: int = 1024, steps: int = 1):
-    """Runs the reference CPU code (or the C port) on `threads` independent
-    n x n replicas for `steps` RK4 steps each; returns (Mcell-steps/s, kind, sample)."""
+    """Runs the reference CPU code on `threads` independent n x n replicas
+    for `steps` RK4 steps each (one host thread per replica; the reference is
+    single-threaded); returns (Mcell-steps/s, build description)."""
     import numpy as np
     import oracle_lib
-    if oracle_lib.reference_available():
-        lib, kind = oracle_lib.reference(), "reference"
-    else:
-        lib, kind = oracle_lib.oracle(), "port"
+    lib, build = oracle_lib.timing_reference()
     rng = np.random.default_rng(7)
     states = [0.05 * (2.0 * rng.random((1, n, n)) - 1.0) for _ in range(threads)]
 
@@ -143,7 +153,11 @@ def cpu_sample(threads: int, n: int = 1024, steps: int = 1):
     for t in ts:
         t.join()
     dt = time.perf_counter() - t0
-    return threads * n * n * steps / dt / 1e6, kind, f"{threads} x RK4 on {n}x{n}, {steps} step(s) each"
+    return threads * n * n * steps / dt / 1e6, build
+
+
+def cpu_kind(build: str) -> str:
+    return "port" if build.startswith("C port") else "reference"
 
 
 def run_reference(args, rank: int, world: int):
@@ -153,19 +167,24 @@ def run_reference(args, rank: int, world: int):
     for _ in range(args.warmup):
         cpu_sample(threads)
     t0 = time.perf_counter()
-    rates = [cpu_sample(threads)[0] for _ in range(args.steps)]
+    rates = []
+    build = ""
+    for _ in range(args.steps):
+        r, build = cpu_sample(threads)
+        rates.append(r)
     wall = time.perf_counter() - t0
-    _, kind, sample = cpu_sample(1, 256, 1)
     value = statistics.median(rates)
+    sample = f"{threads} host threads, each one independent 1024x1024 replica, 1 RK4 step per timed step ({build})"
     line = {
         "impl": "reference", "metric": "Mcell-steps/s (plain FP64 RK4 Cahn-Hilliard)", "value": value,
         "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "ch2d-rk4-fp64-order2", "grid": f"{NX}x{NY} (CPU sample 1024x1024 per thread)",
+        "config": {"workload": "ch2d-rk4-fp64-order2",
+                   "grid": f"{threads} x 1024x1024 replicas (a bounded CPU sample of the 8192x8192 workload)",
                    "dt": DT, "kappa": 1.0, "mobility": 1.0},
-        "cpu_baseline": {"value": value, "unit": "Mcell-steps/s", "cores": threads, "kind": kind,
-                         "sample": f"{threads} threads x independent 1024x1024 replica, 1 RK4 step per timed step"},
+        "cpu_baseline": {"value": value, "unit": "Mcell-steps/s", "cores": threads, "kind": cpu_kind(build),
+                         "sample": sample},
         "e2e": {"value": value, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -375,10 +394,16 @@ def batch_members(seed=11, n=256):
     return members, ics
 
 
+def stratified(members, k: int = 16):
+    """k member indices spread evenly over the members sorted by side (the
+    smallest and the largest included)."""
+    order = sorted(range(len(members)), key=lambda i: (members[i][0], i))
+    return sorted({order[round(j * (len(order) - 1) / (k - 1))] for j in range(k)})
+
+
 def form_batched(gc, peak, steps=1000):
     import numpy as np
     import torch
-    import oracle_lib
     members, ics = batch_members()
     cells = sum(m[0] * m[1] for m in members)
     b = gc.ChBatch(members, order=4, dtype=torch.float32)
@@ -412,18 +437,23 @@ def form_batched(gc, peak, steps=1000):
             torch.cuda.synchronize()
             tot += s.elapsed_time(e) / 20
         plain[tag] = {"ms_per_step": tot, "Mcell-steps/s": cells / tot / 1e3}
-    # Accuracy against the FP64 oracle on the four smallest members.
-    oracle = oracle_lib.oracle()
-    idx = sorted(range(len(members)), key=lambda i: members[i][0])[:4]
+    # Accuracy of the FP32 ensemble after all steps, per member, on 16
+    # members spread over the whole size range, against the FP64 solution of
+    # the same member from the same (FP32-rounded) initial state.  The FP64
+    # solution is the plain FP64 GPU path, which the parity tests hold
+    # bit-identical to the CPU oracle (order 4 included).
     errs = []
-    for i in idx:
+    for i in stratified(members):
         nx, ny, mob, kap, dt = members[i]
-        c0 = ics[i].astype(np.float32).astype(np.float64).reshape(1, ny, nx)
-        want = oracle.ch_integrate(4, mob, kap, c0, dt, steps)
-        got = b.get_member(i).reshape(1, ny, nx)
-        fr = oracle.ch_free_energy(want, kap) + nx * ny / 4.0
-        errs.append({"member": i, "side": nx, "l2_err": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
-                     "f_err": abs((f1[i] + nx * ny / 4.0) - fr) / abs(fr)})
+        want = torch.from_numpy(ics[i].astype(np.float32).astype(np.float64).reshape(1, ny, nx)).cuda()
+        gg = gc.Grid(nx, ny, 1)
+        gc.ch_integrate(want, gg, gc.CahnHilliardRhs(mob, kap, 4), dt, steps, gc.RK4)
+        got = torch.from_numpy(b.get_member(i).reshape(1, ny, nx)).cuda().double()
+        v4 = nx * ny / 4.0
+        fr = gc.evaluate(want, gg, "ch_free_energy", kappa=kap) + v4
+        errs.append({"member": i, "side": nx, "l2_err": float(torch.linalg.norm(got - want) / torch.linalg.norm(want)),
+                     "f_err": abs((f1[i] + v4) - fr) / abs(fr)})
+        del want, got
     b.close()
     drift = max(abs(a - c) / max(1.0, abs(c)) for a, c in zip(m1, m0))
     return {"workload": "256 CH members, sides log-uniform in [64, 1024] (x16), FP32, order 4, own dt per member",
@@ -431,7 +461,60 @@ def form_batched(gc, peak, steps=1000):
             "GB/s": 52 * cells / ms / 1e6, "frac": 52 * cells / ms / 1e6 / peak, "autotune": tune,
             "plain": plain, "speedup_vs_plain_f32": rate / plain["plain_f32"]["Mcell-steps/s"],
             "speedup_vs_plain_f64": rate / plain["plain_f64"]["Mcell-steps/s"],
-            "max_mass_drift": drift, "oracle_check_smallest_members": errs}
+            "max_mass_drift": drift,
+            "accuracy": {"against": "FP64 plain RK4 of the same member (bit-identical to the oracle)",
+                         "members": errs, "sides": sorted({r["side"] for r in errs}),
+                         "l2_err_max": max(r["l2_err"] for r in errs), "f_err_max": max(r["f_err"] for r in errs)}}
+
+
+def form_config1(gc, steps=2000, every=100):
+    """The plain method exactly as configured: 128 x 128 x 1, FP64, h = 1,
+    M = kappa = 1, order-2 Laplacian twice, RK4 at dt = 0.01 for 2000 steps
+    from c = 0 plus U[-0.05, 0.05] i.i.d. draws of mt19937_64(seed 42)
+    (gc_random_ic, no mean subtraction).  Reports the GPU rate, the mass
+    drift and the free energy (f = (c^2 - 1)^2 / 4 convention: F + V/4) every
+    100 steps, and the reference's own CPU build on one core for the same
+    run (the CPU baseline of this configuration)."""
+    import torch
+    import oracle_lib
+    n = 128
+    g = gc.Grid(n, n, 1)
+    rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
+    c0 = gc.random_ic(g, 42, 0.05, subtract_mean=False)
+    psi0 = torch.from_numpy(c0).cuda()
+    w = psi0.clone()
+    gc.ch_integrate(w, g, rhs, DT, 64, gc.RK4)
+    psi = psi0.clone()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    gc.ch_integrate(psi, g, rhs, DT, steps, gc.RK4)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    v4 = g.size / 4.0
+    h = psi0.clone()
+    F = [gc.evaluate(h, g, "ch_free_energy", kappa=1.0) + v4]
+    mass0 = gc.integrate(h, g, gc.Kahan)
+    for _ in range(steps // every):
+        gc.ch_integrate(h, g, rhs, DT, every, gc.RK4)
+        F.append(gc.evaluate(h, g, "ch_free_energy", kappa=1.0) + v4)
+    mass1 = gc.integrate(h, g, gc.Kahan)
+    lib, build = oracle_lib.timing_reference()
+    t0 = time.perf_counter()
+    lib.ch_integrate(2, 1.0, 1.0, c0, DT, steps)
+    cpu_s = time.perf_counter() - t0
+    rate = g.size * steps / ms / 1e3
+    return {"workload": "ch2d-rk4-fp64-order2 128x128, dt 0.01, 2000 steps, IC mt19937_64(42) U[-0.05,0.05] "
+                        "no mean subtraction",
+            "steps": steps, "ms_total": ms, "us_per_step": 1e3 * ms / steps, "Mcell-steps/s": rate,
+            "history_equals_timed_run": bool(torch.equal(h, psi)),
+            "mass_initial": mass0, "mass_final": mass1, "mass_drift": mass1 - mass0,
+            "F_every_100_steps": F,
+            "cpu_baseline": {"value": g.size * steps / cpu_s / 1e6, "unit": "Mcell-steps/s", "cores": 1,
+                             "kind": cpu_kind(build), "seconds": cpu_s,
+                             "sample": f"the same 2000-step run, one host thread ({build})"},
+            "speedup_vs_cpu_1core": rate / (g.size * steps / cpu_s / 1e6)}
 
 
 def form_learned(gc, n_train=32, n_eval=4, fine_steps=5000, t_end=200.0, tols=(0.003, 0.01, 0.03), log=None):
@@ -518,21 +601,69 @@ def form_snapshots(gc, steps=2000, every=500):
     return out
 
 
+def _sig(x, digits=4):
+    """x rounded to `digits` significant digits (lists and dicts element-wise)."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, list):
+        return [_sig(v, digits) for v in x]
+    if isinstance(x, dict):
+        return {k: _sig(v, digits) for k, v in x.items()}
+    return x
+
+
+def form_summary(name: str, r: dict) -> dict:
+    """The few figures of a form that the headline line carries."""
+    if "error" in r:
+        return {"error": r["error"][:160]}
+    if name == "operators":
+        keys = ("laplacian2", "laplacian4", "gradient2", "divergence2", "biharmonic2", "integrate",
+                "evaluate_free_energy")
+        return {k: {op: _sig(v[op]["frac"], 3) for op in keys if op in v}
+                for k, v in r["results"].items() if k.endswith("512")}
+    if name == "fvm":
+        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "frac": r["frac"], "mass_drift_rel": r["mass_drift_rel"]})
+    if name == "config1":
+        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "us_per_step": r["us_per_step"],
+                     "cpu_1core_Mcell-steps/s": r["cpu_baseline"]["value"], "speedup_vs_cpu_1core": r["speedup_vs_cpu_1core"],
+                     "mass_drift": r["mass_drift"], "F_0": r["F_every_100_steps"][0],
+                     "F_2000": r["F_every_100_steps"][-1]})
+    if name == "batched":
+        acc = r["accuracy"]
+        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "frac": r["frac"],
+                     "speedup_vs_plain_f32": r["speedup_vs_plain_f32"], "speedup_vs_plain_f64": r["speedup_vs_plain_f64"],
+                     "members_checked": len(acc["members"]), "sides_checked": [min(acc["sides"]), max(acc["sides"])],
+                     "l2_err_max": acc["l2_err_max"], "f_err_max": acc["f_err_max"]})
+    if name.startswith("learned"):
+        out = {"trajectories": r["train"]["trajectories"], "heldout_seeds": r["eval"]["seeds"]}
+        for nm, v in r["eval"]["schemes"].items():
+            out[nm] = _sig({"speedup": v["speedup_vs_plain"], "fallback_rate": v["fallback_rate"],
+                            "l2_max": v["l2_err_max"], "f_err_max": v["f_err_max"]}, 3)
+        return out
+    if name == "snapshots":
+        return _sig({"overhead_pct": r["overhead_pct"]})
+    return {}
+
+
 def run_forms(gc, names, peak):
-    forms = {}
+    """Runs each form, prints its full result as its own JSON line
+    ({"form": name, ...}) and returns the short summaries for the headline."""
     table = {"operators": lambda: form_operators(gc, peak), "fvm": lambda: form_fvm(gc, peak),
-             "snapshots": lambda: form_snapshots(gc),
+             "snapshots": lambda: form_snapshots(gc), "config1": lambda: form_config1(gc),
              "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc),
              # the learned workload at its full size: 512 training trajectories, 64 held-out seeds
              "learned_full": lambda: form_learned(gc, n_train=512, n_eval=64, tols=(0.003, 0.01))}
+    summaries = {}
     for nm in names:
         t0 = time.perf_counter()
         try:
-            forms[nm] = table[nm]()
+            r = table[nm]()
         except Exception as exc:  # a failing form is reported, the headline stands
-            forms[nm] = {"error": f"{type(exc).__name__}: {exc}"}
-        forms[nm]["wall_s"] = time.perf_counter() - t0
-    return forms
+            r = {"error": f"{type(exc).__name__}: {exc}"}
+        r["wall_s"] = time.perf_counter() - t0
+        print(json.dumps({"form": nm, **r}), flush=True)
+        summaries[nm] = form_summary(nm, r)
+    return summaries
 
 
 def max_over_ranks(value: float, dist, device) -> float:
@@ -618,18 +749,15 @@ def run_ours(args, rank: int, world: int, local: int):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = f"cuda:{local}"
 
     g = gc.Grid(args.grid, args.grid, 1)
     rhs = gc.CahnHilliardRhs(1.0, 1.0, 2)
     rng = np.random.default_rng(1000 + rank)
     psi0 = 0.05 * (2.0 * rng.random(g.shape) - 1.0)
-    psi = torch.from_numpy(psi0).to(f"cuda:{local}")
-    ctx = gc.context()
-
-    # Warm-up: W steps, at least one 16-step graph unit so that the step
-    # graph is captured before the timed region.
-    gc.ch_integrate(psi, g, rhs, DT, max(args.warmup, 16), gc.RK4)
-    torch.cuda.synchronize()
+    psi = torch.from_numpy(psi0).to(dev)
+    cells = g.size
+    K = args.steps
 
     def barrier():
         if dist is not None:
@@ -637,28 +765,46 @@ def run_ours(args, rank: int, world: int, local: int):
         torch.cuda.synchronize()
 
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    with ClockSampler(local) as clocks:
+
+    def block() -> float:
+        """Exactly K RK4 steps, bracketed by a barrier and a device
+        synchronize on both sides; returns the CUDA-event milliseconds."""
+        barrier()
         start.record()
-        gc.ch_integrate(psi, g, rhs, DT, args.steps, gc.RK4)
+        gc.ch_integrate(psi, g, rhs, DT, K, gc.RK4)
         end.record()
-        torch.cuda.synchronize()
-    barrier()
-    ms = max_over_ranks(start.elapsed_time(end), dist, f"cuda:{local}")
-    cells = g.size
-    value = whole_job_rate(world, cells, args.steps, ms)
-    ms_per_step = ms / args.steps
+        barrier()
+        return start.elapsed_time(end)
+
+    # Warm-up: W untimed steps (at least one 16-step graph unit, so the step
+    # graphs are captured), then one untimed block to size the timed region.
+    gc.ch_integrate(psi, g, rhs, DT, max(args.warmup, 16), gc.RK4)
+    est = max_over_ranks(block(), dist, dev)
+    # Timed region: blocks of exactly K steps repeated until about
+    # args.min_seconds of device time have passed, so that the clock sampler
+    # (every 100 ms) sees the load; the value is the median block (max over
+    # ranks per block).
+    n_blocks = int(min(1000, max(3, math.ceil(1000.0 * args.min_seconds / max(est, 1e-3)))))
+    with ClockSampler(local) as clocks:
+        times = [block() for _ in range(n_blocks)]
+    if dist is not None:
+        t = torch.tensor(times, dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times = t.tolist()
+    ms = statistics.median(times)
+    value = whole_job_rate(world, cells, K, ms)
+    ms_per_step = ms / K
     achieved = BYTES_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e9
     peak, peak_kind = peaks()
 
     # e2e: pinned host field -> the C-ABI call -> pinned host field, in
-    # chunks of `chunk` steps (one upload and one snapshot per chunk), copies
+    # chunks of K steps (one upload and one download per chunk), copies
     # inside the timing.  Chunks are independent runs from the same host
     # field and alternate between two contexts on two streams, so one
     # chunk's copies overlap the other's steps (the first upload and the last
-    # download stay exposed).
-    chunk = min(args.steps, 100)
-    n_chunks = max(1, args.steps // chunk)
+    # download stay exposed); as many chunks as the timed region had blocks.
+    chunk = K
+    n_chunks = max(2, n_blocks)
     host_psi = torch.from_numpy(psi0).pin_memory()
     streams = [torch.cuda.Stream() for _ in range(2)]
     ctxs = [gc.Context(local, s.cuda_stream) for s in streams]
@@ -684,48 +830,44 @@ def run_ours(args, rank: int, world: int, local: int):
         torch.cuda.current_stream().wait_stream(s)
     e1.record()
     torch.cuda.synchronize()
-    ems = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{local}")
+    ems = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     e2e = whole_job_rate(world, cells, chunk * n_chunks, ems)
     for c in ctxs:
         c.close()
 
-    launches = 4 * args.steps  # four stage kernels per RK4 step
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, kind, sample = cpu_sample(1, 2048, 2)
-        cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": 1, "kind": kind,
-               "sample": f"1 thread, RK4 on 2048x2048, 2 steps ({sample.split(',')[0]})"}
-    forms = None
+        rate, build = cpu_sample(1, 2048, 2)
+        cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": 1, "kind": cpu_kind(build),
+               "sample": f"1 host thread, RK4 on 2048x2048, 2 steps ({build})"}
+    summaries = None
     if rank == 0 and world == 1 and args.forms != "headline":
-        names = ["operators", "fvm", "batched", "learned"] if args.forms == "all" else args.forms.split(",")
-        forms = run_forms(gc, [n for n in names if n != "headline"], peaks()[0])
+        names = DEFAULT_FORMS if args.forms == "all" else args.forms.split(",")
+        summaries = run_forms(gc, [n for n in names if n != "headline"], peak)
     if rank == 0:
-        traffic = None
-        if NCU_TRAFFIC_PER_CELL_STEP is not None:
-            traffic = NCU_TRAFFIC_PER_CELL_STEP * cells / 4.0
+        traffic = NCU_TRAFFIC_PER_CELL_STEP * cells / 4.0 if NCU_TRAFFIC_PER_CELL_STEP is not None else None
         line = {
             "metric": "Mcell-steps/s (plain FP64 RK4 Cahn-Hilliard)", "value": value, "unit": "Mcell-steps/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "ch2d-rk4-fp64-order2", "grid": f"{g.nx}x{g.ny}", "dt": DT, "kappa": 1.0,
                        "mobility": 1.0, "ic": "U[-0.05,0.05] seeded", "l2": "fields 512 MiB each > L2 (no flush)",
+                       "timing": f"median of {n_blocks} blocks of {K} steps (CUDA events, max over ranks)",
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "ch_tma_x2_kernel (RK4 stages 1-3) + ch_tma_kernel (stage 4): "
-                                   "4 launches per step, 104 B/cell-step algorithmic",
-                         "traffic_unit": "bytes per launch (average of the 4 stage launches)"},
+                         "kernel": "RK4 stage kernels, 4 launches per step, 104 B/cell-step algorithmic"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": cells * 8 / chunk,
                     "d2h_bytes_per_step": cells * 8 / chunk,
-                    "note": f"pinned host field -> device, {chunk} RK4 steps via gc_ch_integrate, device -> host; "
-                             "chunks alternate between two contexts on two streams"},
-            "gpu_launches": launches,
+                    "note": f"{n_chunks} chunks of {chunk} steps: pinned host -> device, gc_ch_integrate, "
+                            "device -> pinned host; two contexts on two streams"},
+            "gpu_launches": 4 * K * n_blocks,
             "clocks": clocks.summary(),
         }
-        if forms is not None:
-            line["forms"] = forms
+        if summaries is not None:
+            line["forms"] = summaries
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -743,6 +885,8 @@ def main():
     ap.add_argument("--case", default=None,
                     help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
                          "batch64_f32, ch_f32_4096, eval_fe_320")
+    ap.add_argument("--min-seconds", type=float, default=1.5,
+                    help="repeat the K-step timed block until this much device time has passed")
     ap.add_argument("--forms", default="all",
                     help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full,snapshots "
                          "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")

@@ -1110,7 +1110,7 @@ GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtyp
 // Advances one 2-D double field by n_coarse coarse steps of
 // dt_fine * fine_per_coarse.  Each coarse step proposes B(c) + delta(c)
 // (c + delta(c) without a base step) and accepts it when the free energy
-// does not rise by more than energy_tol and the trapezoid residual
+// does not rise by more than energy_tol + energy_rtol |F| and the trapezoid residual
 // |(c1 - c0)/Dt - (f(c0) + f(c1))/2| / |(f(c0) + f(c1))/2| is at most
 // residual_tol; otherwise the step is taken by fine_per_coarse plain RK4
 // steps.  The proposal (base step, network, candidate, acceptance
@@ -1216,8 +1216,12 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
     GC_TRY(read_stats());
     const double F1 = sums[0];
     const double res = sums[2] > 0.0 ? std::sqrt(sums[1] / sums[2]) : 0.0;
-    const bool accept = F1 <= F0 + pol->energy_tol && res <= pol->residual_tol;
+    const bool energy_ok = F1 <= F0 + (pol->energy_tol + pol->energy_rtol * std::fabs(F0));
+    const bool residual_ok = res <= pol->residual_tol;
+    const bool accept = energy_ok && residual_ok;
     sres.last_residual = res;
+    if (!energy_ok) ++sres.rejected_energy;
+    if (!residual_ok) ++sres.rejected_residual;
     if (accept) {
       GC_CUDA(cudaMemcpyAsync(psi, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       F0 = F1;
@@ -1234,6 +1238,8 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
   if (stats) {
     stats->accepted += sres.accepted;
     stats->fallbacks += sres.fallbacks;
+    stats->rejected_energy += sres.rejected_energy;
+    stats->rejected_residual += sres.rejected_residual;
     stats->last_residual = sres.last_residual;
   }
   return GC_OK;

@@ -605,11 +605,12 @@ class ChBatch:
 
 class gc_corrector_policy(C.Structure):
     _fields_ = [("dt_fine", C.c_double), ("fine_per_coarse", C.c_int32),
-                ("residual_tol", C.c_double), ("energy_tol", C.c_double)]
+                ("residual_tol", C.c_double), ("energy_tol", C.c_double), ("energy_rtol", C.c_double)]
 
 
 class gc_corrector_stats(C.Structure):
-    _fields_ = [("accepted", C.c_int64), ("fallbacks", C.c_int64), ("last_residual", C.c_double)]
+    _fields_ = [("accepted", C.c_int64), ("fallbacks", C.c_int64), ("rejected_energy", C.c_int64),
+                ("rejected_residual", C.c_int64), ("last_residual", C.c_double)]
 
 
 for _name, _args in {
@@ -632,6 +633,12 @@ lib.gc_corrector_num_params.restype = C.c_int32
 lib.gc_corrector_num_params.argtypes = []
 
 CORRECTOR_LAYERS, CORRECTOR_CHANNELS = 6, 32
+# Default relative free-energy tolerance of the accept/reject judge: a rise
+# of F by one part in 1e10 per coarse step is accepted.  It is far above the
+# FP64 round-off of F's sum (about cells x 1e-16 x the mean density, 1e-16 of
+# |F|) and far below the 1e-3 free-energy error target (1250 coarse steps to
+# t = 200 could add at most 1.25e-7 of |F|).
+ENERGY_RTOL = 1e-10
 
 
 def corrector_init_params(seed: int = 0, last_scale: float = 0.1, inputs: int = 1):
@@ -750,12 +757,18 @@ class Corrector:
         return loss.value
 
     def advance(self, psi, grid: Grid, rhs: "CahnHilliardRhs", n_coarse: int, dt_fine: float = 0.01,
-                fine_per_coarse: int = 16, residual_tol: float = 0.05, energy_tol: float = 0.0):
-        pol = gc_corrector_policy(dt_fine, fine_per_coarse, residual_tol, energy_tol)
+                fine_per_coarse: int = 16, residual_tol: float = 0.05, energy_tol: float = 0.0,
+                energy_rtol: float = ENERGY_RTOL):
+        """n_coarse learned coarse steps of psi (in place), each accepted when
+        F rises by at most energy_tol + energy_rtol |F| and the trapezoid
+        residual is at most residual_tol, else replaced by plain RK4 steps;
+        returns the counts, with the rejections by cause."""
+        pol = gc_corrector_policy(dt_fine, fine_per_coarse, residual_tol, energy_tol, energy_rtol)
         st = gc_corrector_stats()
         _check(lib.gc_corrector_advance(self.handle, C.byref(grid.c()), C.byref(rhs.c()), psi.data_ptr(),
                                         n_coarse, C.byref(pol), C.byref(st)))
-        return {"accepted": st.accepted, "fallbacks": st.fallbacks, "last_residual": st.last_residual}
+        return {"accepted": st.accepted, "fallbacks": st.fallbacks, "rejected_energy": st.rejected_energy,
+                "rejected_residual": st.rejected_residual, "last_residual": st.last_residual}
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -957,3 +970,21 @@ def check_finite(field, grid: Grid, ctx=None) -> None:
     first = C.c_int64(-1)
     _check(lib.gc_check_finite(_ctx(ctx), C.byref(grid.c()), _dtype_code(field), _components(field.numel(), grid),
                                field.data_ptr(), C.byref(first)))
+
+
+# --- seeded initial condition (makeRandomIc) ---------------------------------
+lib.gc_random_ic.argtypes = [C.POINTER(gc_grid), C.c_uint64, C.c_double, C.c_int32, C.c_void_p]
+lib.gc_random_ic.restype = C.c_int
+
+
+def random_ic(grid: Grid, seed: int, amplitude: float, subtract_mean: bool = True):
+    """makeRandomIc (examples/common/cahn_hilliard.hpp:85-103): one draw per
+    cell of uniform_real_distribution(-amplitude, amplitude) over
+    mt19937_64(seed), in flat index order, the mean subtracted (or, with
+    subtract_mean=False, the raw draws: 0 plus i.i.d. uniform noise).
+    Returns a host float64 array of shape (nz, ny, nx)."""
+    import numpy as np
+    out = np.empty(grid.shape, dtype=np.float64)
+    _check(lib.gc_random_ic(C.byref(grid.c()), C.c_uint64(seed), float(amplitude), int(bool(subtract_mean)),
+                            out.ctypes.data))
+    return out

@@ -20,7 +20,8 @@ import time
 
 import numpy as np
 
-from . import CahnHilliardRhs, Corrector, Grid, RK4, ch_integrate, ch_rhs, ch_rkc, corrector_init_params, evaluate
+from . import (ENERGY_RTOL, CahnHilliardRhs, Corrector, Grid, RK4, ch_integrate, ch_rhs, ch_rkc,
+               corrector_init_params, evaluate)
 
 DT_FINE = 0.01
 FINE_PER_COARSE = 16
@@ -112,18 +113,21 @@ def _free_energy_baseline(psi, g: Grid) -> float:
     return evaluate(psi, g, "ch_free_energy", kappa=1.0) + g.size * g.cell_volume / 4.0
 
 
-def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, energy_tol: float = 0.0) -> dict:
+def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, energy_tol: float = 0.0,
+                     energy_rtol: float = ENERGY_RTOL) -> dict:
     """schemes: list of (name, corrector, residual_tol).  Per seed the plain
     fine RK4 reference runs once; every scheme advances the same initial
     state by coarse steps with the plain-RK4 fallback and is compared with
-    it at t_end."""
+    it at t_end.  Fallbacks are also counted by cause (the proposal raised F
+    beyond energy_tol + energy_rtol |F|, or its residual exceeded the
+    scheme's tolerance; a proposal can fail both)."""
     import torch
     g = Grid(size, size, 1)
     rhs = CahnHilliardRhs(1.0, 1.0, 2)
     n_fine = int(round(t_end / DT_FINE))
     n_coarse = n_fine // FINE_PER_COARSE
     t_fine = 0.0
-    rec = {name: {"l2": [], "ferr": [], "acc": 0, "fb": 0, "t": 0.0} for name, _, _ in schemes}
+    rec = {name: {"l2": [], "ferr": [], "acc": 0, "fb": 0, "rej_e": 0, "rej_r": 0, "t": 0.0} for name, _, _ in schemes}
     for s in seeds:
         c0 = torch.from_numpy(initial_condition(s, size)).cuda()
         ref = c0.clone()
@@ -138,21 +142,25 @@ def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, ener
             x = c0.clone()
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            st = net.advance(x, g, rhs, n_coarse, DT_FINE, FINE_PER_COARSE, tol, energy_tol)
+            st = net.advance(x, g, rhs, n_coarse, DT_FINE, FINE_PER_COARSE, tol, energy_tol, energy_rtol)
             torch.cuda.synchronize()
             r["t"] += time.perf_counter() - t1
             r["acc"] += st["accepted"]
             r["fb"] += st["fallbacks"]
+            r["rej_e"] += st["rejected_energy"]
+            r["rej_r"] += st["rejected_residual"]
             r["l2"].append(float(torch.linalg.norm(x - ref) / torch.linalg.norm(ref)))
             r["ferr"].append(abs(_free_energy_baseline(x, g) - fr) / abs(fr))
     cells_steps = len(seeds) * size * size * n_coarse * FINE_PER_COARSE
     out = {"seeds": len(seeds), "t_end": t_end, "coarse_steps_per_scheme": n_coarse * len(seeds),
+           "energy_tol": energy_tol, "energy_rtol": energy_rtol,
            "plain_mcell_steps": cells_steps / t_fine / 1e6, "schemes": {}}
     for name, _, tol in schemes:
         r = rec[name]
         out["schemes"][name] = {
             "residual_tol": tol, "accepted": r["acc"], "fallbacks": r["fb"],
             "fallback_rate": r["fb"] / max(r["acc"] + r["fb"], 1),
+            "rejected_energy": r["rej_e"], "rejected_residual": r["rej_r"],
             "l2_err_mean": float(np.mean(r["l2"])), "l2_err_max": float(np.max(r["l2"])),
             "f_err_mean": float(np.mean(r["ferr"])), "f_err_max": float(np.max(r["ferr"])),
             "mcell_steps_equiv": cells_steps / r["t"] / 1e6, "speedup_vs_plain": t_fine / r["t"]}

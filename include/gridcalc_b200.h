@@ -299,6 +299,16 @@ GC_API gc_status gc_ch_rkc(gc_context* ctx, const gc_grid* g, gc_dtype dt, const
                            double dt_step, int32_t n_steps, int32_t stages);
 GC_API double gc_rkc_stability_bound(int32_t stages);
 
+/* makeRandomIc (examples/common/cahn_hilliard.hpp:85-103): fills the HOST
+ * buffer out (nx*ny*nz doubles, i fastest) with one draw per cell, in flat
+ * index order, of std::uniform_real_distribution<double>(-amplitude,
+ * amplitude) over std::mt19937_64(seed) -- the bytes the reference's build
+ * produces with libstdc++.  subtract_mean != 0 then subtracts the draws' mean
+ * (sequential sum / n) as the reference does; 0 keeps the raw draws
+ * (c = 0 plus i.i.d. uniform noise).  No GPU work. */
+GC_API gc_status gc_random_ic(const gc_grid* g, uint64_t seed, double amplitude, int32_t subtract_mean,
+                              double* out);
+
 /* solve::diffuse(psi, double D, dt, n_steps, tag) (solve/Diffusion.hpp:89-112):
  * constant-D heat equation with the order-2 Laplacian and the tag's CFL check. */
 GC_API gc_status gc_diffuse(gc_context* ctx, const gc_grid* g, gc_dtype dt, void* psi,
@@ -368,12 +378,15 @@ typedef struct gc_corrector_policy {
   double dt_fine;           /* fine RK4 step (the plain method's dt) */
   int32_t fine_per_coarse;  /* fine steps one coarse step replaces */
   double residual_tol;      /* accept when the trapezoid residual is at most this */
-  double energy_tol;        /* accept when F rises by at most this */
+  double energy_tol;        /* accept when F rises by at most energy_tol + energy_rtol |F| */
+  double energy_rtol;
 } gc_corrector_policy;
 
 typedef struct gc_corrector_stats {
-  int64_t accepted;         /* coarse steps taken by the network */
-  int64_t fallbacks;        /* coarse steps taken by plain RK4 instead */
+  int64_t accepted;           /* coarse steps taken by the network */
+  int64_t fallbacks;          /* coarse steps taken by plain RK4 instead */
+  int64_t rejected_energy;    /* fallbacks whose proposal raised F beyond the tolerance */
+  int64_t rejected_residual;  /* fallbacks whose proposal's residual exceeded residual_tol */
   double last_residual;
 } gc_corrector_stats;
 

@@ -455,6 +455,16 @@ void ref_make_random_ic(int nx, int ny, int nz, double hx, double hy, double hz,
   store(ch::makeRandomIc(g, seed, amplitude), out);
 }
 
+// The draws of makeRandomIc before its mean subtraction
+// (examples/common/cahn_hilliard.hpp:89-95): std::mt19937_64(seed) through
+// std::uniform_real_distribution<double>(-amplitude, amplitude), one per
+// value, in order.  Pins the product's generator when it keeps raw draws.
+void ref_uniform_draws(uint64_t seed, double amplitude, size_t n, double* out) {
+  std::mt19937_64 rng(seed);
+  std::uniform_real_distribution<double> dist(-amplitude, amplitude);
+  for (size_t i = 0; i < n; ++i) out[i] = dist(rng);
+}
+
 // Constant-D heat equation, solve/Diffusion.hpp:89-112.
 int ref_diffuse_const(int nx, int ny, int nz, double hx, double hy, double hz, double* psi,
                       double D, double dt, int n_steps, int integrator) {

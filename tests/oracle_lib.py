@@ -213,6 +213,13 @@ class Reference(_Lib):
         self.lib.ref_make_random_ic(*self._g(shape, h), C.c_uint64(seed), _d(amplitude), _ptr(out))
         return out
 
+    def uniform_draws(self, seed: int, amplitude: float, n: int) -> np.ndarray:
+        """makeRandomIc's draws before the mean subtraction (std::mt19937_64 +
+        std::uniform_real_distribution of the C++ library this was built with)."""
+        out = np.zeros(n)
+        self.lib.ref_uniform_draws(C.c_uint64(seed), _d(amplitude), C.c_size_t(n), _ptr(out))
+        return out
+
 
 def oracle() -> Oracle:
     return Oracle()
@@ -224,3 +231,37 @@ def reference_available() -> bool:
 
 def reference() -> Reference:
     return Reference()
+
+
+# CPU flags each x86-64 micro-architecture level needs (x86-64 psABI).
+_LEVEL_FLAGS = {
+    "v4": {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl", "avx2", "fma", "bmi2"},
+    "v3": {"avx", "avx2", "fma", "bmi1", "bmi2", "movbe", "f16c", "abm", "xsave"},
+}
+
+
+def _cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def timing_reference():
+    """The reference build for the timed CPU baseline: the release build
+    (-O3 -DNDEBUG) for the highest x86-64 level this CPU supports, else the
+    parity build.  Returns (library, description)."""
+    flags = _cpu_flags()
+    for level in ("v4", "v3"):
+        path = os.path.join(ORACLE_DIR, "_ref", f"libgcref_{level}.so")
+        if os.path.exists(path) and _LEVEL_FLAGS[level] <= flags:
+            lib = Reference.__new__(Reference)
+            _Lib.__init__(lib, path, "ref_")
+            return lib, f"reference headers, g++ -O3 -DNDEBUG -march=x86-64-{level}"
+    if reference_available():
+        return reference(), "reference headers, g++ -O3 -DNDEBUG -ffp-contract=off (parity build)"
+    return oracle(), "C port of the reference (oracle/gc_oracle.c), gcc -O2"

@@ -170,6 +170,9 @@ def test_rejected_steps_fall_back_to_plain_rk4_exactly(gc, oracle):
     g = gc.Grid(size, size, 1)
     stats = net.advance(t, g, gc.CahnHilliardRhs(1.0, 1.0, 2), n_coarse=5, residual_tol=0.5)
     assert stats["fallbacks"] == 5 and stats["accepted"] == 0
+    # By cause: an unchanged proposal keeps F (energy check passes) but its
+    # residual is 1 > 0.5.
+    assert stats["rejected_residual"] == 5 and stats["rejected_energy"] == 0
     torch.cuda.synchronize()
     want = oracle.ch_integrate(2, 1.0, 1.0, psi0, 0.01, 80)
     assert np.array_equal(t.cpu().numpy(), want[0])
