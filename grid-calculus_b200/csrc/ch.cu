@@ -371,12 +371,8 @@ gc_status launch_tma(gc_context* ctx, const StageParams<T>& p) {
   if (!make_tensor_map_2d(&mpsi, p.psi, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
   if (KIN && !make_tensor_map_2d(&mkin, p.kin, p.nx, p.ny, eb, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
   auto kern = ch_tma_kernel<T, ORDER, MODE, KIN>;
-  static int ctas_per_sm = 0;  // one instantiation per template argument set
-  if (ctas_per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::BYTES)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kTmaThreads, L::BYTES));
-    if (ctas_per_sm < 1) ctas_per_sm = 1;
-  }
+  int ctas_per_sm = 1;
+  GC_TRY(kernel_setup(kern, kTmaThreads, L::BYTES, &ctas_per_sm));
   const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
   const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
   const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(ctas_per_sm) * ctx->num_sms));
@@ -687,12 +683,8 @@ gc_status launch_tma_x2(gc_context* ctx, const StageParams<double>& p) {
   if (!make_tensor_map_2d(&mpsi, p.psi, p.nx, p.ny, 8, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
   if (KIN && !make_tensor_map_2d(&mkin, p.kin, p.nx, p.ny, 8, L::YX, L::YY)) return GC_ERR_UNSUPPORTED;
   auto kern = ch_tma_x2_kernel<ORDER, MODE, KIN>;
-  static int ctas_per_sm = 0;  // one instantiation per template argument set
-  if (ctas_per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(L::BYTES)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas_per_sm, kern, kX2DT * L::NTY, L::BYTES));
-    if (ctas_per_sm < 1) ctas_per_sm = 1;
-  }
+  int ctas_per_sm = 1;
+  GC_TRY(kernel_setup(kern, kX2DT * L::NTY, L::BYTES, &ctas_per_sm));
   const int tiles_x = div_up(p.nx, L::TX), tiles_y = div_up(p.ny, L::TY);
   const long long ntiles = static_cast<long long>(tiles_x) * tiles_y;
   const long long slots = static_cast<long long>(ctas_per_sm) * ctx->num_sms;
@@ -735,12 +727,8 @@ gc_status launch_pipe(gc_context* ctx, const StageParams<T>& p) {
   constexpr int TX = kT2W - 2 * W<2, ORDER>::R;
   constexpr size_t smem = pipe_smem<T, ORDER, kT2W, kT2Y>();
   auto kern = ch_pipe_kernel<T, ORDER, MODE>;
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT2W * kT2TY, smem));
-    if (per_sm < 1) per_sm = 1;
-  }
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, kT2W * kT2TY, smem, &per_sm));
   const int tiles_x = div_up(p.nx, TX), tiles_y = div_up(p.ny, kT2Y);
   const int n_tiles = tiles_x * tiles_y;
   const int grid = std::max(1, std::min(n_tiles, per_sm * ctx->num_sms));
@@ -767,12 +755,8 @@ gc_status launch_pipe_x2(gc_context* ctx, const StageParams<float>& p) {
   constexpr int TX = 2 * kX2T - 2 * W<2, ORDER>::R;
   constexpr size_t smem = pipe_smem_x2<ORDER, kX2T, kT2Y>();
   auto kern = ch_pipe_x2_kernel<ORDER, MODE>;
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kX2T * kT2TY, smem));
-    if (per_sm < 1) per_sm = 1;
-  }
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, kX2T * kT2TY, smem, &per_sm));
   const int tiles_x = div_up(p.nx, TX), tiles_y = div_up(p.ny, kT2Y);
   const int n_tiles = tiles_x * tiles_y;
   const int grid = std::max(1, std::min(n_tiles, per_sm * ctx->num_sms));

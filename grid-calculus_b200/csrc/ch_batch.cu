@@ -252,12 +252,8 @@ template <int ORDER, int MODE, int TW, int TY, int NTY>
 gc_status launch_batch_shape_x2(gc_ch_batch* b, const BatchBuffers<float>& buf, int stage) {
   constexpr size_t smem = pipe_smem_x2<ORDER, TW, TY>();
   auto kern = ch_batch_x2_kernel<ORDER, MODE, TW, TY, NTY>;
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TW * NTY, smem));
-    if (per_sm < 1) per_sm = 1;
-  }
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, TW * NTY, smem, &per_sm));
   const int grid = std::max(1, std::min(b->n_items, per_sm * b->ctx->num_sms));
   kern<<<grid, dim3(TW, NTY), smem, b->ctx->stream>>>(static_cast<const Member<float>*>(b->member_table),
                                                      static_cast<const int4*>(b->items), b->n_items, buf, stage);
@@ -272,12 +268,8 @@ gc_status launch_batch_shape(gc_ch_batch* b, const BatchBuffers<T>& buf, int sta
   }
   constexpr size_t smem = pipe_smem<T, ORDER, TW, TY>();
   auto kern = ch_batch_kernel<T, ORDER, MODE, TW, TY, NTY>;
-  static int per_sm = 0;
-  if (per_sm == 0) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TW * NTY, smem));
-    if (per_sm < 1) per_sm = 1;
-  }
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, TW * NTY, smem, &per_sm));
   const int grid = std::max(1, std::min(b->n_items, per_sm * b->ctx->num_sms));
   kern<<<grid, dim3(TW, NTY), smem, b->ctx->stream>>>(static_cast<const Member<T>*>(b->member_table),
                                                      static_cast<const int4*>(b->items), b->n_items, buf, stage);

@@ -68,6 +68,11 @@ struct gc_context {
   uint64_t graph_key[kGraphSlots][8] = {};
   uint64_t graph_used[kGraphSlots] = {};
   uint64_t graph_clock = 0;
+  // FFT plans of the spectral entry points: one set per context, so each
+  // context's transforms run on its own stream with their own work area;
+  // released by gc_context_destroy through spectral_release.
+  void* spectral_plans = nullptr;
+  void (*spectral_release)(void*) = nullptr;
 };
 
 namespace gcb {
@@ -92,6 +97,18 @@ gc_status require_axes(const gc_grid* g, int radius);
 // Per-axis radii (an axis with radius 0 accepts any extent).
 gc_status require_axes3(const gc_grid* g, int rx, int ry, int rz);
 gc_status check_ctx(gc_context* ctx);
+
+// Opts kernel `kern` into `smem` bytes of dynamic shared memory on the
+// current device and, with ctas_per_sm, returns how many CTAs of `threads`
+// threads and `smem` bytes fit on one SM (at least 1).  The attribute belongs
+// to one device's context, so it is set once per (kernel, device) -- not once
+// per process -- under a lock, since contexts may be driven from several host
+// threads.
+gc_status kernel_setup_raw(const void* kern, int threads, size_t smem, int* ctas_per_sm);
+template <class K>
+inline gc_status kernel_setup(K* kern, int threads, size_t smem, int* ctas_per_sm = nullptr) {
+  return kernel_setup_raw(reinterpret_cast<const void*>(kern), threads, smem, ctas_per_sm);
+}
 
 // Stream-ordered building blocks for other parts of the library (no
 // validation, no Call scope, no allocation): enqueue on ctx->stream only, so

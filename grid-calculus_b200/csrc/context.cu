@@ -1,7 +1,10 @@
 // Context, error state, scratch and memory helpers of the C ABI.
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -40,6 +43,32 @@ Call::~Call() {
   if (!ctx || !ctx->ev_out) return;
   if (cudaEventRecord(ctx->ev_out, ctx->stream) == cudaSuccess)
     cudaStreamWaitEvent(ctx->user_stream, ctx->ev_out, 0);
+}
+
+gc_status kernel_setup_raw(const void* kern, int threads, size_t smem, int* ctas_per_sm) {
+  int dev = 0;
+  GC_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> smem_set;             // (kernel, device) -> bytes
+  static std::map<std::tuple<const void*, int, int, size_t>, int> occupancy;  // (kernel, device, threads, bytes)
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kern, dev);
+  auto it = smem_set.find(key);
+  if (smem > 48 * 1024 && (it == smem_set.end() || it->second < smem)) {
+    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    smem_set[key] = smem;
+  }
+  if (ctas_per_sm) {
+    const auto okey = std::make_tuple(kern, dev, threads, smem);
+    auto ot = occupancy.find(okey);
+    if (ot == occupancy.end()) {
+      int n = 0;
+      GC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem));
+      ot = occupancy.emplace(okey, n < 1 ? 1 : n).first;
+    }
+    *ctas_per_sm = ot->second;
+  }
+  return GC_OK;
 }
 
 // core::Grid constructor preconditions (core/Grid.hpp:39-52).
@@ -172,6 +201,7 @@ GC_API gc_status gc_context_destroy(gc_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& ge : ctx->graph_exec)
     if (ge) cudaGraphExecDestroy(ge);
+  if (ctx->spectral_release) ctx->spectral_release(ctx->spectral_plans);
   for (auto& s : ctx->scratch)
     if (s.ptr) cudaFree(s.ptr);
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);

@@ -780,11 +780,7 @@ template <int EPI, int NT, bool STORE_Z>
 gc_status launch_conv(gc_corrector* c, int batch, const __nv_bfloat16* in, const __nv_bfloat16* w,
                       const float* bias, __nv_bfloat16* oz, __nv_bfloat16* oy, float* of, const __nv_bfloat16* zp) {
   auto kern = conv3x3_umma_kernel<EPI, STORE_Z>;
-  static bool attr = false;  // one flag per instantiation
-  if (!attr) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kUSmem));
-    attr = true;
-  }
+  GC_TRY(kernel_setup(kern, kUThreads, kUSmem));
   const int tiles_x = div_up(c->W, kUM);
   const int tpi = tiles_x * div_up(c->H, kUR);
   const int n_tiles = batch * tpi;

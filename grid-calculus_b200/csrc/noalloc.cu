@@ -25,8 +25,10 @@
 // Host code must not pass the array's name to a kernel: in host code it is
 // a host-side stand-in, not a device address.  The first call on each
 // device, with that device current, looks up the device address with
-// cudaGetSymbolAddress (and sets the chunk kernel's shared-memory limit);
-// make that first call before any stream capture.
+// cudaGetSymbolAddress (and sets the chunk kernel's shared-memory limit) and
+// keeps both for the life of the process; make that first call before any
+// stream capture, and do not reset the device after it (cudaDeviceReset
+// unloads the module, which would leave the kept address stale).
 #include <mutex>
 #include <string>
 

@@ -168,11 +168,7 @@ gc_status launch_partial(gc_context* ctx, PartialParams& p) {
   const size_t smem = sizeof(T) * static_cast<size_t>(2 * p.rz + 1 + kPRing) * (PX + 2 * p.R) * (PY + 2 * p.R);
   // rx, ry <= 4 (axis_table): one instantiation per (WX, WY).
   void (*kern)(const PartialParams) = kernel_for<T>(p.rx, p.ry);
-  static bool attr[5][5] = {};
-  if (!attr[p.rx][p.ry]) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
-    attr[p.rx][p.ry] = true;
-  }
+  GC_TRY(kernel_setup(kern, PX * PY, smem));
   kern<<<dim3(tiles_x, tiles_y, chunks), dim3(PX, PY), smem, ctx->stream>>>(p);
   GC_CHECK_LAUNCH("partial_kernel");
   return GC_OK;

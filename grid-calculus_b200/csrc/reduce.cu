@@ -186,12 +186,8 @@ gc_status pairwise_sum(gc_context* ctx, const T* x, long long n, double* result)
   if (s != GC_OK) return s;
   double* a = static_cast<double*>(buf);
   const size_t smem = sizeof(double) * (padpos(kChunkMax) + 8 + kNodeMax);
-  static bool attr_set[2] = {false, false};
   auto kern = pairwise_chunks<T>;
-  if (!attr_set[sizeof(T) == 8]) {
-    GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    attr_set[sizeof(T) == 8] = true;
-  }
+  GC_TRY(kernel_setup(kern, kSumThreads, smem));
   const long long grid = std::min<long long>(plan.nchunks, static_cast<long long>(ctx->num_sms) * 3);
   kern<<<static_cast<unsigned>(grid), kSumThreads, smem, ctx->stream>>>(x, n, plan.depth, plan.nchunks, a);
   GC_CHECK_LAUNCH("pairwise_chunks");

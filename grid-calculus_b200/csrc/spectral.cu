@@ -31,17 +31,32 @@ struct PlanKey {
   }
 };
 
-std::mutex g_plan_mu;
-std::map<PlanKey, cufftHandle> g_plans;  // plans live for the process
+// The plans of one context.  A context is driven by one host thread at a time
+// and runs everything on its own stream, so its plans need no lock, are bound
+// to that stream once, and their work areas are never shared with another
+// context's transforms.
+struct PlanCache {
+  std::map<PlanKey, cufftHandle> plans;
+};
+
+void release_plans(void* p) {
+  auto* cache = static_cast<PlanCache*>(p);
+  for (auto& kv : cache->plans) cufftDestroy(kv.second);
+  delete cache;
+}
 
 // A D2Z (inverse = 0) or Z2D plan over the grid, `batch` fields laid out
 // back to back.  Axes y and z of extent 1 are dropped from the rank; x is
 // always the transformed-to-half axis.
 gc_status plan_for(gc_context* ctx, const gc_grid* g, int batch, int inverse, cufftHandle* out) {
-  std::lock_guard<std::mutex> lock(g_plan_mu);
+  if (!ctx->spectral_plans) {
+    ctx->spectral_plans = new PlanCache;
+    ctx->spectral_release = release_plans;
+  }
+  auto& plans = static_cast<PlanCache*>(ctx->spectral_plans)->plans;
   const PlanKey key{ctx->device, g->nx, g->ny, g->nz, batch, inverse};
-  auto it = g_plans.find(key);
-  if (it == g_plans.end()) {
+  auto it = plans.find(key);
+  if (it == plans.end()) {
     int n[3];
     int rank = 0;
     if (g->nz > 1) n[rank++] = g->nz;
@@ -60,9 +75,12 @@ gc_status plan_for(gc_context* ctx, const gc_grid* g, int batch, int inverse, cu
       return fail(GC_ERR_CUDA, "spectral: cuFFT plan for " + std::to_string(g->nx) + "x" + std::to_string(g->ny) +
                                    "x" + std::to_string(g->nz) + " failed (" + std::to_string(static_cast<int>(r)) + ")");
     }
-    it = g_plans.emplace(key, h).first;
+    if (cufftSetStream(h, ctx->stream) != CUFFT_SUCCESS) {
+      cufftDestroy(h);
+      return fail(GC_ERR_CUDA, "spectral: cufftSetStream failed");
+    }
+    it = plans.emplace(key, h).first;
   }
-  if (cufftSetStream(it->second, ctx->stream) != CUFFT_SUCCESS) return fail(GC_ERR_CUDA, "spectral: cufftSetStream failed");
   *out = it->second;
   return GC_OK;
 }

@@ -390,12 +390,7 @@ gc_status launch_zring(gc_context* ctx, const OpParams<T>& p0) {
   p.zc = div_up(p.nz, chunks);
   chunks = div_up(p.nz, p.zc);
   auto kern = zring_kernel<T, OP, ORDER>;
-  static bool attr = false;
-  if (!attr) {
-    if (smem > 48 * 1024)
-      GC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    attr = true;
-  }
+  GC_TRY(kernel_setup(kern, BX * BY, smem));
   dim3 grid(tiles_x, tiles_y, chunks), block(BX, BY);
   kern<<<grid, block, smem, ctx->stream>>>(p);
   GC_CHECK_LAUNCH("zring_kernel");

@@ -165,7 +165,9 @@ GC_API gc_status gc_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, co
  * field to 2^29 cells (larger fields get GC_ERR_INVALID_ARG).  All calls
  * share that array: calls that overlap on the GPU race, so keep them on one
  * stream.  The first call on each device (with that device current) looks
- * up the array's device address; make it before any stream capture. */
+ * up the array's device address and keeps it for the life of the process;
+ * make it before any stream capture, and do not reset the device
+ * (cudaDeviceReset) after it, since the kept address would then be stale. */
 GC_API gc_status gc_integrate_noalloc(const gc_grid* g, gc_dtype dt, const void* in,
                                       double* result_dev, void* stream);
 

@@ -123,3 +123,28 @@ def test_rejections(gc):
         gc.spectral_laplacian(torch.zeros((8, 8, 1), device="cuda", dtype=torch.float64), gc.Grid(1, 8, 8))
     with pytest.raises(ValueError, match="0..8"):
         gc.spectral_partial(torch.zeros((8, 8, 8), device="cuda", dtype=torch.float64), g, (9, 0, 0))
+
+
+def test_two_contexts_on_two_streams_same_shape(gc):
+    """Each context keeps its own FFT plans bound to its own stream: two
+    contexts transforming the same shape at the same time, on two streams,
+    give exactly what one context gives alone (shared plans would let one
+    context's transform run on the other's stream and share its work area)."""
+    import torch
+    n = 96
+    g = gc.Grid(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n)
+    rng = np.random.default_rng(3)
+    fields = [_dev(rng.standard_normal((n, n, n))) for _ in range(2)]
+    want = [_host(gc.spectral_laplacian(f, g)) for f in fields]
+    streams = [torch.cuda.Stream() for _ in range(2)]
+    ctxs = [gc.Context(0, s.cuda_stream) for s in streams]
+    outs = [torch.empty_like(f) for f in fields]
+    for rep in range(4):
+        for j in range(2):
+            with torch.cuda.stream(streams[j]):
+                gc.spectral_laplacian(fields[j], g, out=outs[j], ctx=ctxs[j])
+        torch.cuda.synchronize()
+        for j in range(2):
+            assert np.array_equal(outs[j].cpu().numpy(), want[j]), (rep, j)
+    for c in ctxs:
+        c.close()

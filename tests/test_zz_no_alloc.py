@@ -48,6 +48,33 @@ def test_noalloc_matches_integrate_twice(gc):
     assert torch.cuda.mem_get_info()[0] == free_before
 
 
+def test_noalloc_back_to_back_on_one_stream(gc):
+    """The usage the header prescribes: calls queued one after another on one
+    (non-default) stream, with no host wait between them, each reusing the
+    shared array; every result lands in its own element and all equal
+    gc_integrate bit for bit after one synchronize."""
+    import torch
+    f = _bind(gc)
+    rng = np.random.default_rng(6)
+    cases = [(gc.Grid(300, 200, 7), torch.float64), (gc.Grid(4096, 4096, 1), torch.float64),
+             (gc.Grid(77, 1, 1), torch.float32)]
+    inputs = [torch.from_numpy(rng.standard_normal(g.shape)).to("cuda", dt) for g, dt in cases]
+    want = [gc.integrate(x, g) for x, (g, _) in zip(inputs, cases)]
+    side = torch.cuda.Stream()
+    results = torch.full((6,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        for rep in range(2):
+            for k, (x, (g, dt)) in enumerate(zip(inputs, cases)):
+                code = 0 if dt == torch.float64 else 1
+                ptr = results.data_ptr() + 8 * (3 * rep + k)
+                assert f(C.byref(g.c()), code, x.data_ptr(), ptr, side.cuda_stream) == 0, \
+                    gc.lib.gc_last_error().decode()
+    side.synchronize()
+    got = results.cpu().tolist()
+    assert got == want + want, (got, want)
+
+
 def test_noalloc_rejects_oversized_field(gc):
     import torch
     f = _bind(gc)
