@@ -854,6 +854,11 @@ gc_status enqueue_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp
 template <class T>
 gc_status integrate_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, T* psi,
                       double dt, int n_steps, gc_integrator integ) {
+  if (ctx->cluster_stepping && g->nz == 1) {
+    bool done = false;
+    GC_TRY(ch_cluster_integrate(ctx, g, sizeof(T) == 8 ? GC_F64 : GC_F32, cp, psi, dt, n_steps, integ, &done));
+    if (done) return GC_OK;
+  }
   const size_t n = cells(g);
   const size_t bytes = n * sizeof(T);
   void *vb = nullptr, *v1 = nullptr, *v2 = nullptr, *v3 = nullptr;

@@ -73,6 +73,8 @@ struct gc_context {
   // released by gc_context_destroy through spectral_release.
   void* spectral_plans = nullptr;
   void (*spectral_release)(void*) = nullptr;
+  // gc_context_set_option switches.
+  bool cluster_stepping = true;
 };
 
 namespace gcb {
@@ -97,6 +99,12 @@ gc_status require_axes(const gc_grid* g, int radius);
 // Per-axis radii (an axis with radius 0 accepts any extent).
 gc_status require_axes3(const gc_grid* g, int rx, int ry, int rz);
 gc_status check_ctx(gc_context* ctx);
+
+// Whole-integration fast path for 2-D grids whose state fits in one
+// thread-block cluster's shared memory (ch_cluster.cu): *done reports whether
+// it ran (false: the grid does not fit, take the multi-launch path).
+gc_status ch_cluster_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
+                               double dt_step, int n_steps, gc_integrator integ, bool* done);
 
 // Opts kernel `kern` into `smem` bytes of dynamic shared memory on the
 // current device and, with ctas_per_sm, returns how many CTAs of `threads`

@@ -195,6 +195,14 @@ GC_API gc_status gc_context_create(gc_context** out, int device, void* stream) {
   return GC_OK;
 }
 
+GC_API gc_status gc_context_set_option(gc_context* ctx, int32_t option, int32_t value) {
+  if (!ctx) return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: null context");
+  switch (option) {
+    case GC_OPT_CLUSTER_STEPPING: ctx->cluster_stepping = value != 0; return GC_OK;
+  }
+  return fail(GC_ERR_INVALID_ARG, "gc_context_set_option: unknown option " + std::to_string(option));
+}
+
 GC_API gc_status gc_context_destroy(gc_context* ctx) {
   if (!ctx) return GC_OK;
   cudaSetDevice(ctx->device);

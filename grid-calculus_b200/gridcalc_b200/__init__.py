@@ -171,6 +171,11 @@ class Grid:
         return gc_grid(self.nx, self.ny, self.nz, self.hx, self.hy, self.hz)
 
 
+OPT_CLUSTER_STEPPING = 0
+lib.gc_context_set_option.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+lib.gc_context_set_option.restype = C.c_int
+
+
 class Context:
     """A gc_context: one CUDA stream plus cached scratch and graphs."""
 
@@ -182,6 +187,11 @@ class Context:
 
     def synchronize(self) -> None:
         _check(lib.gc_synchronize(self.handle))
+
+    def set_cluster_stepping(self, enabled: bool) -> None:
+        """GC_OPT_CLUSTER_STEPPING: small 2-D grids advance in one
+        cluster-resident launch (default) or through the per-stage kernels."""
+        _check(lib.gc_context_set_option(self.handle, OPT_CLUSTER_STEPPING, int(bool(enabled))))
 
     def close(self) -> None:
         if self.handle:
@@ -249,6 +259,16 @@ def _dtype_code(t) -> int:
     if t.dtype == torch.float32:
         return F32
     raise ValueError(f"gridcalc_b200: fields must be float64 or float32, got {t.dtype}")
+
+
+def _dtype_code_of(dtype) -> int:
+    """The gc_dtype code of a torch dtype."""
+    import torch
+    if dtype == torch.float64:
+        return F64
+    if dtype == torch.float32:
+        return F32
+    raise ValueError(f"gridcalc_b200: fields must be float64 or float32, got {dtype}")
 
 
 def _require(t, grid: Grid, comps: int = 1):
@@ -488,6 +508,16 @@ def ch_rkc(psi, grid: Grid, rhs: CahnHilliardRhs, dt: float, n_steps: int, stage
 def rkc_stability_bound(stages: int) -> float:
     """beta(s): RKC2 is stable for dt * lambda_max <= beta(s)."""
     return lib.gc_rkc_stability_bound(stages)
+
+
+lib.gc_ch_cluster_ctas.argtypes = [C.POINTER(gc_grid), C.c_int, C.c_int32, C.c_int]
+lib.gc_ch_cluster_ctas.restype = C.c_int32
+
+
+def ch_cluster_ctas(grid: Grid, dtype, order: int, tag=RK4) -> int:
+    """CTAs of the cluster-resident launch ch_integrate uses for this grid
+    (0: the grid does not fit; the per-stage kernels run)."""
+    return lib.gc_ch_cluster_ctas(C.byref(grid.c()), _dtype_code_of(dtype), order, tag.code)
 
 
 def ch_integrate(psi, grid: Grid, rhs: CahnHilliardRhs, dt: float, n_steps: int, tag=RK4, ctx=None):

@@ -87,6 +87,14 @@ typedef struct gc_context gc_context;
  * reduction partials, captured graphs). */
 GC_API gc_status gc_context_create(gc_context** out, int device, void* stream);
 GC_API gc_status gc_context_destroy(gc_context* ctx);
+/* Context switches (no reference counterpart).
+ *   GC_OPT_CLUSTER_STEPPING (default 1): gc_ch_integrate advances a 2-D grid
+ *     whose whole state fits in the shared memory of one thread-block
+ *     cluster (up to 16 CTAs; about 240 x 240 doubles with RK4) in a single
+ *     cluster-resident launch for all its steps; 0 always uses the per-stage
+ *     kernels.  Both give the same values (bit for bit in double). */
+typedef enum gc_option { GC_OPT_CLUSTER_STEPPING = 0 } gc_option;
+GC_API gc_status gc_context_set_option(gc_context* ctx, int32_t option, int32_t value);
 GC_API gc_status gc_synchronize(gc_context* ctx);
 /* Failure-detection self-test (no reference counterpart): launches one
  * thread that waits on a device flag nothing sets, gives up after
@@ -286,10 +294,17 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt,
  * (solve/RK4.hpp:99-154, solve/ExplicitEuler.hpp:79-112) with the
  * Cahn-Hilliard RHS, psi advanced in place.  RK4 runs four fused stage
  * kernels per step (each reads and writes every field once); the steps are
- * replayed from a captured CUDA graph. */
+ * replayed from a captured CUDA graph.  A 2-D grid whose state fits in one
+ * thread-block cluster's shared memory (gc_ch_cluster_ctas > 0) instead runs
+ * all n_steps in one cluster-resident launch (GC_OPT_CLUSTER_STEPPING). */
 GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
                                  const gc_ch_params* p, void* psi, double dt_step,
                                  int n_steps, gc_integrator integrator);
+/* CTAs of the cluster that gc_ch_integrate uses for this 2-D grid, storage
+ * type, Laplacian order and integrator (one slab of rows per CTA, the
+ * slab's psi, stage fields and halos in that CTA's shared memory); 0 when
+ * the state does not fit and the per-stage kernels run.  No GPU work. */
+GC_API int32_t gc_ch_cluster_ctas(const gc_grid* g, gc_dtype dt, int32_t order, gc_integrator integrator);
 
 /* RKC2 (damped second-order Runge-Kutta-Chebyshev, eps = 2/13) with
  * `stages` stages (2..64): n_steps steps of dt_step, psi in place, same RHS

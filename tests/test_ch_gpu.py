@@ -13,6 +13,16 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True, params=["cluster", "stages"])
+def stepping_path(request, gc):
+    """Every test runs twice: with small 2-D grids in one cluster-resident
+    launch (the default) and with the per-stage kernels forced."""
+    ctx = gc.context()
+    ctx.set_cluster_stepping(request.param == "cluster")
+    yield request.param
+    ctx.set_cluster_stepping(True)
+
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.npz")
 
 
