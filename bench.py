@@ -518,20 +518,25 @@ def form_config1(gc, steps=2000, every=100):
 
 
 def form_learned(gc, n_train=32, n_eval=4, fine_steps=5000, t_end=200.0, tols=(0.003, 0.01, 0.03), log=None):
+    """Trains the corrector on n_train trajectories and evaluates it on
+    n_eval held-out seeds to t_end (the configured workload: 512 and 64)."""
     import gridcalc_b200.learned as L
     size, batch = 512, 16
     net = L.new_corrector(size, batch, seed=0)
     base_only = L.new_corrector(size, 1, zero=True)
     tr = L.train(net, range(1000, 1000 + n_train), size=size, fine_steps=fine_steps, batch=batch, log=log)
     prof = L.residual_profile(net, range(1000, 1002), size=size)
-    schemes = [(f"learned_tol{t:g}", net, t) for t in tols] + [(f"base_only_tol{t:g}", base_only, t) for t in tols]
+    # The network's rejected steps try the base step alone before plain RK4;
+    # the base-only scheme (all-zero network: its proposal is the base step)
+    # goes straight to plain RK4.
+    schemes = ([(f"learned_tol{t:g}", net, t, True) for t in tols] +
+               [(f"base_only_tol{t:g}", base_only, t, False) for t in tols])
     ev = L.evaluate_heldout(schemes, range(9000, 9000 + n_eval), size=size, t_end=t_end)
     net.close()
     base_only.close()
     return {"workload": "learned coarse step (dt 0.16 = 16 fine RK4 steps: one 6-stage RKC2 step + the CNN's "
                         "correction) on 512^2 CH, kappa = M = 1",
-            "budget": f"{n_train} training trajectories x {fine_steps} fine steps, {n_eval} held-out seeds to t = {t_end} "
-                      "(the full configuration uses 512 and 64)",
+            "budget": f"{n_train} training trajectories x {fine_steps} fine steps, {n_eval} held-out seeds to t = {t_end}",
             "train": tr, "residual_profile": prof["rows"], "eval": ev}
 
 
@@ -638,6 +643,7 @@ def form_summary(name: str, r: dict) -> dict:
         out = {"trajectories": r["train"]["trajectories"], "heldout_seeds": r["eval"]["seeds"]}
         for nm, v in r["eval"]["schemes"].items():
             out[nm] = _sig({"speedup": v["speedup_vs_plain"], "fallback_rate": v["fallback_rate"],
+                            "base_steps": v.get("accepted_base", 0),
                             "l2_max": v["l2_err_max"], "f_err_max": v["f_err_max"]}, 3)
         return out
     if name == "snapshots":
@@ -650,9 +656,11 @@ def run_forms(gc, names, peak):
     ({"form": name, ...}) and returns the short summaries for the headline."""
     table = {"operators": lambda: form_operators(gc, peak), "fvm": lambda: form_fvm(gc, peak),
              "snapshots": lambda: form_snapshots(gc), "config1": lambda: form_config1(gc),
-             "batched": lambda: form_batched(gc, peak), "learned": lambda: form_learned(gc),
-             # the learned workload at its full size: 512 training trajectories, 64 held-out seeds
-             "learned_full": lambda: form_learned(gc, n_train=512, n_eval=64, tols=(0.003, 0.01))}
+             "batched": lambda: form_batched(gc, peak),
+             # the learned workload at its configured size: 512 training trajectories, 64 held-out seeds
+             "learned": lambda: form_learned(gc, n_train=512, n_eval=64, tols=(0.003, 0.01)),
+             # a reduced budget for quick checks: 32 trajectories, 4 held-out seeds
+             "learned_small": lambda: form_learned(gc)}
     summaries = {}
     for nm in names:
         t0 = time.perf_counter()
@@ -725,6 +733,11 @@ def run_case(name: str) -> None:
         g = gc.Grid(n, n, 1)
         x = (0.05 * (2 * torch.rand(1, n, n, device="cuda", dtype=torch.float64) - 1)).float()
         gc.ch_integrate(x, g, gc.CahnHilliardRhs(1.0, 1.0, 2), DT, 32, gc.RK4)
+    elif name == "fused_4096":      # fused RK4 step kernel, 4096^2 FP64 order 2 (one launch per step)
+        n = 4096
+        g = gc.Grid(n, n, 1)
+        x = 0.05 * (2 * torch.rand(1, n, n, device="cuda", dtype=torch.float64) - 1)
+        gc.ch_integrate(x, g, gc.CahnHilliardRhs(1.0, 1.0, 2), DT, 3, gc.RK4)
     elif name == "eval_fe_320":     # func::evaluate of the recorded free energy, 320^3 FP64 (fused NVRTC kernel)
         n = 320
         g = gc.Grid(n, n, n, 1 / n, 1 / n, 1 / n)
@@ -884,12 +897,13 @@ def main():
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--case", default=None,
                     help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
-                         "batch64_f32, ch_f32_4096, eval_fe_320")
+                         "batch64_f32, ch_f32_4096, fused_4096, eval_fe_320")
     ap.add_argument("--min-seconds", type=float, default=1.5,
                     help="repeat the K-step timed block until this much device time has passed")
     ap.add_argument("--forms", default="all",
-                    help="'all', 'headline' or a comma list of operators,fvm,batched,learned,learned_full,snapshots "
-                         "(learned_full: 512 training trajectories and 64 held-out seeds; minutes)")
+                    help="'all', 'headline' or a comma list of config1,operators,fvm,batched,learned,learned_small,"
+                         "snapshots (learned: 512 training trajectories and 64 held-out seeds, minutes; "
+                         "learned_small: 32 and 4)")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.case:

@@ -828,6 +828,13 @@ StageParams<T> base_params(const gc_grid* g, const gc_ch_params* cp) {
 template <class T>
 gc_status enqueue_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const T* src,
                        T* dst, T* k1, T* k2, T* k3, double dt, gc_integrator integ) {
+  if constexpr (sizeof(T) == 8) {
+    if (integ == GC_RK4 && ctx->fused_step) {
+      bool done = false;
+      GC_TRY(ch_fused_step(ctx, g, cp, src, dst, dt, &done));
+      if (done) return GC_OK;
+    }
+  }
   StageParams<T> p = base_params<T>(g, cp);
   p.psi = src;
   const int order = cp->order;
@@ -881,7 +888,7 @@ gc_status integrate_t(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp,
                            bits_of(cp->mobility),
                            bits_of(cp->kappa),
                            (static_cast<uint64_t>(cp->order) << 8) | (static_cast<uint64_t>(integ) << 4) |
-                               (sizeof(T) == 8 ? 1u : 2u) | (0xC4ULL << 56)};
+                               (sizeof(T) == 8 ? 1u : 2u) | (ctx->fused_step ? 1ULL << 16 : 0) | (0xC4ULL << 56)};
   return run_steps<T>(ctx, psi, pb, bytes, n_steps, key, [&](const T* src, T* dst) {
     return enqueue_step<T>(ctx, g, cp, src, dst, k1, k2, k3, dt, integ);
   });

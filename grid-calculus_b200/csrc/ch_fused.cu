@@ -1,0 +1,241 @@
+// Fused RK4 step for 2-D double Cahn-Hilliard at Laplacian order 2: all
+// four stages of one step in one kernel, with psi read from and psi' written
+// to HBM once.
+//
+// solve::integrate(psi, computeRhs, dt, n, RK4{}) (solve/RK4.hpp:99-154,
+// examples/common/cahn_hilliard.hpp:38-59):
+//   k1 = f(psi), k2 = f(psi + dt/2 k1), k3 = f(psi + dt/2 k2),
+//   k4 = f(psi + dt k3), psi' = psi + (dt/6 (k1 + k4) + dt/3 (k2 + k3)),
+//   f(y) = M lap(mu), mu = -y + y^3 - kappa lap(y).
+// The stage kernels (ch.cu) move 13 field passes per step through HBM and
+// are bound by it.  Here a persistent CTA owns a TX x TY output tile and
+// stages psi on the tile plus a halo of H = 8R cells (R = 1, the stencil
+// radius): each stage's f needs its input y on 2R more cells than it
+// produces, so stage s produces k_s on a halo of H - 2R s and the last
+// stage exactly the tile.  Per stage, in shared memory:
+//   mu pass  mu = -y + y^3 - kappa lap(y) on halo H - 2R s + R
+//            (y = psi in stage 1, else the y buffer)
+//   k pass   k = M lap(mu) on halo H - 2R s; y of the next stage
+//            (psi + dt/2 k, psi + dt/2 k, psi + dt k) overwrites the y
+//            buffer; on the tile k1 is kept, k2 kept and then replaced by
+//            k2 + k3, and stage 4 writes psi' to global memory.
+// HBM traffic per step is psi once (the halo's overlap with neighbouring
+// tiles comes from L2) and psi' once: 16 B per cell instead of 104.  The
+// price is the halo's extra arithmetic (about 1.4x at 64 x 28 tiles): the
+// kernel is bound by the FP64 pipe and shared memory, not by HBM.
+//
+// Interior tiles arrive by one TMA box (x offset a multiple of 8 doubles);
+// tiles touching the grid edge load their wrapped frame with plain loads.
+// The next tile's box is prefetched into L2 while this one computes.  Every
+// operation is the stage kernels' (tap_sum, lap_xy, chem_pot, mobility,
+// the same RK4 combination), so results are bit-identical to them and to
+// the CPU reference.  The single TMA wait is bounded: on expiry the CTA
+// records GC_ERR_TIMEOUT in the context's status word and leaves.
+#include <algorithm>
+
+#include "ch_tile.cuh"
+#include "common.cuh"
+#include "tma.cuh"
+
+namespace gcb {
+namespace {
+
+constexpr int kFzThreads = 512;
+constexpr int kFzWarps = kFzThreads / 32;
+constexpr long long kFzWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
+constexpr size_t kFzMaxCells = size_t(2048) * 2048;  // larger grids take the stage kernels
+
+constexpr size_t fz_al(size_t b) { return (b + 127) / 128 * 128; }
+
+struct FzLayout {
+  static constexpr int R = 1;
+  static constexpr int H = 8 * R;         // four stages x 2R
+  static constexpr int TX = 64, TY = 28;  // output tile
+  static constexpr int SX = TX + 2 * H;   // frame row (80 doubles, 640 B)
+  static constexpr int SY = TY + 2 * H;   // frame rows
+  static constexpr int YR0 = 2 * R;       // first frame row the y buffer holds (halo 6R)
+  static constexpr int YROWS = SY - 2 * YR0;
+  static constexpr int MR0 = R;           // first frame row the mu buffer holds (halo 7R)
+  static constexpr int MROWS = SY - 2 * MR0;
+  static constexpr size_t OFF_PSI = 128;  // after the mbarrier
+  static constexpr size_t OFF_Y = OFF_PSI + fz_al(sizeof(double) * SX * SY);
+  static constexpr size_t OFF_MU = OFF_Y + fz_al(sizeof(double) * SX * YROWS);
+  static constexpr size_t OFF_K1 = OFF_MU + fz_al(sizeof(double) * SX * MROWS);
+  static constexpr size_t OFF_K23 = OFF_K1 + fz_al(sizeof(double) * TX * TY);
+  static constexpr size_t BYTES = OFF_K23 + fz_al(sizeof(double) * TX * TY) + 128;  // + alignment slack
+  static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(double) * SX * SY);
+};
+static_assert(FzLayout::BYTES <= 113 * 1024, "two CTAs per SM");
+static_assert((FzLayout::SX * 8) % 16 == 0 && FzLayout::H % 2 == 0, "TMA box rows and x offsets stay 16-byte multiples");
+
+struct FzParams {
+  StageParams<double> p;   // RHS constants, nx, ny
+  const double* psi;       // state in
+  double* out;             // state out (another buffer)
+  double half_dt, dt, c6, c3;
+  int tiles_x, tiles_y;
+};
+
+// Calls f(r, c) for the frame cells of rows [r0, r1) x columns [c0, c1):
+// warps over rows, lanes over columns.
+template <class F>
+__device__ __forceinline__ void fz_region(int r0, int r1, int c0, int c1, F&& f) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = r0 + warp; r < r1; r += kFzWarps)
+    for (int c = c0 + lane; c < c1; c += 32) f(r, c);
+}
+
+__global__ void __launch_bounds__(kFzThreads, 2)
+    ch_fused_rk4_kernel(const FzParams a, const __grid_constant__ CUtensorMap m_psi, int* status) {
+  using L = FzLayout;
+  using T = double;
+  constexpr int R = L::R, H = L::H, TX = L::TX, TY = L::TY, SX = L::SX, SY = L::SY;
+  const StageParams<T>& p = a.p;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+  int* s_abort = reinterpret_cast<int*>(base + 64);
+  T* ps = reinterpret_cast<T*>(base + L::OFF_PSI);
+  T* ys = reinterpret_cast<T*>(base + L::OFF_Y);
+  T* ms = reinterpret_cast<T*>(base + L::OFF_MU);
+  T* k1s = reinterpret_cast<T*>(base + L::OFF_K1);
+  T* k23s = reinterpret_cast<T*>(base + L::OFF_K23);
+  const int nx = p.nx, ny = p.ny, tid = threadIdx.x;
+  const int ntiles = a.tiles_x * a.tiles_y;
+
+  auto origin = [&](int tl, int& x0, int& y0) {
+    x0 = (tl % a.tiles_x) * TX;
+    y0 = (tl / a.tiles_x) * TY;
+  };
+  auto interior = [&](int x0, int y0) { return x0 - H >= 0 && x0 - H + SX <= nx && y0 - H >= 0 && y0 - H + SY <= ny; };
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    *s_abort = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  uint32_t phase = 0;
+  for (int tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    int x0, y0;
+    origin(tl, x0, y0);
+    const bool in = interior(x0, y0);
+    if (tid == 0) {
+      const int next = tl + static_cast<int>(gridDim.x);
+      if (in) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, L::TX_BYTES);
+        tma_load_2d(ps, &m_psi, x0 - H, y0 - H, bar);
+      }
+      if (next < ntiles) {
+        int nx0, ny0;
+        origin(next, nx0, ny0);
+        if (interior(nx0, ny0)) tma_prefetch_2d(&m_psi, nx0 - H, ny0 - H);
+      }
+    }
+    if (in) {
+      const long long t0 = clock64();
+      while (!mbar_try_wait(bar, phase)) {
+        if (clock64() - t0 > kFzWaitCycles) {
+          *s_abort = 1;
+          atomicExch(status, static_cast<int>(GC_ERR_TIMEOUT));
+          break;
+        }
+      }
+      phase ^= 1u;
+    } else {
+      for (int e = tid; e < SX * SY; e += kFzThreads) {
+        const int r = e / SX, c = e - r * SX;
+        ps[e] = __ldg(a.psi + static_cast<size_t>(wrap(y0 - H + r, ny)) * nx + wrap(x0 - H + c, nx));
+      }
+    }
+    __syncthreads();
+    if (*s_abort) break;
+
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+      // Halos: y_s on hy, mu on hy - R, k_s on hy - 2R.
+      const int hy = H - 2 * R * s;
+      const int hm = hy - R, hk = hy - 2 * R;
+      // mu pass.
+      fz_region(H - hm, H + TY + hm, H - hm, H + TX + hm, [&](int r, int c) {
+        const T* yr = s == 0 ? ps + r * SX : ys + (r - L::YR0) * SX;
+        const T yc = yr[c];
+        const T ax = tap_sum<T, 2, 2>([&](int o) { return o == 0 ? yc : yr[c + o]; });
+        const T ay = tap_sum<T, 2, 2>([&](int o) { return yr[o * SX + c]; });
+        ms[(r - L::MR0) * SX + c] = chem_pot(p, yc, lap_xy(p, ax, ay));
+      });
+      __syncthreads();
+      // k pass and the stage's update.
+      fz_region(H - hk, H + TY + hk, H - hk, H + TX + hk, [&](int r, int c) {
+        const T* mr = ms + (r - L::MR0) * SX;
+        const T mc = mr[c];
+        const T ax = tap_sum<T, 2, 2>([&](int o) { return o == 0 ? mc : mr[c + o]; });
+        const T ay = tap_sum<T, 2, 2>([&](int o) { return mr[o * SX + c]; });
+        const T rhs = mobility(p, lap_xy(p, ax, ay));
+        const T pc = ps[r * SX + c];
+        if (s < 3) ys[(r - L::YR0) * SX + c] = Ar<T>::add(pc, Ar<T>::mul(s < 2 ? a.half_dt : a.dt, rhs));
+        const int tr = r - H, tc = c - H;
+        if (tr >= 0 && tr < TY && tc >= 0 && tc < TX) {
+          const int t = tr * TX + tc;
+          if (s == 0) {
+            k1s[t] = rhs;
+          } else if (s == 1) {
+            k23s[t] = rhs;
+          } else if (s == 2) {
+            k23s[t] = Ar<T>::add(k23s[t], rhs);
+          } else if (y0 + tr < ny && x0 + tc < nx) {
+            const T s14 = Ar<T>::add(k1s[t], rhs);
+            a.out[static_cast<size_t>(y0 + tr) * nx + (x0 + tc)] =
+                Ar<T>::add(pc, Ar<T>::add(Ar<T>::mul(a.c6, s14), Ar<T>::mul(a.c3, k23s[t])));
+          }
+        }
+      });
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const double* src, double* dst,
+                        double dt, bool* done) {
+  using L = FzLayout;
+  *done = false;
+  if (g->nz != 1 || cp->order != 2 || g->nx < L::SX || g->ny < L::SY) return GC_OK;
+  // Measured on B200 per RK4 step (fused / four stage kernels): 256^2 13.8 /
+  // 23.3 us, 1024^2 34.4 / 47.0, 2048^2 128 / 131, 4096^2 503 / 426, 8192^2
+  // 1951 / 1562: the stage kernels win once the grid fills the GPU.
+  if (cells(g) > kFzMaxCells) return GC_OK;
+  CUtensorMap m{};
+  if (!make_tensor_map_2d(&m, src, g->nx, g->ny, 8, L::SX, L::SY)) return GC_OK;
+  FzParams a{};
+  StageParams<double>& p = a.p;
+  p.nx = g->nx; p.ny = g->ny; p.nz = 1;
+  p.ihx2 = 1.0 / (g->hx * g->hx);
+  p.ihy2 = 1.0 / (g->hy * g->hy);
+  p.ihz2 = 1.0 / (g->hz * g->hz);
+  p.mob = cp->mobility;
+  p.kappa = cp->kappa;
+  p.unit_h = p.ihx2 == 1.0 && p.ihy2 == 1.0 && p.ihz2 == 1.0;
+  p.unit_m = p.mob == 1.0;
+  p.unit_k = p.kappa == 1.0;
+  a.psi = src;
+  a.out = dst;
+  a.half_dt = 0.5 * dt;
+  a.dt = dt;
+  a.c6 = dt / 6.0;
+  a.c3 = dt / 3.0;
+  a.tiles_x = div_up(g->nx, L::TX);
+  a.tiles_y = div_up(g->ny, L::TY);
+  int per_sm = 1;
+  GC_TRY(kernel_setup(ch_fused_rk4_kernel, kFzThreads, L::BYTES, &per_sm));
+  const long long ntiles = static_cast<long long>(a.tiles_x) * a.tiles_y;
+  const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(per_sm) * ctx->num_sms));
+  ch_fused_rk4_kernel<<<grid, kFzThreads, L::BYTES, ctx->stream>>>(a, m, ctx->device_status);
+  GC_CHECK_LAUNCH("ch_fused_rk4_kernel");
+  *done = true;
+  return GC_OK;
+}
+
+}  // namespace gcb

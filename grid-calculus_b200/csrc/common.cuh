@@ -75,6 +75,7 @@ struct gc_context {
   void (*spectral_release)(void*) = nullptr;
   // gc_context_set_option switches.
   bool cluster_stepping = true;
+  bool fused_step = true;
 };
 
 namespace gcb {
@@ -105,6 +106,12 @@ gc_status check_ctx(gc_context* ctx);
 // it ran (false: the grid does not fit, take the multi-launch path).
 gc_status ch_cluster_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, const gc_ch_params* cp, void* psi,
                                double dt_step, int n_steps, gc_integrator integ, bool* done);
+
+// One RK4 step of a 2-D double grid at order 2 in one fused kernel
+// (ch_fused.cu), src -> dst; *done reports whether it ran (false: the grid
+// or its layout does not suit it, use the stage kernels).
+gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const double* src, double* dst,
+                        double dt, bool* done);
 
 // Opts kernel `kern` into `smem` bytes of dynamic shared memory on the
 // current device and, with ctas_per_sm, returns how many CTAs of `threads`

@@ -199,6 +199,7 @@ GC_API gc_status gc_context_set_option(gc_context* ctx, int32_t option, int32_t 
   if (!ctx) return fail(GC_ERR_INVALID_ARG, "gridcalc_b200: null context");
   switch (option) {
     case GC_OPT_CLUSTER_STEPPING: ctx->cluster_stepping = value != 0; return GC_OK;
+    case GC_OPT_FUSED_STEP: ctx->fused_step = value != 0; return GC_OK;
   }
   return fail(GC_ERR_INVALID_ARG, "gc_context_set_option: unknown option " + std::to_string(option));
 }

@@ -1179,6 +1179,25 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
   GC_TRY(read_stats());
   double F0 = sums[0];
   gc_corrector_stats sres{};
+  // The base step alone, B(psi) (left in bbuf by the proposal), under the
+  // same test; taken when it passes.  F0 is updated on success.
+  gc_status base_st = GC_OK;
+  auto tried_base = [&](double& f0) -> bool {
+    if ((base_st = ch_rhs_enqueue(ctx, g, GC_F64, cp, c->bbuf, f1)) != GC_OK) return false;
+    if ((base_st = stats_enqueue(psi, c->bbuf)) != GC_OK) return false;
+    if ((base_st = read_stats()) != GC_OK) return false;
+    const double Fb = sums[0];
+    const double rb = sums[2] > 0.0 ? std::sqrt(sums[1] / sums[2]) : 0.0;
+    if (Fb <= f0 + (pol->energy_tol + pol->energy_rtol * std::fabs(f0)) && rb <= pol->residual_tol) {
+      if (cudaMemcpyAsync(psi, c->bbuf, sizeof(double) * n, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+        base_st = cuda_fail(cudaGetLastError(), "gc_corrector_advance: base step copy");
+        return false;
+      }
+      f0 = Fb;
+      return true;
+    }
+    return false;
+  };
   for (int k = 0; k < n_coarse; ++k) {
     GC_TRY(corr_layout(c));
     if (c->prop_exec && std::memcmp(key, c->prop_key, sizeof(key)) == 0) {
@@ -1222,20 +1241,25 @@ GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const g
       GC_CUDA(cudaMemcpyAsync(psi, cand, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
       F0 = F1;
       ++sres.accepted;
+    } else if (pol->try_base && c->base && tried_base(F0)) {
+      ++sres.accepted_base;
     } else {
       if ((s = gc_ch_integrate(ctx, g, GC_F64, cp, psi, pol->dt_fine, pol->fine_per_coarse, GC_RK4)) != GC_OK)
         return s;
+      if (base_st != GC_OK) return base_st;
       GC_TRY(stats_enqueue(nullptr, psi));
       GC_TRY(read_stats());
       F0 = sums[0];
       ++sres.fallbacks;
     }
+    if (base_st != GC_OK) return base_st;
   }
   if (stats) {
     stats->accepted += sres.accepted;
     stats->fallbacks += sres.fallbacks;
     stats->rejected_energy += sres.rejected_energy;
     stats->rejected_residual += sres.rejected_residual;
+    stats->accepted_base += sres.accepted_base;
     stats->last_residual = sres.last_residual;
   }
   return GC_OK;

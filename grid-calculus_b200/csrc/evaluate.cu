@@ -38,7 +38,7 @@ namespace gcb {
 namespace {
 
 constexpr int kChunkCells = 8192;   // pairwise chunk bound (pairwise.cuh kChunkMax)
-constexpr int kEvalThreads = 256;
+constexpr int kEvalThreads = 512;
 
 // Kernel argument; the device source declares the same layout.
 struct EvalGrid {
@@ -234,11 +234,16 @@ __device__ __forceinline__ double gc_seq_sum(const double* s, int a, int b) {
   return acc;
 }
 
-extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
-                                                                   double* __restrict__ partial) {
+// 512 threads (16 warps) per CTA.  With the 68.7 KB chunk stage three CTAs fit
+// on an SM (48 warps to hide the neighbour loads' latency) where the program
+// fits in 40 registers: GC_MIN_CTAS is 3 for scalar integrands of arity 1
+// and 2, 2 (64 registers) for vector integrands and 1 (no register cap) for
+// scalar arity 3 and 4, the caps under which the programs do not spill.
+extern "C" __global__ void __launch_bounds__(512, GC_MIN_CTAS) gc_eval_pairwise(const EvalGrid g, int depth, gc_i64 nchunks,
+                                                                      double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* s = (double*)smem_raw;
-  double* ns = s + gc_padpos(8192) + 8;
+  double* ns = s + gc_padpos(8192) + 8;   // 128 half-node sums, then the node tree
   for (gc_i64 c = blockIdx.x; c < nchunks; c += gridDim.x) {
     gc_i64 lo = 0, hi = g.n;
     gc_descend(lo, hi, c, depth);
@@ -246,7 +251,7 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGri
     // Two consecutive cells per thread and iteration.
     int i, j, k;
     gc_locate(g, lo + 2 * threadIdx.x, i, j, k);
-    for (int e = 2 * threadIdx.x; e < len; e += 512) {
+    for (int e = 2 * threadIdx.x; e < len; e += 1024) {
       if (e + 1 < len && i + 1 < g.nx) {
         double a, b;
         gc_cell_pair(g, lo + e, i, j, k, a, b);
@@ -272,20 +277,36 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_pairwise(const EvalGri
     while (((len + (1 << d2) - 1) >> d2) > 128) ++d2;
     const int nodes = 1 << d2;
     __syncthreads();
-    if (threadIdx.x < nodes) {
+    // A leaf node of m <= 128 values is summed in order from 0.0, and one of
+    // m > 64 as its two halves [0, m/2) and [m/2, m) summed that way and then
+    // added: threads 2n and 2n + 1 take node n's halves at the same time.
+    if (threadIdx.x < 2 * nodes) {
+      const int node = threadIdx.x >> 1, half = threadIdx.x & 1;
       gc_i64 a = 0, b = len;
-      gc_descend(a, b, threadIdx.x, d2);
+      gc_descend(a, b, node, d2);
       const int m = (int)(b - a);
-      double v;
+      double v = 0.0;
       if (m <= 64) {
-        v = gc_seq_sum(s, (int)a, (int)b);
+        if (half == 0) v = gc_seq_sum(s, (int)a, (int)b);
       } else {
         const int h = m / 2;
-        v = __dadd_rn(gc_seq_sum(s, (int)a, (int)a + h), gc_seq_sum(s, (int)a + h, (int)b));
+        v = half == 0 ? gc_seq_sum(s, (int)a, (int)a + h) : gc_seq_sum(s, (int)a + h, (int)b);
       }
       ns[threadIdx.x] = v;
     }
     __syncthreads();
+    {
+      double v = 0.0;
+      if (threadIdx.x < nodes) {
+        gc_i64 a = 0, b = len;
+        gc_descend(a, b, threadIdx.x, d2);
+        const double v0 = ns[2 * threadIdx.x], v1 = ns[2 * threadIdx.x + 1];
+        v = (b - a) <= 64 ? v0 : __dadd_rn(v0, v1);
+      }
+      __syncthreads();
+      if (threadIdx.x < nodes) ns[threadIdx.x] = v;
+      __syncthreads();
+    }
     for (int w = nodes >> 1; w >= 1; w >>= 1) {
       double v = 0.0;
       if (threadIdx.x < w) v = __dadd_rn(ns[2 * threadIdx.x], ns[2 * threadIdx.x + 1]);
@@ -346,7 +367,7 @@ extern "C" __global__ void __launch_bounds__(256) gc_eval_kahan(const EvalGrid g
 )GCSRC";
 
 static_assert(kKahanBlocks == 1024 && kKahanThreads == 256, "the device source bakes in the compensated sum's shape");
-static_assert(kEvalThreads == 256, "the device source bakes in 256 threads per block");
+static_assert(kEvalThreads == 512, "the device source bakes in 512 threads per block");
 
 constexpr int n_inputs(int comps, int arity) {
   return comps == 1 ? (arity == 1 ? 1 : arity + 2) : (arity == 1 ? 3 : 12);
@@ -425,6 +446,8 @@ std::string program_source(const gc_program* f, gc_dtype dt) {
   std::string s = "#define GC_T " + std::string(dt == GC_F64 ? "double" : "float") + "\n";
   s += "#define GC_COMPS " + std::to_string(f->components) + "\n";
   s += "#define GC_ARITY " + std::to_string(f->arity) + "\n";
+  s += "#define GC_MIN_CTAS " +
+       std::string(f->components == 1 ? (f->arity <= 2 ? "3" : "1") : "2") + "\n";
   s += kDeviceSource;
   s += integrand_source(f);
   return s;
@@ -502,7 +525,7 @@ gc_status compile(gc_context* ctx, const std::string& src, Compiled* out) {
   if (drv.load(&mod, cubin.data()) != CUDA_SUCCESS || drv.get(&c.pairwise, mod, "gc_eval_pairwise") != CUDA_SUCCESS ||
       drv.get(&c.kahan, mod, "gc_eval_kahan") != CUDA_SUCCESS)
     return fail(GC_ERR_CUDA, "gc_evaluate_program: loading the compiled integrand failed");
-  const int smem = static_cast<int>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+  const int smem = static_cast<int>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 2 * 128));
   if (drv.attr(c.pairwise, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem) != CUDA_SUCCESS)
     return fail(GC_ERR_CUDA, "gc_evaluate_program: shared-memory attribute refused");
   g_jit.emplace(key, c);
@@ -593,7 +616,7 @@ gc_status run_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void
     long long nchunks = plan.nchunks;
     void* args[] = {&a, &depth, &nchunks, &partial};
     const unsigned grid = static_cast<unsigned>(std::min<long long>(nchunks, static_cast<long long>(ctx->num_sms) * 3));
-    const unsigned smem = static_cast<unsigned>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 128));
+    const unsigned smem = static_cast<unsigned>(sizeof(double) * (kChunkCells + kChunkCells / 64 + 8 + 2 * 128));
     if (drv.launch(k.pairwise, grid, 1, 1, kEvalThreads, 1, 1, smem, ctx->stream, args, nullptr) != CUDA_SUCCESS)
       return fail(GC_ERR_CUDA, "gc_evaluate_program: launch failed");
     if ((s = pairwise_finish(ctx, partial, nchunks, &total)) != GC_OK) return s;

@@ -172,6 +172,7 @@ class Grid:
 
 
 OPT_CLUSTER_STEPPING = 0
+OPT_FUSED_STEP = 1
 lib.gc_context_set_option.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
 lib.gc_context_set_option.restype = C.c_int
 
@@ -192,6 +193,11 @@ class Context:
         """GC_OPT_CLUSTER_STEPPING: small 2-D grids advance in one
         cluster-resident launch (default) or through the per-stage kernels."""
         _check(lib.gc_context_set_option(self.handle, OPT_CLUSTER_STEPPING, int(bool(enabled))))
+
+    def set_fused_step(self, enabled: bool) -> None:
+        """GC_OPT_FUSED_STEP: 2-D double RK4 at order 2 runs one fused kernel
+        per step (default) or the four stage kernels."""
+        _check(lib.gc_context_set_option(self.handle, OPT_FUSED_STEP, int(bool(enabled))))
 
     def close(self) -> None:
         if self.handle:
@@ -635,12 +641,13 @@ class ChBatch:
 
 class gc_corrector_policy(C.Structure):
     _fields_ = [("dt_fine", C.c_double), ("fine_per_coarse", C.c_int32),
-                ("residual_tol", C.c_double), ("energy_tol", C.c_double), ("energy_rtol", C.c_double)]
+                ("residual_tol", C.c_double), ("energy_tol", C.c_double), ("energy_rtol", C.c_double),
+                ("try_base", C.c_int32)]
 
 
 class gc_corrector_stats(C.Structure):
     _fields_ = [("accepted", C.c_int64), ("fallbacks", C.c_int64), ("rejected_energy", C.c_int64),
-                ("rejected_residual", C.c_int64), ("last_residual", C.c_double)]
+                ("rejected_residual", C.c_int64), ("accepted_base", C.c_int64), ("last_residual", C.c_double)]
 
 
 for _name, _args in {
@@ -788,17 +795,20 @@ class Corrector:
 
     def advance(self, psi, grid: Grid, rhs: "CahnHilliardRhs", n_coarse: int, dt_fine: float = 0.01,
                 fine_per_coarse: int = 16, residual_tol: float = 0.05, energy_tol: float = 0.0,
-                energy_rtol: float = ENERGY_RTOL):
+                energy_rtol: float = ENERGY_RTOL, try_base: bool = True):
         """n_coarse learned coarse steps of psi (in place), each accepted when
         F rises by at most energy_tol + energy_rtol |F| and the trapezoid
-        residual is at most residual_tol, else replaced by plain RK4 steps;
-        returns the counts, with the rejections by cause."""
-        pol = gc_corrector_policy(dt_fine, fine_per_coarse, residual_tol, energy_tol, energy_rtol)
+        residual is at most residual_tol; a rejected step is taken by the
+        base step alone when that passes the same test (try_base, with a base
+        step set), else by plain RK4 steps.  Returns the counts, with the
+        network's rejections by cause."""
+        pol = gc_corrector_policy(dt_fine, fine_per_coarse, residual_tol, energy_tol, energy_rtol, int(try_base))
         st = gc_corrector_stats()
         _check(lib.gc_corrector_advance(self.handle, C.byref(grid.c()), C.byref(rhs.c()), psi.data_ptr(),
                                         n_coarse, C.byref(pol), C.byref(st)))
         return {"accepted": st.accepted, "fallbacks": st.fallbacks, "rejected_energy": st.rejected_energy,
-                "rejected_residual": st.rejected_residual, "last_residual": st.last_residual}
+                "rejected_residual": st.rejected_residual, "accepted_base": st.accepted_base,
+                "last_residual": st.last_residual}
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -115,7 +115,7 @@ def _free_energy_baseline(psi, g: Grid) -> float:
 
 def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, energy_tol: float = 0.0,
                      energy_rtol: float = ENERGY_RTOL) -> dict:
-    """schemes: list of (name, corrector, residual_tol).  Per seed the plain
+    """schemes: list of (name, corrector, residual_tol[, try_base]).  Per seed the plain
     fine RK4 reference runs once; every scheme advances the same initial
     state by coarse steps with the plain-RK4 fallback and is compared with
     it at t_end.  Fallbacks are also counted by cause (the proposal raised F
@@ -127,7 +127,9 @@ def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, ener
     n_fine = int(round(t_end / DT_FINE))
     n_coarse = n_fine // FINE_PER_COARSE
     t_fine = 0.0
-    rec = {name: {"l2": [], "ferr": [], "acc": 0, "fb": 0, "rej_e": 0, "rej_r": 0, "t": 0.0} for name, _, _ in schemes}
+    schemes = [tuple(sc) + (True,) if len(sc) == 3 else tuple(sc) for sc in schemes]
+    rec = {sc[0]: {"l2": [], "ferr": [], "acc": 0, "fb": 0, "rej_e": 0, "rej_r": 0, "acc_b": 0, "t": 0.0}
+           for sc in schemes}
     for s in seeds:
         c0 = torch.from_numpy(initial_condition(s, size)).cuda()
         ref = c0.clone()
@@ -137,29 +139,31 @@ def evaluate_heldout(schemes, seeds, size: int = 512, t_end: float = 200.0, ener
         torch.cuda.synchronize()
         t_fine += time.perf_counter() - t0
         fr = _free_energy_baseline(ref, g)
-        for name, net, tol in schemes:
+        for name, net, tol, try_base in schemes:
             r = rec[name]
             x = c0.clone()
             torch.cuda.synchronize()
             t1 = time.perf_counter()
-            st = net.advance(x, g, rhs, n_coarse, DT_FINE, FINE_PER_COARSE, tol, energy_tol, energy_rtol)
+            st = net.advance(x, g, rhs, n_coarse, DT_FINE, FINE_PER_COARSE, tol, energy_tol, energy_rtol, try_base)
             torch.cuda.synchronize()
             r["t"] += time.perf_counter() - t1
             r["acc"] += st["accepted"]
             r["fb"] += st["fallbacks"]
             r["rej_e"] += st["rejected_energy"]
             r["rej_r"] += st["rejected_residual"]
+            r["acc_b"] += st["accepted_base"]
             r["l2"].append(float(torch.linalg.norm(x - ref) / torch.linalg.norm(ref)))
             r["ferr"].append(abs(_free_energy_baseline(x, g) - fr) / abs(fr))
     cells_steps = len(seeds) * size * size * n_coarse * FINE_PER_COARSE
     out = {"seeds": len(seeds), "t_end": t_end, "coarse_steps_per_scheme": n_coarse * len(seeds),
            "energy_tol": energy_tol, "energy_rtol": energy_rtol,
            "plain_mcell_steps": cells_steps / t_fine / 1e6, "schemes": {}}
-    for name, _, tol in schemes:
+    for name, _, tol, try_base in schemes:
         r = rec[name]
+        total = r["acc"] + r["acc_b"] + r["fb"]
         out["schemes"][name] = {
-            "residual_tol": tol, "accepted": r["acc"], "fallbacks": r["fb"],
-            "fallback_rate": r["fb"] / max(r["acc"] + r["fb"], 1),
+            "residual_tol": tol, "try_base": try_base, "accepted": r["acc"], "accepted_base": r["acc_b"],
+            "fallbacks": r["fb"], "fallback_rate": r["fb"] / max(total, 1),
             "rejected_energy": r["rej_e"], "rejected_residual": r["rej_r"],
             "l2_err_mean": float(np.mean(r["l2"])), "l2_err_max": float(np.max(r["l2"])),
             "f_err_mean": float(np.mean(r["ferr"])), "f_err_max": float(np.max(r["ferr"])),

@@ -92,8 +92,13 @@ GC_API gc_status gc_context_destroy(gc_context* ctx);
  *     whose whole state fits in the shared memory of one thread-block
  *     cluster (up to 16 CTAs; about 240 x 240 doubles with RK4) in a single
  *     cluster-resident launch for all its steps; 0 always uses the per-stage
- *     kernels.  Both give the same values (bit for bit in double). */
-typedef enum gc_option { GC_OPT_CLUSTER_STEPPING = 0 } gc_option;
+ *     kernels.  Both give the same values (bit for bit in double).
+ *   GC_OPT_FUSED_STEP (default 1): gc_ch_integrate runs each RK4 step of a
+ *     2-D double grid at order 2 as one fused kernel (all four stages on a
+ *     tile with an 8-cell halo in shared memory; psi read and psi' written
+ *     once per step); 0 uses the four stage kernels.  Same values, bit for
+ *     bit. */
+typedef enum gc_option { GC_OPT_CLUSTER_STEPPING = 0, GC_OPT_FUSED_STEP = 1 } gc_option;
 GC_API gc_status gc_context_set_option(gc_context* ctx, int32_t option, int32_t value);
 GC_API gc_status gc_synchronize(gc_context* ctx);
 /* Failure-detection self-test (no reference counterpart): launches one
@@ -294,7 +299,8 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt,
  * (solve/RK4.hpp:99-154, solve/ExplicitEuler.hpp:79-112) with the
  * Cahn-Hilliard RHS, psi advanced in place.  RK4 runs four fused stage
  * kernels per step (each reads and writes every field once); the steps are
- * replayed from a captured CUDA graph.  A 2-D grid whose state fits in one
+ * replayed from a captured CUDA graph (a 2-D double grid at order 2 runs one
+ * fused kernel per step instead, GC_OPT_FUSED_STEP).  A 2-D grid whose state fits in one
  * thread-block cluster's shared memory (gc_ch_cluster_ctas > 0) instead runs
  * all n_steps in one cluster-resident launch (GC_OPT_CLUSTER_STEPPING). */
 GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
@@ -397,6 +403,8 @@ typedef struct gc_corrector_policy {
   double residual_tol;      /* accept when the trapezoid residual is at most this */
   double energy_tol;        /* accept when F rises by at most energy_tol + energy_rtol |F| */
   double energy_rtol;
+  int32_t try_base;         /* with a base step: a rejected proposal B(c) + delta is followed by
+                               the same test on B(c) alone before falling back to plain RK4 */
 } gc_corrector_policy;
 
 typedef struct gc_corrector_stats {
@@ -404,6 +412,7 @@ typedef struct gc_corrector_stats {
   int64_t fallbacks;          /* coarse steps taken by plain RK4 instead */
   int64_t rejected_energy;    /* fallbacks whose proposal raised F beyond the tolerance */
   int64_t rejected_residual;  /* fallbacks whose proposal's residual exceeded residual_tol */
+  int64_t accepted_base;      /* coarse steps taken by the base step alone (try_base) */
   double last_residual;
 } gc_corrector_stats;
 
@@ -437,7 +446,11 @@ GC_API gc_status gc_corrector_gradient(gc_corrector* c, int32_t batch, gc_dtype 
 /* One Adam step (beta 0.9 / 0.999) on that loss. */
 GC_API gc_status gc_corrector_train_step(gc_corrector* c, int32_t batch, gc_dtype dt, const void* cin,
                                          const void* target, float lr, double* loss);
-/* Learned coarse steps on one double field with the plain-RK4 fallback. */
+/* Learned coarse steps on one double field with the plain-RK4 fallback
+ * (and, with pol->try_base, the base step alone as the first fallback).
+ * rejected_energy / rejected_residual count the network's rejected
+ * proposals by cause (one can fail both); accepted_base of them were taken
+ * by the base step alone, fallbacks by plain RK4. */
 GC_API gc_status gc_corrector_advance(gc_corrector* c, const gc_grid* g, const gc_ch_params* cp, double* psi,
                                       int32_t n_coarse, const gc_corrector_policy* pol,
                                       gc_corrector_stats* stats);
