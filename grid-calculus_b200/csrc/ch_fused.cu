@@ -22,7 +22,10 @@
 // HBM traffic per step is psi once (the halo's overlap with neighbouring
 // tiles comes from L2) and psi' once: 16 B per cell instead of 104.  The
 // price is the halo's extra arithmetic (about 1.4x at 64 x 28 tiles): the
-// kernel is bound by the FP64 pipe and shared memory, not by HBM.
+// kernel is bound by instruction issue (FP64 arithmetic and shared-memory
+// accesses), not by HBM.  Every stage is its own template instance with
+// compile-time regions, and each thread walks a column strip keeping three
+// rows in registers, so a cell costs three shared-memory reads.
 //
 // Interior tiles arrive by one TMA box (x offset a multiple of 8 doubles);
 // tiles touching the grid edge load their wrapped frame with plain loads.
@@ -43,7 +46,6 @@ namespace {
 constexpr int kFzThreads = 512;
 constexpr int kFzWarps = kFzThreads / 32;
 constexpr long long kFzWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
-constexpr size_t kFzMaxCells = size_t(2048) * 2048;  // larger grids take the stage kernels
 
 constexpr size_t fz_al(size_t b) { return (b + 127) / 128 * 128; }
 
@@ -76,21 +78,123 @@ struct FzParams {
   int tiles_x, tiles_y;
 };
 
-// Calls f(r, c) for the frame cells of rows [r0, r1) x columns [c0, c1):
-// warps over rows, lanes over columns.
-template <class F>
-__device__ __forceinline__ void fz_region(int r0, int r1, int c0, int c1, F&& f) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r = r0 + warp; r < r1; r += kFzWarps)
-    for (int c = c0 + lane; c < c1; c += 32) f(r, c);
+// The cells of a W x NR region (frame offset of its first cell: base) in
+// column strips: thread t takes column t % W and rows [j RP, j RP + RP) of
+// it, j = t / W < NS, with NS = 512 / W strips of RP = ceil(NR / NS) rows.
+// f(off, rr, cc, k) for each of its cells in order down the column (k the
+// cell's index within the strip, for the caller's register window).
+template <int W, int NR, class F>
+__device__ __forceinline__ void fz_strips(int base, F&& f) {
+  constexpr int SX = FzLayout::SX;
+  constexpr int NS = kFzThreads / W;
+  constexpr int RP = (NR + NS - 1) / NS;
+  const int t = threadIdx.x, j = t / W, cc = t - j * W;
+  if (j < NS) {
+    const int r0 = j * RP;
+    int off = base + r0 * SX + cc;
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+      if (RP * NS == NR || r0 + k < NR) f(off, r0 + k, cc, k);
+      off += SX;
+    }
+  }
 }
 
+// One stage S (0..3) of the fused step on the tile at (x0, y0).  Regions and
+// the stage's update are compile-time constants: the mu pass covers the
+// tile plus hm = H - 2R S - R cells, the k pass the tile plus hk = hm - R.
+// Each thread walks a column strip and keeps the centre column's three rows
+// in registers, so a cell reads three values from shared memory (the new
+// row below, the two x neighbours).  UNIT: unit spacing, mobility and kappa
+// (the multiplies by 1 are skipped, as the stage kernels' exact shortcuts do).
+template <int S, bool UNIT>
+__device__ __forceinline__ void fz_stage(const FzParams& a, const double* __restrict__ ps, double* __restrict__ ys,
+                                         double* __restrict__ ms, double* __restrict__ k1s,
+                                         double* __restrict__ k23s, int x0, int y0) {
+  using L = FzLayout;
+  using T = double;
+  constexpr int R = L::R, H = L::H, TX = L::TX, TY = L::TY, SX = L::SX;
+  constexpr int hy = H - 2 * R * S, hm = hy - R, hk = hm - R;
+  constexpr int YOFF = L::YR0 * SX, MOFF = L::MR0 * SX;  // frame offset of each buffer's first row
+  const StageParams<T>& p = a.p;
+
+  // mu = -y + y^3 - kappa lap(y)
+  {
+    constexpr int W = TX + 2 * hm, NR = TY + 2 * hm, B = H - hm;
+    const T* yb = S == 0 ? ps : ys - YOFF;  // indexed by frame offset (valid rows only)
+    T w0 = 0.0, w1 = 0.0;
+    fz_strips<W, NR>(B * SX + B, [&](int off, int, int, int k) {
+      if (k == 0) {
+        w0 = yb[off - SX];
+        w1 = yb[off];
+      }
+      const T w2 = yb[off + SX];
+      const T yc = w1;
+      const T ax = Ar<T>::add(Ar<T>::add(yb[off - 1], Ar<T>::mul(-2.0, yc)), yb[off + 1]);
+      const T ay = Ar<T>::add(Ar<T>::add(w0, Ar<T>::mul(-2.0, yc)), w2);
+      w0 = w1;
+      w1 = w2;
+      T mu;
+      if constexpr (UNIT) {
+        mu = Ar<T>::sub(Ar<T>::add(-yc, Ar<T>::mul(Ar<T>::mul(yc, yc), yc)), Ar<T>::add(ax, ay));
+      } else {
+        mu = chem_pot(p, yc, lap_xy(p, ax, ay));
+      }
+      ms[off - MOFF] = mu;
+    });
+  }
+  __syncthreads();
+  // k = M lap(mu), then the stage's update
+  {
+    constexpr int W = TX + 2 * hk, NR = TY + 2 * hk, B = H - hk;
+    const T* mb = ms - MOFF;
+    T w0 = 0.0, w1 = 0.0;
+    fz_strips<W, NR>(B * SX + B, [&](int off, int rr, int cc, int k) {
+      if (k == 0) {
+        w0 = mb[off - SX];
+        w1 = mb[off];
+      }
+      const T w2 = mb[off + SX];
+      const T mc = w1;
+      const T ax = Ar<T>::add(Ar<T>::add(mb[off - 1], Ar<T>::mul(-2.0, mc)), mb[off + 1]);
+      const T ay = Ar<T>::add(Ar<T>::add(w0, Ar<T>::mul(-2.0, mc)), w2);
+      w0 = w1;
+      w1 = w2;
+      T rhs;
+      if constexpr (UNIT) {
+        rhs = Ar<T>::add(ax, ay);
+      } else {
+        rhs = mobility(p, lap_xy(p, ax, ay));
+      }
+      const T pc = ps[off];
+      if constexpr (S < 3) {
+        ys[off - YOFF] = Ar<T>::add(pc, Ar<T>::mul(S < 2 ? a.half_dt : a.dt, rhs));
+        const int tr = rr - hk, tc = cc - hk;
+        if (static_cast<unsigned>(tr) < static_cast<unsigned>(TY) && static_cast<unsigned>(tc) < static_cast<unsigned>(TX)) {
+          const int t = tr * TX + tc;
+          if constexpr (S == 0) k1s[t] = rhs;
+          else if constexpr (S == 1) k23s[t] = rhs;
+          else k23s[t] = Ar<T>::add(k23s[t], rhs);
+        }
+      } else {  // the region is the tile
+        const int t = rr * TX + cc;
+        if (y0 + rr < p.ny && x0 + cc < p.nx) {
+          const T s14 = Ar<T>::add(k1s[t], rhs);
+          a.out[static_cast<size_t>(y0 + rr) * p.nx + (x0 + cc)] =
+              Ar<T>::add(pc, Ar<T>::add(Ar<T>::mul(a.c6, s14), Ar<T>::mul(a.c3, k23s[t])));
+        }
+      }
+    });
+  }
+  __syncthreads();
+}
+
+template <bool UNIT>
 __global__ void __launch_bounds__(kFzThreads, 2)
     ch_fused_rk4_kernel(const FzParams a, const __grid_constant__ CUtensorMap m_psi, int* status) {
   using L = FzLayout;
   using T = double;
-  constexpr int R = L::R, H = L::H, TX = L::TX, TY = L::TY, SX = L::SX, SY = L::SY;
-  const StageParams<T>& p = a.p;
+  constexpr int H = L::H, TX = L::TX, TY = L::TY, SX = L::SX, SY = L::SY;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   uint64_t* bar = reinterpret_cast<uint64_t*>(base);
@@ -100,7 +204,7 @@ __global__ void __launch_bounds__(kFzThreads, 2)
   T* ms = reinterpret_cast<T*>(base + L::OFF_MU);
   T* k1s = reinterpret_cast<T*>(base + L::OFF_K1);
   T* k23s = reinterpret_cast<T*>(base + L::OFF_K23);
-  const int nx = p.nx, ny = p.ny, tid = threadIdx.x;
+  const int nx = a.p.nx, ny = a.p.ny, tid = threadIdx.x;
   const int ntiles = a.tiles_x * a.tiles_y;
 
   auto origin = [&](int tl, int& x0, int& y0) {
@@ -151,48 +255,10 @@ __global__ void __launch_bounds__(kFzThreads, 2)
     }
     __syncthreads();
     if (*s_abort) break;
-
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s) {
-      // Halos: y_s on hy, mu on hy - R, k_s on hy - 2R.
-      const int hy = H - 2 * R * s;
-      const int hm = hy - R, hk = hy - 2 * R;
-      // mu pass.
-      fz_region(H - hm, H + TY + hm, H - hm, H + TX + hm, [&](int r, int c) {
-        const T* yr = s == 0 ? ps + r * SX : ys + (r - L::YR0) * SX;
-        const T yc = yr[c];
-        const T ax = tap_sum<T, 2, 2>([&](int o) { return o == 0 ? yc : yr[c + o]; });
-        const T ay = tap_sum<T, 2, 2>([&](int o) { return yr[o * SX + c]; });
-        ms[(r - L::MR0) * SX + c] = chem_pot(p, yc, lap_xy(p, ax, ay));
-      });
-      __syncthreads();
-      // k pass and the stage's update.
-      fz_region(H - hk, H + TY + hk, H - hk, H + TX + hk, [&](int r, int c) {
-        const T* mr = ms + (r - L::MR0) * SX;
-        const T mc = mr[c];
-        const T ax = tap_sum<T, 2, 2>([&](int o) { return o == 0 ? mc : mr[c + o]; });
-        const T ay = tap_sum<T, 2, 2>([&](int o) { return mr[o * SX + c]; });
-        const T rhs = mobility(p, lap_xy(p, ax, ay));
-        const T pc = ps[r * SX + c];
-        if (s < 3) ys[(r - L::YR0) * SX + c] = Ar<T>::add(pc, Ar<T>::mul(s < 2 ? a.half_dt : a.dt, rhs));
-        const int tr = r - H, tc = c - H;
-        if (tr >= 0 && tr < TY && tc >= 0 && tc < TX) {
-          const int t = tr * TX + tc;
-          if (s == 0) {
-            k1s[t] = rhs;
-          } else if (s == 1) {
-            k23s[t] = rhs;
-          } else if (s == 2) {
-            k23s[t] = Ar<T>::add(k23s[t], rhs);
-          } else if (y0 + tr < ny && x0 + tc < nx) {
-            const T s14 = Ar<T>::add(k1s[t], rhs);
-            a.out[static_cast<size_t>(y0 + tr) * nx + (x0 + tc)] =
-                Ar<T>::add(pc, Ar<T>::add(Ar<T>::mul(a.c6, s14), Ar<T>::mul(a.c3, k23s[t])));
-          }
-        }
-      });
-      __syncthreads();
-    }
+    fz_stage<0, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<1, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<2, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<3, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
   }
 }
 
@@ -203,10 +269,9 @@ gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* c
   using L = FzLayout;
   *done = false;
   if (g->nz != 1 || cp->order != 2 || g->nx < L::SX || g->ny < L::SY) return GC_OK;
-  // Measured on B200 per RK4 step (fused / four stage kernels): 256^2 13.8 /
-  // 23.3 us, 1024^2 34.4 / 47.0, 2048^2 128 / 131, 4096^2 503 / 426, 8192^2
-  // 1951 / 1562: the stage kernels win once the grid fills the GPU.
-  if (cells(g) > kFzMaxCells) return GC_OK;
+  // Measured on B200 per RK4 step (fused / four stage kernels): 256^2 9.2 /
+  // 24.5 us, 1024^2 22.8 / 45.7, 2048^2 80.6 / 130, 4096^2 311 / 427,
+  // 8192^2 1193 / 1553: the fused kernel wins at every size.
   CUtensorMap m{};
   if (!make_tensor_map_2d(&m, src, g->nx, g->ny, 8, L::SX, L::SY)) return GC_OK;
   FzParams a{};
@@ -228,11 +293,13 @@ gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* c
   a.c3 = dt / 3.0;
   a.tiles_x = div_up(g->nx, L::TX);
   a.tiles_y = div_up(g->ny, L::TY);
+  const bool unit = p.unit_h && p.unit_m && p.unit_k;
+  auto kern = unit ? ch_fused_rk4_kernel<true> : ch_fused_rk4_kernel<false>;
   int per_sm = 1;
-  GC_TRY(kernel_setup(ch_fused_rk4_kernel, kFzThreads, L::BYTES, &per_sm));
+  GC_TRY(kernel_setup(kern, kFzThreads, L::BYTES, &per_sm));
   const long long ntiles = static_cast<long long>(a.tiles_x) * a.tiles_y;
   const int grid = static_cast<int>(std::min<long long>(ntiles, static_cast<long long>(per_sm) * ctx->num_sms));
-  ch_fused_rk4_kernel<<<grid, kFzThreads, L::BYTES, ctx->stream>>>(a, m, ctx->device_status);
+  kern<<<grid, kFzThreads, L::BYTES, ctx->stream>>>(a, m, ctx->device_status);
   GC_CHECK_LAUNCH("ch_fused_rk4_kernel");
   *done = true;
   return GC_OK;

@@ -122,3 +122,41 @@ def test_autotune_and_cache(gc, oracle, tmp_path):
     assert json.loads(b2.autotune(steps_per_trial=4, cache_path=cache))["cached"] is True
     b.close()
     b2.close()
+
+
+def test_large_members(gc, oracle):
+    """Members at the top of the ensemble's size range (512^2 and 640 x 576):
+    in double bit-identical to the oracle after 20 steps; in float, after
+    1000 steps at each member's stable dt, within 1e-4 (L2) and 1e-5 (free
+    energy) of the FP64 solution from the same FP32-rounded start (the plain
+    FP64 path, itself bit-identical to the oracle)."""
+    import torch
+    members = [(512, 512, 1.0, 1.0, stable_dt(1.0)), (96, 80, 1.0, 1.7, stable_dt(1.7)),
+               (640, 576, 1.0, 0.6, stable_dt(0.6))]
+    init = ics(members, seed=21)
+    b = gc.ChBatch(members, order=4, dtype=torch.float64)
+    for i, c0 in enumerate(init):
+        b.set_member(i, c0)
+    b.run(20)
+    for i in (0, 2):
+        nx, ny, mob, kap, dt = members[i]
+        want = oracle.ch_integrate(4, mob, kap, init[i].reshape(1, ny, nx), dt, 20)
+        assert np.array_equal(b.get_member(i), want.reshape(ny, nx)), i
+    b.close()
+    b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    start = [c.astype(np.float32).astype(np.float64) for c in init]
+    for i, c0 in enumerate(start):
+        b.set_member(i, c0)
+    b.run(1000)
+    _, energy = b.diagnostics()
+    for i, (nx, ny, mob, kap, dt) in enumerate(members):
+        g = gc.Grid(nx, ny, 1)
+        want = torch.from_numpy(start[i].reshape(1, ny, nx)).cuda()
+        gc.ch_integrate(want, g, gc.CahnHilliardRhs(mob, kap, 4), dt, 1000, gc.RK4)
+        got = torch.from_numpy(b.get_member(i).reshape(1, ny, nx)).cuda().double()
+        l2 = float(torch.linalg.norm(got - want) / torch.linalg.norm(want))
+        assert l2 < 1e-4, (i, l2)
+        v4 = nx * ny / 4.0
+        f_ref = gc.evaluate(want, g, "ch_free_energy", kappa=kap) + v4
+        assert abs(energy[i] + v4 - f_ref) / abs(f_ref) < 1e-5, (i, energy[i] + v4, f_ref)
+    b.close()
