@@ -54,14 +54,26 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 NX = NY = 8192
 DT = 0.01
-# Algorithmic HBM bytes per cell-step of the fused RK4 (13 field passes of
-# 8-byte doubles: stage 1 reads psi and writes k1, stages 2-3 read psi and
-# k_prev and write k_s, stage 4 reads psi, k1, k2, k3 and writes psi').
+# Algorithmic HBM bytes per cell-step of RK4 (13 field passes of 8-byte
+# doubles: stage 1 reads psi and writes k1, stages 2-3 read psi and k_prev
+# and write k_s, stage 4 reads psi, k1, k2, k3 and writes psi'), the fixed
+# definition the roofline fraction is quoted on.  The fused step kernel
+# keeps the stage fields in shared memory and moves about 16 B per
+# cell-step, so against HBM it is not bandwidth-bound; FP64_OPS_PER_CELL_STEP
+# gives its arithmetic for the FP64 comparison.
 BYTES_PER_CELL_STEP = 13 * 8
-# DRAM bytes (read + write) per RK4 step per cell measured by ncu for the
-# four stage kernels (one full capture on 4096^2: 1648.0 MB per step for
-# 16.8 M cells; both sizes are beyond L2, so it scales with the cell count).
-NCU_TRAFFIC_PER_CELL_STEP = 98.2
+# FP64 operations per cell-step of the fused kernel at order 2 with unit
+# spacing, mobility and kappa, counted from its source: per 64 x 28 tile,
+# mu on 10,448 cells (11 operations each), k with the next stage's y on
+# 7,808 cells (9 each), the last stage's k and psi' on 1,792 cells (12
+# each) and 1,792 k2 + k3 additions: 208,496 per 1,792 cells.
+FP64_OPS_PER_CELL_STEP = 208496 / 1792
+FP64_NOMINAL_TOPS = 18.6  # 64 FP64 lanes x 148 SMs x 1.965 GHz, one operation per lane and clock
+# DRAM bytes (read + write) per RK4 step per cell of the fused step kernel,
+# from one ncu capture of one launch on 4096^2 (136.2 MB read + 96.5 MB
+# written for 16.8 M cells; the fields are beyond L2 at both sizes, so it
+# scales with the cell count to the 8192^2 launch).
+NCU_TRAFFIC_PER_CELL_STEP = (136.164608e6 + 96.456448e6) / 4096 ** 2
 # Forms the default run measures after the headline (each its own JSON line).
 DEFAULT_FORMS = ["config1", "operators", "fvm", "batched", "learned"]
 
@@ -211,7 +223,6 @@ def _cuda_time(fn, reps=5):
 # tap added from 0, non-unit products multiplied first), and the
 # 15-operation combination (diff/Biharmonic.hpp:70-99).
 BIHARMONIC_FP64_OPS = {2: 3 * 7 + 3 * 14 + 15, 4: 3 * 13 + 3 * 50 + 15, 6: 3 * 17 + 3 * 98 + 15}
-FP64_NOMINAL_TOPS = 18.5
 
 
 def fourier_field(n, seed, device, dtype):
@@ -858,7 +869,7 @@ def run_ours(args, rank: int, world: int, local: int):
         names = DEFAULT_FORMS if args.forms == "all" else args.forms.split(",")
         summaries = run_forms(gc, [n for n in names if n != "headline"], peak)
     if rank == 0:
-        traffic = NCU_TRAFFIC_PER_CELL_STEP * cells / 4.0 if NCU_TRAFFIC_PER_CELL_STEP is not None else None
+        traffic = NCU_TRAFFIC_PER_CELL_STEP * cells if NCU_TRAFFIC_PER_CELL_STEP is not None else None
         line = {
             "metric": "Mcell-steps/s (plain FP64 RK4 Cahn-Hilliard)", "value": value, "unit": "Mcell-steps/s",
             "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -870,13 +881,17 @@ def run_ours(args, rank: int, world: int, local: int):
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "RK4 stage kernels, 4 launches per step, 104 B/cell-step algorithmic"},
+                         "kernel": "ch_fused_rk4_kernel, 1 launch per RK4 step; achieved on the 104 B/cell-step "
+                                   "of the unfused method; traffic = ncu DRAM bytes per launch",
+                         "fp64_Tops": FP64_OPS_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e12,
+                         "fp64_frac_of_nominal": FP64_OPS_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e12
+                         / FP64_NOMINAL_TOPS},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": cells * 8 / chunk,
                     "d2h_bytes_per_step": cells * 8 / chunk,
                     "note": f"{n_chunks} chunks of {chunk} steps: pinned host -> device, gc_ch_integrate, "
                             "device -> pinned host; two contexts on two streams"},
-            "gpu_launches": 4 * K * n_blocks,
+            "gpu_launches": K * n_blocks,
             "clocks": clocks.summary(),
         }
         if summaries is not None:

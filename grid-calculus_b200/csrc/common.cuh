@@ -74,7 +74,7 @@ struct gc_context {
   void* spectral_plans = nullptr;
   void (*spectral_release)(void*) = nullptr;
   // gc_context_set_option switches.
-  bool cluster_stepping = true;
+  bool cluster_stepping = false;
   bool fused_step = true;
 };
 

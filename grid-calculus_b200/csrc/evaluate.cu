@@ -220,6 +220,20 @@ __device__ __forceinline__ void gc_locate(const EvalGrid& g, gc_i64 c, int& i, i
 
 __device__ __forceinline__ int gc_padpos(int e) { return e + (e >> 6); }
 
+// Bulk prefetch into L2 of cells [first, first + count) of every component:
+// the 16-byte-aligned bytes inside that range (the bulk copy's alignment
+// rule; the few bytes at either end are left out, so nothing outside the
+// field is touched).
+__device__ __forceinline__ void gc_prefetch_l2(const EvalGrid& g, gc_i64 first, gc_i64 count) {
+  for (int comp = 0; comp < GC_COMPS; ++comp) {
+    const unsigned long long a = (unsigned long long)((const GC_T*)g.field + (gc_i64)comp * g.n + first);
+    const unsigned long long b = a + (unsigned long long)count * sizeof(GC_T);
+    const unsigned long long a16 = (a + 15) & ~15ull, b16 = b & ~15ull;
+    if (b16 > a16)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a16), "r"((unsigned)(b16 - a16)) : "memory");
+  }
+}
+
 __device__ __forceinline__ void gc_descend(gc_i64& lo, gc_i64& hi, gc_i64 idx, int depth) {
   for (int b = depth - 1; b >= 0; --b) {
     const gc_i64 mid = lo + (hi - lo) / 2;
@@ -248,6 +262,12 @@ extern "C" __global__ void __launch_bounds__(512, GC_MIN_CTAS) gc_eval_pairwise(
     gc_i64 lo = 0, hi = g.n;
     gc_descend(lo, hi, c, depth);
     const int len = (int)(hi - lo);
+    // The next chunk of this CTA streams into L2 while this one is formed.
+    if (threadIdx.x == 0 && c + gridDim.x < nchunks) {
+      gc_i64 nlo = 0, nhi = g.n;
+      gc_descend(nlo, nhi, c + gridDim.x, depth);
+      gc_prefetch_l2(g, nlo, nhi - nlo);
+    }
     // Two consecutive cells per thread and iteration.
     int i, j, k;
     gc_locate(g, lo + 2 * threadIdx.x, i, j, k);

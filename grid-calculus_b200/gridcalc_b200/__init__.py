@@ -191,7 +191,8 @@ class Context:
 
     def set_cluster_stepping(self, enabled: bool) -> None:
         """GC_OPT_CLUSTER_STEPPING: small 2-D grids advance in one
-        cluster-resident launch (default) or through the per-stage kernels."""
+        cluster-resident launch (off by default: the fused step kernel is
+        faster on B200)."""
         _check(lib.gc_context_set_option(self.handle, OPT_CLUSTER_STEPPING, int(bool(enabled))))
 
     def set_fused_step(self, enabled: bool) -> None:

@@ -88,11 +88,13 @@ typedef struct gc_context gc_context;
 GC_API gc_status gc_context_create(gc_context** out, int device, void* stream);
 GC_API gc_status gc_context_destroy(gc_context* ctx);
 /* Context switches (no reference counterpart).
- *   GC_OPT_CLUSTER_STEPPING (default 1): gc_ch_integrate advances a 2-D grid
- *     whose whole state fits in the shared memory of one thread-block
- *     cluster (up to 16 CTAs; about 240 x 240 doubles with RK4) in a single
- *     cluster-resident launch for all its steps; 0 always uses the per-stage
- *     kernels.  Both give the same values (bit for bit in double).
+ *   GC_OPT_CLUSTER_STEPPING (default 0): 1 makes gc_ch_integrate advance a
+ *     2-D grid whose whole state fits in the shared memory of one
+ *     thread-block cluster (up to 16 CTAs; about 240 x 240 doubles with RK4)
+ *     in a single cluster-resident launch for all its steps.  Off by
+ *     default: on B200 the fused step kernel below is faster at every such
+ *     size (128^2: 9.2 against 13.1 us per RK4 step).  Same values, bit for
+ *     bit in double.
  *   GC_OPT_FUSED_STEP (default 1): gc_ch_integrate runs each RK4 step of a
  *     2-D double grid at order 2 as one fused kernel (all four stages on a
  *     tile with an 8-cell halo in shared memory; psi read and psi' written
@@ -300,9 +302,10 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt,
  * Cahn-Hilliard RHS, psi advanced in place.  RK4 runs four fused stage
  * kernels per step (each reads and writes every field once); the steps are
  * replayed from a captured CUDA graph (a 2-D double grid at order 2 runs one
- * fused kernel per step instead, GC_OPT_FUSED_STEP).  A 2-D grid whose state fits in one
- * thread-block cluster's shared memory (gc_ch_cluster_ctas > 0) instead runs
- * all n_steps in one cluster-resident launch (GC_OPT_CLUSTER_STEPPING). */
+ * fused kernel per step instead, GC_OPT_FUSED_STEP).  With
+ * GC_OPT_CLUSTER_STEPPING on, a 2-D grid whose state fits in one
+ * thread-block cluster's shared memory (gc_ch_cluster_ctas > 0) runs all
+ * n_steps in one cluster-resident launch. */
 GC_API gc_status gc_ch_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt,
                                  const gc_ch_params* p, void* psi, double dt_step,
                                  int n_steps, gc_integrator integrator);

@@ -16,6 +16,15 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def cluster_path(gc):
+    """The cluster-resident path is opt-in: on for every test here."""
+    ctx = gc.context()
+    ctx.set_cluster_stepping(True)
+    yield
+    ctx.set_cluster_stepping(False)
+
+
 def dev(a, dtype=None):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype or torch.float64)
@@ -85,15 +94,18 @@ def test_non_unit_spacing_mobility_kappa(gc, oracle, order):
 
 def test_same_as_stage_kernels(gc):
     """The cluster launch and the per-stage kernels give the same double
-    trajectory, on one context switched between the two paths."""
+    trajectory (order 4: the fused step kernel does not take it), on one
+    context switched between the two paths."""
     import torch
     g = gc.Grid(160, 144, 1)
     psi0 = _ic((1, 144, 160), 77)
     rhs = gc.CahnHilliardRhs(1.0, 1.0, 4)
     ctx = gc.Context(0, torch.cuda.current_stream().cuda_stream)
+    ctx.set_cluster_stepping(True)
     a, b = dev(psi0), dev(psi0)
     gc.ch_integrate(a, g, rhs, 0.005, 40, gc.RK4, ctx=ctx)
     ctx.set_cluster_stepping(False)
+    ctx.set_fused_step(False)
     gc.ch_integrate(b, g, rhs, 0.005, 40, gc.RK4, ctx=ctx)
     torch.cuda.synchronize()
     assert torch.equal(a, b)

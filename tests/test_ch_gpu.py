@@ -14,17 +14,17 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(autouse=True, params=["default", "fused", "stages"])
+@pytest.fixture(autouse=True, params=["cluster", "fused", "stages"])
 def stepping_path(request, gc):
-    """Every test runs three times: with the default paths (small 2-D grids
-    in one cluster-resident launch, larger 2-D double order-2 grids one fused
-    kernel per RK4 step), with the fused step kernel also on the small grids,
-    and with the four stage kernels forced."""
+    """Every test runs three times: with small 2-D grids in one
+    cluster-resident launch (and larger 2-D double order-2 grids one fused
+    kernel per RK4 step), with the default paths (the fused step kernel for
+    every 2-D double order-2 grid), and with the four stage kernels forced."""
     ctx = gc.context()
-    ctx.set_cluster_stepping(request.param == "default")
+    ctx.set_cluster_stepping(request.param == "cluster")
     ctx.set_fused_step(request.param != "stages")
     yield request.param
-    ctx.set_cluster_stepping(True)
+    ctx.set_cluster_stepping(False)
     ctx.set_fused_step(True)
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.npz")
