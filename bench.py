@@ -714,6 +714,12 @@ def run_case(name: str) -> None:
         x = torch.rand(16, 512, 512, device="cuda", dtype=torch.float64)
         for _ in range(2):
             net.forward(x)
+    elif name == "learned_b1_512":  # one learned coarse-step proposal on 512^2 (base step, features, 6 convolutions)
+        import gridcalc_b200.learned as L
+        net = L.new_corrector(512, 1, seed=0)
+        c = torch.from_numpy(L.initial_condition(9000, 512)).cuda()[None].contiguous()
+        for _ in range(3):
+            net.forward(c)
     elif name == "lap2_384":        # 3-D laplacian order 2, 384^3 FP64 (plane ring)
         n = 384
         g = gc.Grid(n, n, n, 1 / n, 1 / n, 1 / n)
@@ -911,7 +917,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--case", default=None,
-                    help="run one small profiling workload and exit: conv_b16_512, lap2_384, fvm_256, "
+                    help="run one small profiling workload and exit: conv_b16_512, learned_b1_512, lap2_384, fvm_256, "
                          "batch64_f32, ch_f32_4096, fused_4096, eval_fe_320")
     ap.add_argument("--min-seconds", type=float, default=1.5,
                     help="repeat the K-step timed block until this much device time has passed")
