@@ -633,29 +633,26 @@ def form_summary(name: str, r: dict) -> dict:
     if "error" in r:
         return {"error": r["error"][:160]}
     if name == "operators":
-        keys = ("laplacian2", "laplacian4", "gradient2", "divergence2", "biharmonic2", "integrate",
-                "evaluate_free_energy")
-        return {k: {op: _sig(v[op]["frac"], 3) for op in keys if op in v}
-                for k, v in r["results"].items() if k.endswith("512")}
+        res = r["results"].get("f64_512", {})
+        keys = (("lap2", "laplacian2"), ("grad2", "gradient2"), ("div2", "divergence2"), ("bih2", "biharmonic2"),
+                ("int", "integrate"), ("eval_fe", "evaluate_free_energy"))
+        return {"f64_512_frac": {short: _sig(res[k]["frac"], 2) for short, k in keys if k in res}}
     if name == "fvm":
-        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "frac": r["frac"], "mass_drift_rel": r["mass_drift_rel"]})
+        return _sig({"Mcs": r["Mcell-steps/s"], "frac": r["frac"], "drift": r["mass_drift_rel"]}, 3)
     if name == "config1":
-        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "us_per_step": r["us_per_step"],
-                     "cpu_1core_Mcell-steps/s": r["cpu_baseline"]["value"], "speedup_vs_cpu_1core": r["speedup_vs_cpu_1core"],
-                     "mass_drift": r["mass_drift"], "F_0": r["F_every_100_steps"][0],
-                     "F_2000": r["F_every_100_steps"][-1]})
+        return _sig({"Mcs": r["Mcell-steps/s"], "cpu_1core_Mcs": r["cpu_baseline"]["value"],
+                     "drift": r["mass_drift"], "F_2000": r["F_every_100_steps"][-1]}, 4)
     if name == "batched":
         acc = r["accuracy"]
-        return _sig({"Mcell-steps/s": r["Mcell-steps/s"], "frac": r["frac"],
-                     "speedup_vs_plain_f32": r["speedup_vs_plain_f32"], "speedup_vs_plain_f64": r["speedup_vs_plain_f64"],
-                     "members_checked": len(acc["members"]), "sides_checked": [min(acc["sides"]), max(acc["sides"])],
-                     "l2_err_max": acc["l2_err_max"], "f_err_max": acc["f_err_max"]})
+        return _sig({"Mcs": r["Mcell-steps/s"], "frac": r["frac"], "x_plain_f32": r["speedup_vs_plain_f32"],
+                     "x_plain_f64": r["speedup_vs_plain_f64"], "l2_max": acc["l2_err_max"],
+                     "f_max": acc["f_err_max"]}, 3)
     if name.startswith("learned"):
-        out = {"trajectories": r["train"]["trajectories"], "heldout_seeds": r["eval"]["seeds"]}
+        out = {"traj": r["train"]["trajectories"], "seeds": r["eval"]["seeds"]}
         for nm, v in r["eval"]["schemes"].items():
-            out[nm] = _sig({"speedup": v["speedup_vs_plain"], "fallback_rate": v["fallback_rate"],
-                            "base_steps": v.get("accepted_base", 0),
-                            "l2_max": v["l2_err_max"], "f_err_max": v["f_err_max"]}, 3)
+            if nm.endswith("tol0.003"):
+                out[nm.replace("_tol0.003", "")] = _sig({"x_plain": v["speedup_vs_plain"], "fallb": v["fallback_rate"],
+                                                         "l2_max": v["l2_err_max"], "f_max": v["f_err_max"]}, 3)
         return out
     if name == "snapshots":
         return _sig({"overhead_pct": r["overhead_pct"]})
@@ -869,7 +866,7 @@ def run_ours(args, rank: int, world: int, local: int):
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, build = cpu_sample(1, 2048, 2)
         cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": 1, "kind": cpu_kind(build),
-               "sample": f"1 host thread, RK4 on 2048x2048, 2 steps ({build})"}
+               "sample": f"1 thread, RK4 2048^2 x 2 steps, {build.split(', ')[-1]}"}
     summaries = None
     if rank == 0 and world == 1 and args.forms != "headline":
         names = DEFAULT_FORMS if args.forms == "all" else args.forms.split(",")
@@ -882,24 +879,23 @@ def run_ours(args, rank: int, world: int, local: int):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "ch2d-rk4-fp64-order2", "grid": f"{g.nx}x{g.ny}", "dt": DT, "kappa": 1.0,
-                       "mobility": 1.0, "ic": "U[-0.05,0.05] seeded", "l2": "fields 512 MiB each > L2 (no flush)",
-                       "timing": f"median of {n_blocks} blocks of {K} steps (CUDA events, max over ranks)",
-                       "parallelism": f"replicas{world}"},
+                       "mobility": 1.0, "ic": "U[-0.05,0.05] seeded", "l2": "fields 512 MiB > L2, no flush",
+                       "timing": f"median of {n_blocks} blocks of {K} steps", "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": "ch_fused_rk4_kernel, 1 launch per RK4 step; achieved on the 104 B/cell-step "
-                                   "of the unfused method; traffic = ncu DRAM bytes per launch",
+                         "kernel": "ch_fused_rk4_kernel, 1 launch/step; achieved on 104 B/cell-step",
                          "fp64_Tops": FP64_OPS_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e12,
                          "fp64_frac_of_nominal": FP64_OPS_PER_CELL_STEP * cells / (ms_per_step / 1e3) / 1e12
                          / FP64_NOMINAL_TOPS},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mcell-steps/s", "h2d_bytes_per_step": cells * 8 / chunk,
                     "d2h_bytes_per_step": cells * 8 / chunk,
-                    "note": f"{n_chunks} chunks of {chunk} steps: pinned host -> device, gc_ch_integrate, "
-                            "device -> pinned host; two contexts on two streams"},
+                    "note": f"{n_chunks} x (H2D, {chunk} steps, D2H), 2 streams"},
             "gpu_launches": K * n_blocks,
             "clocks": clocks.summary(),
         }
+        line["roofline"] = {k: (_sig(v) if isinstance(v, float) and k != "peak" else v)
+                            for k, v in line["roofline"].items()}
         if summaries is not None:
             line["forms"] = summaries
         print(json.dumps(line), flush=True)
