@@ -57,7 +57,7 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
         objs = list(ex.map(lambda s: _compile(s, extra or []), srcs))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
-               "-L", CUDA_LIB, "-lcudart", "-lnvrtc", "-lcufft", "-Xlinker", f"-rpath,{CUDA_LIB}"]
+               "-L", CUDA_LIB, "-lcudart", "-lnvrtc", "-Xlinker", f"-rpath,{CUDA_LIB}"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -44,7 +44,6 @@ namespace gcb {
 namespace {
 
 constexpr int kFzThreads = 512;
-constexpr int kFzWarps = kFzThreads / 32;
 constexpr long long kFzWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
 
 constexpr size_t fz_al(size_t b) { return (b + 127) / 128 * 128; }

@@ -1,6 +1,6 @@
 // Drop-in for the reference header of the same path: spectral::partial,
 // laplacian, biharmonic and gradient (spectral/Derivatives.hpp) computed on
-// the GPU (cuFFT transforms around this library's multiplier kernel).  The
+// the GPU (this library's own FFT kernels around its multiplier kernel).  The
 // reference compiles these only with GRIDCALC_USE_FFT; here they are always
 // available.
 #pragma once

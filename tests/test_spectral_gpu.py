@@ -148,3 +148,32 @@ def test_two_contexts_on_two_streams_same_shape(gc):
             assert np.array_equal(outs[j].cpu().numpy(), want[j]), (rep, j)
     for c in ctxs:
         c.close()
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 64), (1, 2, 4096), (1, 3, 6000), (2, 96, 50)])
+def test_own_transform_lengths(gc, shape):
+    """The library's transforms at lengths the golden grids do not reach:
+    power-of-two lines (radix-2, up to 4096 with the line beyond 48 KB of
+    shared memory) and long non-power-of-two lines (direct DFT, 6000), against
+    torch's double-precision FFT of the same field."""
+    import torch
+    rng = np.random.default_rng(sum(shape))
+    f = rng.standard_normal(shape)
+    nz, ny, nx = shape
+    h = (0.5, 0.25, 1.0)
+    g = gc.Grid(nx, ny, nz, *h)
+    x = _dev(f)
+    ft = torch.from_numpy(f)
+    kx = torch.fft.rfftfreq(nx, d=h[0]) * 2 * np.pi
+    ky = torch.fft.fftfreq(ny, d=h[1]) * 2 * np.pi
+    kz = torch.fft.fftfreq(nz, d=h[2]) * 2 * np.pi
+    k2 = kx[None, None, :] ** 2 + ky[None, :, None] ** 2 + kz[:, None, None] ** 2
+    want = torch.fft.irfftn(-k2 * torch.fft.rfftn(ft), s=shape).numpy()
+    assert _close(_host(gc.spectral_laplacian(x, g)), want), shape
+    # d/dx: the Nyquist mode of an even axis is zeroed for an odd count
+    mult = 1j * kx[None, None, :]
+    if nx % 2 == 0:
+        mult = mult.clone()
+        mult[..., -1] = 0
+    want_dx = torch.fft.irfftn(mult * torch.fft.rfftn(ft), s=shape).numpy()
+    assert _close(_host(gc.spectral_partial(x, g, (1, 0, 0))), want_dx), shape
