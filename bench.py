@@ -742,6 +742,12 @@ def run_case(name: str) -> None:
         for i, (nx, ny, *_) in enumerate(members):
             b.set_member(i, 0.05 * (2 * rng.random((ny, nx)) - 1))
         b.run(16)
+    elif name == "batch256_f32":    # the batched form's ensemble (256 members, 46.4 M cells), FP32 order 4, 16 steps
+        members, ics = batch_members()
+        b = gc.ChBatch(members, order=4, dtype=torch.float32)
+        for i, c in enumerate(ics):
+            b.set_member(i, c)
+        b.run(16)
     elif name == "ch_f32_4096":     # plain FP32 RK4 CH, 4096^2 (two-column tiles)
         n = 4096
         g = gc.Grid(n, n, 1)
@@ -914,7 +920,7 @@ def main():
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--case", default=None,
                     help="run one small profiling workload and exit: conv_b16_512, learned_b1_512, lap2_384, fvm_256, "
-                         "batch64_f32, ch_f32_4096, fused_4096, eval_fe_320")
+                         "batch64_f32, batch256_f32, ch_f32_4096, fused_4096, eval_fe_320")
     ap.add_argument("--min-seconds", type=float, default=1.5,
                     help="repeat the K-step timed block until this much device time has passed")
     ap.add_argument("--forms", default="all",

@@ -11,8 +11,13 @@
 // steps are captured into a CUDA graph and replayed.  The tile shape comes
 // from a small set of compiled candidates; gc_ch_batch_autotune times each
 // on the actual ensemble and keeps the fastest (optionally recorded in a
-// JSON file keyed by device and ensemble).  Mass and free energy are
-// reduced per member in double with compensated sums in a fixed order.
+// JSON file keyed by device and ensemble).  One more candidate fuses the
+// four stages: a persistent launch per step in which a CTA stages each
+// (member, tile) work item's psi on the tile plus a halo of 8R cells and
+// runs all four stages in shared memory (as the single-grid fused step,
+// ch_fused.cu), so psi is read and psi' written once per step instead of 13
+// field passes.  Mass and free energy are reduced per member in double with
+// compensated sums in a fixed order.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -51,7 +56,10 @@ struct TileShape {
   int tw, ty, nty;
 };
 constexpr TileShape kShapes[] = {{32, 16, 4}, {64, 8, 4}, {64, 16, 4}, {64, 32, 8}};
-constexpr int kNumShapes = 4;
+constexpr int kNumStageShapes = 4;
+constexpr int kFusedShape = 4;   // the fused four-stage kernel (orders 2 and 4)
+constexpr int kNumShapes = 5;
+static_assert(kFusedShape == GC_BATCH_FUSED, "the C ABI's shape number of the fused kernel");
 
 // Work source of the ensemble: item k is (member, tile origin); the stage
 // selects the RK slots and coefficient (1..3 = RK4 stages writing k1..k3,
@@ -127,6 +135,185 @@ __global__ void __launch_bounds__(TW * NTY) ch_batch_x2_kernel(const Member<floa
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const BatchSource<float> src{members, items, n_items, buf, stage};
   pipelined_tiles_x2<ORDER, MODE, TW, TY, NTY>(src, smem_raw);
+}
+
+// ---- fused four-stage step ------------------------------------------------
+// Output tile 64 x TY (TY = 32 for float, 16 for double); frame = tile plus
+// H = 8R cells on every side, double-buffered so the next item's frame
+// arrives (cp.async, wrapped per element) while this one computes.  Stage S
+// forms mu on the tile plus hm = H - 2RS - R cells and k on hm - R, as in
+// ch_fused.cu; the arithmetic per cell is the stage kernels' (tap_sum in
+// tap order, lap_xy, the z term of orders above 2, chem_pot, mobility, the
+// same RK4 combination), so double members stay bit-identical to them.
+constexpr int kBfThreads = 512;
+
+template <class T, int ORDER>
+struct BfLayout {
+  static constexpr int R = W<2, ORDER>::R;
+  static constexpr int H = 8 * R;
+  static constexpr int TX = 64, TY = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+  static constexpr int YR0 = 2 * R, YROWS = SY - 2 * YR0;  // y buffer: frame rows [2R, SY - 2R)
+  static constexpr int MR0 = R, MROWS = SY - 2 * MR0;      // mu buffer: frame rows [R, SY - R)
+  static constexpr int FRAME = SX * SY;
+  static constexpr int OFF_Y = 2 * FRAME;
+  static constexpr int OFF_MU = OFF_Y + SX * YROWS;
+  static constexpr int OFF_K1 = OFF_MU + SX * MROWS;
+  static constexpr int OFF_K23 = OFF_K1 + TX * TY;
+  static constexpr size_t BYTES = sizeof(T) * static_cast<size_t>(OFF_K23 + TX * TY);
+};
+static_assert(BfLayout<float, 4>::BYTES <= 113 * 1024 && BfLayout<float, 2>::BYTES <= 113 * 1024 &&
+                  BfLayout<double, 2>::BYTES <= 113 * 1024,
+              "two CTAs per SM");
+static_assert(BfLayout<double, 4>::BYTES <= 227 * 1024, "one CTA per SM");
+
+// Cells of a W x NR region in column strips (thread t: column t % W, rows
+// [j RP, j RP + RP) with j = t / W < 512 / W); f(off, rr, cc, k) per cell in
+// order down the column, off its frame offset, k its index in the strip.
+template <int SX, int W, int NR, class F>
+__device__ __forceinline__ void bf_strips(int base, F&& f) {
+  constexpr int NS = kBfThreads / W;
+  constexpr int RP = (NR + NS - 1) / NS;
+  const int t = threadIdx.x, j = t / W, cc = t - j * W;
+  if (j < NS) {
+    const int r0 = j * RP;
+    int off = base + r0 * SX + cc;
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+      if (RP * NS == NR || r0 + k < NR) f(off, r0 + k, cc, k);
+      off += SX;
+    }
+  }
+}
+
+// Laplacian at frame offset off of buffer b (frame-indexed), centre c, with
+// the column window win (rows off - R SX .. off + R SX).
+template <class T, int ORDER, int NW>
+__device__ __forceinline__ T bf_lap(const StageParams<T>& p, const T* b, int off, T c, const T (&win)[NW]) {
+  constexpr int R = W<2, ORDER>::R;
+  const T ax = tap_sum<T, 2, ORDER>([&](int o) { return o == 0 ? c : b[off + o]; });
+  const T ay = tap_sum<T, 2, ORDER>([&](int o) { return win[R + o]; });
+  T lap = lap_xy(p, ax, ay);
+  if constexpr (ORDER != 2) lap = lap_z(p, lap, tap_sum<T, 2, ORDER>([&](int) { return c; }));
+  return lap;
+}
+
+template <class T, int ORDER, int S>
+__device__ __forceinline__ void bf_stage(const StageParams<T>& p, const Member<T>& m, T* out, const T* __restrict__ ps,
+                                         T* __restrict__ ys, T* __restrict__ ms, T* __restrict__ k1s,
+                                         T* __restrict__ k23s, int x0, int y0) {
+  using L = BfLayout<T, ORDER>;
+  constexpr int R = L::R, H = L::H, TX = L::TX, TY = L::TY, SX = L::SX, NW = 2 * R + 1;
+  constexpr int hm = H - 2 * R * S - R, hk = hm - R;
+  constexpr int YOFF = L::YR0 * SX, MOFF = L::MR0 * SX;
+  {  // mu = -y + y^3 - kappa lap(y)
+    constexpr int Wd = TX + 2 * hm, NR = TY + 2 * hm, B = H - hm;
+    const T* yb = S == 0 ? ps : ys - YOFF;
+    T win[NW];
+    bf_strips<SX, Wd, NR>(B * SX + B, [&](int off, int, int, int k) {
+      if (k == 0) {
+#pragma unroll
+        for (int q = 0; q < 2 * R; ++q) win[q + 1] = yb[off + (q - R) * SX];
+      }
+#pragma unroll
+      for (int z = 0; z + 1 < NW; ++z) win[z] = win[z + 1];
+      win[NW - 1] = yb[off + R * SX];
+      const T yc = win[R];
+      ms[off - MOFF] = chem_pot(p, yc, bf_lap<T, ORDER>(p, yb, off, yc, win));
+    });
+  }
+  __syncthreads();
+  {  // k = M lap(mu), then the stage's update
+    constexpr int Wd = TX + 2 * hk, NR = TY + 2 * hk, B = H - hk;
+    const T* mb = ms - MOFF;
+    T win[NW];
+    bf_strips<SX, Wd, NR>(B * SX + B, [&](int off, int rr, int cc, int k) {
+      if (k == 0) {
+#pragma unroll
+        for (int q = 0; q < 2 * R; ++q) win[q + 1] = mb[off + (q - R) * SX];
+      }
+#pragma unroll
+      for (int z = 0; z + 1 < NW; ++z) win[z] = win[z + 1];
+      win[NW - 1] = mb[off + R * SX];
+      const T mc = win[R];
+      const T rhs = mobility(p, bf_lap<T, ORDER>(p, mb, off, mc, win));
+      const T pc = ps[off];
+      if constexpr (S < 3) {
+        ys[off - YOFF] = Ar<T>::add(pc, Ar<T>::mul(S < 2 ? m.half : m.dt, rhs));
+        const int tr = rr - hk, tc = cc - hk;
+        if (static_cast<unsigned>(tr) < static_cast<unsigned>(TY) && static_cast<unsigned>(tc) < static_cast<unsigned>(TX)) {
+          const int t = tr * TX + tc;
+          if constexpr (S == 0) k1s[t] = rhs;
+          else if constexpr (S == 1) k23s[t] = rhs;
+          else k23s[t] = Ar<T>::add(k23s[t], rhs);
+        }
+      } else {  // the region is the tile
+        if (y0 + rr < p.ny && x0 + cc < p.nx) {
+          const int t = rr * TX + cc;
+          const T s14 = Ar<T>::add(k1s[t], rhs);
+          out[static_cast<size_t>(y0 + rr) * p.nx + (x0 + cc)] =
+              Ar<T>::add(pc, Ar<T>::add(Ar<T>::mul(m.sixth, s14), Ar<T>::mul(m.third, k23s[t])));
+        }
+      }
+    });
+  }
+  __syncthreads();
+}
+
+template <class T, int ORDER>
+__global__ void __launch_bounds__(kBfThreads) ch_batch_fused_kernel(const Member<T>* __restrict__ members,
+                                                                    const int4* __restrict__ items, int n_items,
+                                                                    const T* __restrict__ psi, T* __restrict__ dst) {
+  using L = BfLayout<T, ORDER>;
+  constexpr int H = L::H, SX = L::SX, FRAME = L::FRAME;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  T* ys = sm + L::OFF_Y;
+  T* ms = sm + L::OFF_MU;
+  T* k1s = sm + L::OFF_K1;
+  T* k23s = sm + L::OFF_K23;
+
+  auto issue = [&](int k, int b) {
+    const int4 w = items[k];
+    const Member<T> m = members[w.x];
+    const T* src = psi + m.off;
+    T* f = sm + b * FRAME;
+    for (int e = threadIdx.x; e < FRAME; e += kBfThreads) {
+      const int r = e / SX, c = e - r * SX;
+      cp_async_elem(f + e, src + static_cast<size_t>(wrap(w.z - H + r, m.ny)) * m.nx + wrap(w.y - H + c, m.nx),
+                    sizeof(T));
+    }
+  };
+
+  if (static_cast<int>(blockIdx.x) < n_items) issue(blockIdx.x, 0);
+  cp_async_commit();
+  int i = 0;
+  for (int k = blockIdx.x; k < n_items; k += gridDim.x, ++i) {
+    const int b = i & 1;
+    if (k + static_cast<int>(gridDim.x) < n_items) issue(k + gridDim.x, b ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();  // every thread's copies of this frame have landed
+    const int4 w = items[k];
+    const Member<T> m = members[w.x];
+    StageParams<T> p{};
+    p.nx = m.nx;
+    p.ny = m.ny;
+    p.nz = 1;
+    p.ihx2 = p.ihy2 = p.ihz2 = T(1);
+    p.unit_h = true;
+    p.mob = m.mob;
+    p.kappa = m.kappa;
+    p.unit_m = m.unit_m;
+    p.unit_k = m.unit_k;
+    const T* ps = sm + b * FRAME;
+    T* out = dst + m.off;
+    bf_stage<T, ORDER, 0>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
+    bf_stage<T, ORDER, 1>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
+    bf_stage<T, ORDER, 2>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
+    bf_stage<T, ORDER, 3>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
+  }
+  cp_async_wait<0>();
 }
 
 // ---- per-member FP64 diagnostics -----------------------------------------
@@ -234,7 +421,7 @@ struct gc_ch_batch {
   void* member_table = nullptr;
   void* items = nullptr;           // int4 work list for the current shape
   int n_items = 0;
-  int shape = 2;                   // index into kShapes
+  int shape = 2;                   // index into kShapes, or kFusedShape
   bool x2 = false;                 // float with all widths even: two-column tiles
   int items_shape = -1;
   void* diag_items = nullptr;
@@ -296,8 +483,23 @@ gc_status launch_batch_order(gc_ch_batch* b, const BatchBuffers<T>& buf, int sta
   }
 }
 
+template <class T, int ORDER>
+gc_status launch_batch_fused(gc_ch_batch* b, const T* src, T* dst) {
+  constexpr size_t smem = BfLayout<T, ORDER>::BYTES;
+  auto kern = ch_batch_fused_kernel<T, ORDER>;
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, kBfThreads, smem, &per_sm));
+  const int grid = std::max(1, std::min(b->n_items, per_sm * b->ctx->num_sms));
+  kern<<<grid, kBfThreads, smem, b->ctx->stream>>>(static_cast<const Member<T>*>(b->member_table),
+                                                  static_cast<const int4*>(b->items), b->n_items, src, dst);
+  GC_CHECK_LAUNCH("ch_batch_fused_kernel");
+  return GC_OK;
+}
+
 template <class T>
 gc_status batch_step(gc_ch_batch* b, const T* src, T* dst) {
+  if (b->shape == kFusedShape)
+    return b->order == 2 ? launch_batch_fused<T, 2>(b, src, dst) : launch_batch_fused<T, 4>(b, src, dst);
   BatchBuffers<T> buf{src, dst, static_cast<T*>(b->slots[2]), static_cast<T*>(b->slots[3]),
                       static_cast<T*>(b->slots[4])};
   gc_status s;
@@ -309,13 +511,19 @@ gc_status batch_step(gc_ch_batch* b, const T* src, T* dst) {
 // (Re)builds the (member, tile) work list for the current shape.
 gc_status build_items(gc_ch_batch* b) {
   if (b->items_shape == b->shape) return GC_OK;
-  const TileShape sh = kShapes[b->shape];
-  const int R = b->order / 2;
-  const int tx = (b->x2 ? 2 * sh.tw : sh.tw) - 2 * R;
+  int tx, ty;
+  if (b->shape == kFusedShape) {
+    tx = 64;
+    ty = b->dtype == GC_F32 ? BfLayout<float, 2>::TY : BfLayout<double, 2>::TY;
+  } else {
+    const TileShape sh = kShapes[b->shape];
+    tx = (b->x2 ? 2 * sh.tw : sh.tw) - b->order;  // the mu region less 2R columns
+    ty = sh.ty;
+  }
   std::vector<int4> items;
   for (int m = 0; m < b->n; ++m) {
     const int nx = b->members[m].nx, ny = b->members[m].ny;
-    for (int y0 = 0; y0 < ny; y0 += sh.ty)
+    for (int y0 = 0; y0 < ny; y0 += ty)
       for (int x0 = 0; x0 < nx; x0 += tx) items.push_back(make_int4(m, x0, y0, 0));
   }
   if (b->items) GC_CUDA(cudaFree(b->items));
@@ -404,6 +612,16 @@ gc_status diag_batch(gc_ch_batch* b, double* mass, double* energy) {
   return GC_OK;
 }
 
+// The fused kernel covers Laplacian orders 2 and 4 (its halo is 8R cells).
+bool shape_fits(const gc_ch_batch* b, int shape) { return shape != kFusedShape || b->order <= 4; }
+
+std::string shape_name(const gc_ch_batch* b, int shape) {
+  if (shape == kFusedShape)
+    return "fused64x" + std::to_string(b->dtype == GC_F32 ? BfLayout<float, 2>::TY : BfLayout<double, 2>::TY);
+  const TileShape s = kShapes[shape];
+  return std::to_string(s.tw) + "x" + std::to_string(s.ty) + "x" + std::to_string(s.nty);
+}
+
 std::string signature(const gc_ch_batch* b) {
   unsigned long long h = 1469598103934665603ULL;
   auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ULL; };
@@ -450,6 +668,12 @@ GC_API gc_status gc_ch_batch_create(gc_context* ctx, int32_t n, const gc_ch_memb
   b->members.assign(members, members + n);
   b->x2 = dt == GC_F32;
   for (int m = 0; m < n; ++m) b->x2 = b->x2 && members[m].nx % 2 == 0;
+  // Default shape, from the B200 trials on a 256-member ensemble (sides 64 to
+  // 1024): the fused kernel for float at orders 2 and 4 (74.5 / 43.5 G
+  // cell-steps/s against 48.9 / 39.7 for the best stage-kernel tile) and for
+  // double at order 2; the 64x16x4 stage tiles otherwise (double at order 4,
+  // where the fused frame allows one CTA per SM: 15.8 against 19.9 G).
+  b->shape = (order == 2 || (order == 4 && dt == GC_F32)) ? kFusedShape : 2;
   b->offsets.resize(n + 1);
   long long off = 0;
   for (int m = 0; m < n; ++m) {
@@ -512,6 +736,15 @@ GC_API gc_status gc_ch_batch_run(gc_ch_batch* b, int32_t n_steps) {
   return b->dtype == GC_F32 ? run_batch<float>(b, n_steps) : run_batch<double>(b, n_steps);
 }
 
+GC_API gc_status gc_ch_batch_set_shape(gc_ch_batch* b, int32_t shape) {
+  if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_set_shape: null batch");
+  if (shape < 0 || shape >= kNumShapes)
+    return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_set_shape: shape must be 0.." + std::to_string(kNumShapes - 1));
+  if (!shape_fits(b, shape)) return fail(GC_ERR_UNSUPPORTED, "gc_ch_batch_set_shape: the fused shape needs order 2 or 4");
+  b->shape = shape;
+  return GC_OK;
+}
+
 GC_API gc_status gc_ch_batch_diagnostics(gc_ch_batch* b, double* mass, double* free_energy) {
   if (!b) return fail(GC_ERR_INVALID_ARG, "gc_ch_batch_diagnostics: null batch");
   Call call(b->ctx);
@@ -542,7 +775,7 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
       const size_t pos = cache_text.find(key + ": {\"shape\": ");
       if (pos != std::string::npos) {
         const int shape = std::atoi(cache_text.c_str() + pos + key.size() + 12);
-        if (shape >= 0 && shape < kNumShapes) {
+        if (shape >= 0 && shape < kNumShapes && shape_fits(b, shape)) {
           b->shape = shape;
           b->tune_report = "{\"cached\": true, \"shape\": " + std::to_string(shape) + "}";
           if (report && report_len) std::snprintf(report, report_len, "%s", b->tune_report.c_str());
@@ -564,6 +797,7 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
   std::string rep = "{";
   gc_status st = GC_OK;
   for (int shp = 0; shp < kNumShapes && st == GC_OK; ++shp) {
+    if (!shape_fits(b, shp)) continue;
     b->shape = shp;
     // warm-up (captures the step graph for this shape), then a timed trial
     st = b->dtype == GC_F32 ? run_batch<float>(b, steps) : run_batch<double>(b, steps);
@@ -574,9 +808,8 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    const TileShape s = kShapes[shp];
     char item[128];
-    std::snprintf(item, sizeof item, "%s\"%dx%dx%d\": %.4f", shp ? ", " : "", s.tw, s.ty, s.nty, ms / steps);
+    std::snprintf(item, sizeof item, "%s\"%s\": %.4f", shp ? ", " : "", shape_name(b, shp).c_str(), ms / steps);
     rep += item;
     if (ms < best) {
       best = ms;
@@ -590,14 +823,12 @@ GC_API gc_status gc_ch_batch_autotune(gc_ch_batch* b, int32_t steps_per_trial, c
   cudaFree(saved);
   if (st != GC_OK) return st;
   b->shape = best_shape;
-  const TileShape s = kShapes[best_shape];
+  const std::string choice = shape_name(b, best_shape);
   char tail[160];
-  std::snprintf(tail, sizeof tail, "}, \"choice\": \"%dx%dx%d\", \"ms_per_step\": %.4f}", s.tw, s.ty, s.nty,
-                best / steps);
+  std::snprintf(tail, sizeof tail, "}, \"choice\": \"%s\", \"ms_per_step\": %.4f}", choice.c_str(), best / steps);
   b->tune_report = "{\"trials_ms_per_step\": " + rep + tail;
   if (cache_path && *cache_path) {
-    const std::string entry = key + ": {\"shape\": " + std::to_string(best_shape) + ", \"choice\": \"" +
-                              std::to_string(s.tw) + "x" + std::to_string(s.ty) + "x" + std::to_string(s.nty) +
+    const std::string entry = key + ": {\"shape\": " + std::to_string(best_shape) + ", \"choice\": \"" + choice +
                               "\", \"trials_ms_per_step\": " + rep + "}}";
     const size_t close = cache_text.rfind('}');
     std::string text;

@@ -71,6 +71,14 @@ struct EvalGrid {
 
 __device__ __forceinline__ double gc_integrand(const double* in);
 
+// Tap offsets in elements: 32-bit when every offset of the field fits
+// (GC_IDX32, set when components x cells < 2^31), else 64-bit.
+#ifdef GC_IDX32
+typedef int gc_ix;
+#else
+typedef gc_i64 gc_ix;
+#endif
+
 #define GC_R (GC_COMPS == 1 ? (GC_ARITY >= 4 ? 2 : GC_ARITY >= 2 ? 1 : 0) : (GC_ARITY >= 2 ? 1 : 0))
 #define GC_NIN (GC_COMPS == 1 ? (GC_ARITY == 1 ? 1 : GC_ARITY + 2) : (GC_ARITY == 1 ? 3 : 12))
 
@@ -93,17 +101,10 @@ __device__ __forceinline__ int gc_off(int i, int o, int n) {
   return o + (t < 0 ? n : 0) - (t >= n ? n : 0);
 }
 
-// Inputs of the arity and the integrand at the cell p points to; xo / yo /
-// zo are the flat offsets of its x, y and z taps.
-__device__ __forceinline__ double gc_eval_at(const EvalGrid& g, const GC_T* __restrict__ p, const gc_i64* xo,
-                                             const gc_i64* yo, const gc_i64* zo) {
-  auto v = [&](int comp, int ox, int oy, int oz) -> double {
-    gc_i64 off = (gc_i64)comp * g.n;
-    if (ox) off += xo[ox + GC_R];
-    if (oy) off += yo[oy + GC_R];
-    if (oz) off += zo[oz + GC_R];
-    return (double)__ldg(p + off);
-  };
+// Inputs of the arity and the integrand of one cell; v(comp, ox, oy, oz)
+// is the value of component comp at tap (ox, oy, oz) from the cell.
+template <class V>
+__device__ __forceinline__ double gc_eval_with(const EvalGrid& g, const V& v) {
   double in[GC_NIN];
 #if GC_COMPS == 1
   in[0] = v(0, 0, 0, 0);
@@ -169,17 +170,30 @@ __device__ __forceinline__ double gc_eval_at(const EvalGrid& g, const GC_T* __re
   return gc_integrand(in);
 }
 
-__device__ __forceinline__ void gc_yz_offsets(const EvalGrid& g, int j, int k, gc_i64* yo, gc_i64* zo) {
-  const gc_i64 plane = (gc_i64)g.nx * g.ny;
+// The integrand at the cell p points to; xo / yo / zo are the flat offsets
+// of its x, y and z taps.
+__device__ __forceinline__ double gc_eval_at(const EvalGrid& g, const GC_T* __restrict__ p, const gc_ix* xo,
+                                             const gc_ix* yo, const gc_ix* zo) {
+  return gc_eval_with(g, [&](int comp, int ox, int oy, int oz) -> double {
+    gc_ix off = (gc_ix)comp * (gc_ix)g.n;
+    if (ox) off += xo[ox + GC_R];
+    if (oy) off += yo[oy + GC_R];
+    if (oz) off += zo[oz + GC_R];
+    return (double)__ldg(p + off);
+  });
+}
+
+__device__ __forceinline__ void gc_yz_offsets(const EvalGrid& g, int j, int k, gc_ix* yo, gc_ix* zo) {
+  const gc_ix plane = (gc_ix)g.nx * (gc_ix)g.ny;
 #pragma unroll
   for (int m = 0; m <= 2 * GC_R; ++m) {
-    yo[m] = (gc_i64)gc_off(j, m - GC_R, g.ny) * g.nx;
-    zo[m] = (gc_i64)gc_off(k, m - GC_R, g.nz) * plane;
+    yo[m] = (gc_ix)gc_off(j, m - GC_R, g.ny) * (gc_ix)g.nx;
+    zo[m] = (gc_ix)gc_off(k, m - GC_R, g.nz) * plane;
   }
 }
 
 __device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, int j, int k) {
-  gc_i64 xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+  gc_ix xo[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
 #pragma unroll
   for (int m = 0; m <= 2 * GC_R; ++m) xo[m] = gc_off(i, m - GC_R, g.nx);
   gc_yz_offsets(g, j, k, yo, zo);
@@ -187,10 +201,10 @@ __device__ __forceinline__ double gc_cell(const EvalGrid& g, gc_i64 c, int i, in
 }
 
 // Cells (i, j, k) and (i + 1, j, k) of one row (i + 1 < nx): the y and z
-// offsets are formed once and the shared x taps are loaded once.
+// offsets are formed once.
 __device__ __forceinline__ void gc_cell_pair(const EvalGrid& g, gc_i64 c, int i, int j, int k, double& a,
                                              double& b) {
-  gc_i64 xa[2 * GC_R + 1], xb[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+  gc_ix xa[2 * GC_R + 1], xb[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
 #pragma unroll
   for (int m = 0; m <= 2 * GC_R; ++m) {
     xa[m] = gc_off(i, m - GC_R, g.nx);
@@ -201,6 +215,41 @@ __device__ __forceinline__ void gc_cell_pair(const EvalGrid& g, gc_i64 c, int i,
   a = gc_eval_at(g, p, xa, yo, zo);
   b = gc_eval_at(g, p + 1, xb, yo, zo);
 }
+
+#ifdef GC_PAIRS
+// The same pair when cell c is even, nx is even and the field is aligned to
+// two elements (GC_PAIRS): both cells' taps with the same (oy, oz) form one
+// aligned two-element load, so the pair reads each such tap once; only the
+// x taps outside the pair are single loads.
+__device__ __forceinline__ void gc_cell_pair_aligned(const EvalGrid& g, gc_i64 c, int i, int j, int k, double& a,
+                                                     double& b) {
+  gc_ix xa[2 * GC_R + 1], xb[2 * GC_R + 1], yo[2 * GC_R + 1], zo[2 * GC_R + 1];
+#pragma unroll
+  for (int m = 0; m <= 2 * GC_R; ++m) {
+    xa[m] = gc_off(i, m - GC_R, g.nx);
+    xb[m] = gc_off(i + 1, m - GC_R, g.nx);
+  }
+  gc_yz_offsets(g, j, k, yo, zo);
+  const GC_T* p = (const GC_T*)g.field + c;
+  auto yz = [&](int comp, int oy, int oz) -> gc_ix {
+    gc_ix off = (gc_ix)comp * (gc_ix)g.n;
+    if (oy) off += yo[oy + GC_R];
+    if (oz) off += zo[oz + GC_R];
+    return off;
+  };
+  auto pr = [&](int comp, int oy, int oz) -> GC_T2 { return __ldg((const GC_T2*)(p + yz(comp, oy, oz))); };
+  a = gc_eval_with(g, [&](int comp, int ox, int oy, int oz) -> double {
+    if (ox == 0) return (double)pr(comp, oy, oz).x;
+    if (ox == 1) return (double)pr(comp, oy, oz).y;
+    return (double)__ldg(p + yz(comp, oy, oz) + xa[ox + GC_R]);
+  });
+  b = gc_eval_with(g, [&](int comp, int ox, int oy, int oz) -> double {
+    if (ox == 0) return (double)pr(comp, oy, oz).y;
+    if (ox == -1) return (double)pr(comp, oy, oz).x;
+    return (double)__ldg(p + 1 + yz(comp, oy, oz) + xb[ox + GC_R]);
+  });
+}
+#endif
 
 // (i, j, k) += a step given as (di, dj, dk) with di < nx, dj < ny.
 __device__ __forceinline__ void gc_advance(int& i, int& j, int& k, int nx, int ny, int di, int dj, int dk) {
@@ -271,10 +320,17 @@ extern "C" __global__ void __launch_bounds__(512, GC_MIN_CTAS) gc_eval_pairwise(
     // Two consecutive cells per thread and iteration.
     int i, j, k;
     gc_locate(g, lo + 2 * threadIdx.x, i, j, k);
+#ifdef GC_PAIRS
+    const bool aligned = (lo & 1) == 0;
+#endif
     for (int e = 2 * threadIdx.x; e < len; e += 1024) {
       if (e + 1 < len && i + 1 < g.nx) {
         double a, b;
-        gc_cell_pair(g, lo + e, i, j, k, a, b);
+#ifdef GC_PAIRS
+        if (aligned) gc_cell_pair_aligned(g, lo + e, i, j, k, a, b);
+        else
+#endif
+          gc_cell_pair(g, lo + e, i, j, k, a, b);
         s[gc_padpos(e)] = a;
         s[gc_padpos(e + 1)] = b;
       } else {
@@ -462,8 +518,13 @@ std::string integrand_source(const gc_program* f) {
   return out;
 }
 
-std::string program_source(const gc_program* f, gc_dtype dt) {
+// idx32: every tap offset of the field fits in 32 bits; pairs: two-element
+// loads of cell pairs are aligned (even nx, field aligned to two elements).
+std::string program_source(const gc_program* f, gc_dtype dt, bool idx32, bool pairs) {
   std::string s = "#define GC_T " + std::string(dt == GC_F64 ? "double" : "float") + "\n";
+  s += "#define GC_T2 " + std::string(dt == GC_F64 ? "double2" : "float2") + "\n";
+  if (idx32) s += "#define GC_IDX32 1\n";
+  if (pairs) s += "#define GC_PAIRS 1\n";
   s += "#define GC_COMPS " + std::to_string(f->components) + "\n";
   s += "#define GC_ARITY " + std::to_string(f->arity) + "\n";
   s += "#define GC_MIN_CTAS " +
@@ -587,7 +648,7 @@ GC_API gc_status gc_evaluate_program(gc_context* ctx, const gc_grid* g, gc_dtype
 
 GC_API size_t gc_program_source(const gc_program* f, gc_dtype dt, char* buf, size_t cap) {
   if (!f || check_program(f) != GC_OK) return 0;
-  const std::string src = program_source(f, dt);
+  const std::string src = program_source(f, dt, false, false);
   if (buf && cap) {
     const size_t n = std::min(cap - 1, src.size());
     std::memcpy(buf, src.data(), n);
@@ -603,12 +664,15 @@ namespace gcb {
 gc_status run_program(gc_context* ctx, const gc_grid* g, gc_dtype dt, const void* field, const gc_program* f,
                       gc_sum sum, double* result) {
   gc_status s;
+  const long long n = static_cast<long long>(cells(g));
+  const size_t esize = dt == GC_F64 ? sizeof(double) : sizeof(float);
+  const bool idx32 = static_cast<long long>(f->components) * n < (1ll << 31);
+  const bool pairs = g->nx % 2 == 0 && reinterpret_cast<uintptr_t>(field) % (2 * esize) == 0;
   Compiled k;
-  if ((s = compile(ctx, program_source(f, dt), &k)) != GC_OK) return s;
+  if ((s = compile(ctx, program_source(f, dt, idx32, pairs), &k)) != GC_OK) return s;
   Driver drv;
   if ((s = driver(&drv)) != GC_OK) return s;
 
-  const long long n = static_cast<long long>(cells(g));
   EvalGrid a{};
   a.field = field;
   a.n = n;

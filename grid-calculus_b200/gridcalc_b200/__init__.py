@@ -107,6 +107,7 @@ _SIGS.update({
     "gc_ch_batch_run": [_vp, C.c_int32],
     "gc_ch_batch_diagnostics": [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "gc_ch_batch_autotune": [_vp, C.c_int32, C.c_char_p, C.c_char_p, C.c_size_t],
+    "gc_ch_batch_set_shape": [_vp, C.c_int32],
 })
 for _name, _args in _SIGS.items():
     _f = getattr(lib, _name)
@@ -613,6 +614,14 @@ class ChBatch:
 
     def run(self, n_steps: int) -> None:
         _check(lib.gc_ch_batch_run(self.handle, n_steps))
+
+    FUSED = 4   # GC_BATCH_FUSED: the fused four-stage kernel
+    SHAPES = ("32x16x4", "64x8x4", "64x16x4", "64x32x8")   # the stage kernels' tiles, 0..3
+
+    def set_shape(self, shape: int) -> None:
+        """Selects a tile shape: 0..3 the stage kernels' tiles (SHAPES),
+        FUSED the four-stage kernel (orders 2 and 4)."""
+        _check(lib.gc_ch_batch_set_shape(self.handle, shape))
 
     def diagnostics(self):
         """(mass, free_energy) per member, FP64 (reference convention)."""

@@ -373,13 +373,23 @@ GC_API gc_status gc_ch_batch_destroy(gc_ch_batch* b);
 GC_API gc_status gc_ch_batch_offsets(gc_ch_batch* b, int64_t* offsets);
 /* Device pointer to the packed state (fill it with gc_memcpy_h2d). */
 GC_API gc_status gc_ch_batch_state(gc_ch_batch* b, void** dev);
-/* Advances every member by n_steps RK4 steps: four persistent launches per
- * step cover the whole ensemble; steps replay from a captured CUDA graph. */
+/* Advances every member by n_steps RK4 steps; steps replay from a captured
+ * CUDA graph.  With the fused shape (GC_BATCH_FUSED, the default at
+ * Laplacian orders 2 and 4) one persistent launch per step runs all four
+ * stages of every (member, tile) work item in shared memory; the other
+ * shapes are four persistent launches per step, one per stage. */
 GC_API gc_status gc_ch_batch_run(gc_ch_batch* b, int32_t n_steps);
+/* Tile shapes: 0..3 the stage kernels' tiles (32x16x4, 64x8x4, 64x16x4,
+ * 64x32x8: threads in x, output rows, thread rows), GC_BATCH_FUSED the fused
+ * four-stage kernel (64 x 32 output tiles for float, 64 x 16 for double;
+ * orders 2 and 4 only, GC_ERR_UNSUPPORTED at order 6).  Results do not
+ * depend on the shape in double; in float they may differ in rounding. */
+#define GC_BATCH_FUSED 4
+GC_API gc_status gc_ch_batch_set_shape(gc_ch_batch* b, int32_t shape);
 /* Per-member mass and free energy (reference convention, order-2 gradient),
  * accumulated in double with compensated sums in a fixed order. */
 GC_API gc_status gc_ch_batch_diagnostics(gc_ch_batch* b, double* mass, double* free_energy);
-/* Times each compiled tile shape on the ensemble (steps_per_trial steps each,
+/* Times each tile shape that fits the order (steps_per_trial steps each,
  * state restored afterwards) and keeps the fastest; with cache_path, reuses
  * or records the choice in a JSON file keyed by device and ensemble.  A JSON
  * report of the trials is written to report. */

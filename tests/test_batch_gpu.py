@@ -32,10 +32,14 @@ def ics(members, seed=3):
     return out
 
 
+@pytest.mark.parametrize("shape", [2, 4], ids=["stage_kernels", "fused"])
 @pytest.mark.parametrize("order", [2, 4])
-def test_f64_ensemble_bit_exact_per_member(gc, oracle, order):
+def test_f64_ensemble_bit_exact_per_member(gc, oracle, order, shape):
+    """Both kernels (four stage launches per step, or the fused four-stage
+    launch) give every double member bit for bit the oracle's result."""
     import torch
     b = gc.ChBatch(MEMBERS, order=order, dtype=torch.float64)
+    b.set_shape(shape)
     init = ics(MEMBERS)
     for i, c0 in enumerate(init):
         b.set_member(i, c0)
@@ -46,11 +50,13 @@ def test_f64_ensemble_bit_exact_per_member(gc, oracle, order):
     b.close()
 
 
-def test_f32_ensemble_error_and_diagnostics(gc, oracle):
+@pytest.mark.parametrize("shape", [2, 4], ids=["stage_kernels", "fused"])
+def test_f32_ensemble_error_and_diagnostics(gc, oracle, shape):
     import torch
     members = [(nx, ny, 1.0, kap, stable_dt(kap)) for nx, ny, kap in
                [(64, 64, 0.5), (96, 80, 1.2), (128, 128, 2.0), (48, 112, 0.8)]]
     b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    b.set_shape(shape)
     init = [c.astype(np.float32).astype(np.float64) for c in ics(members, seed=11)]
     for i, c0 in enumerate(init):
         b.set_member(i, c0)
@@ -112,7 +118,7 @@ def test_autotune_and_cache(gc, oracle, tmp_path):
         b.set_member(i, c0)
     cache = str(tmp_path / "tune.json")
     report = json.loads(b.autotune(steps_per_trial=4, cache_path=cache))
-    assert set(report["trials_ms_per_step"]) == {"32x16x4", "64x8x4", "64x16x4", "64x32x8"}
+    assert set(report["trials_ms_per_step"]) == {"32x16x4", "64x8x4", "64x16x4", "64x32x8", "fused64x32"}
     assert report["choice"] in report["trials_ms_per_step"]
     # tuning restored the state
     assert np.array_equal(b.get_member(2), init[2].astype(np.float32).astype(np.float64))
@@ -124,7 +130,8 @@ def test_autotune_and_cache(gc, oracle, tmp_path):
     b2.close()
 
 
-def test_large_members(gc, oracle):
+@pytest.mark.parametrize("shape", [2, 4], ids=["stage_kernels", "fused"])
+def test_large_members(gc, oracle, shape):
     """Members at the top of the ensemble's size range (512^2 and 640 x 576):
     in double bit-identical to the oracle after 20 steps; in float, after
     1000 steps at each member's stable dt, within 1e-4 (L2) and 1e-5 (free
@@ -135,6 +142,7 @@ def test_large_members(gc, oracle):
                (640, 576, 1.0, 0.6, stable_dt(0.6))]
     init = ics(members, seed=21)
     b = gc.ChBatch(members, order=4, dtype=torch.float64)
+    b.set_shape(shape)
     for i, c0 in enumerate(init):
         b.set_member(i, c0)
     b.run(20)
@@ -144,6 +152,7 @@ def test_large_members(gc, oracle):
         assert np.array_equal(b.get_member(i), want.reshape(ny, nx)), i
     b.close()
     b = gc.ChBatch(members, order=4, dtype=torch.float32)
+    b.set_shape(shape)
     start = [c.astype(np.float32).astype(np.float64) for c in init]
     for i, c0 in enumerate(start):
         b.set_member(i, c0)
@@ -159,4 +168,20 @@ def test_large_members(gc, oracle):
         v4 = nx * ny / 4.0
         f_ref = gc.evaluate(want, g, "ch_free_energy", kappa=kap) + v4
         assert abs(energy[i] + v4 - f_ref) / abs(f_ref) < 1e-5, (i, energy[i] + v4, f_ref)
+    b.close()
+
+
+def test_shape_selection_errors(gc):
+    """The fused shape covers orders 2 and 4 only; shapes outside 0..4 are
+    rejected."""
+    import torch
+    b = gc.ChBatch([(32, 32, 1.0, 1.0, 0.001)], order=6, dtype=torch.float32)
+    with pytest.raises(gc.GcError) as ei:
+        b.set_shape(gc.ChBatch.FUSED)
+    assert ei.value.status == "GC_ERR_UNSUPPORTED"
+    with pytest.raises(gc.GcError) as ei:
+        b.set_shape(5)
+    assert ei.value.status == "GC_ERR_INVALID_ARG"
+    b.set_shape(3)
+    b.run(2)
     b.close()

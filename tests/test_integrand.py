@@ -161,15 +161,18 @@ def test_generated_sources_compile_for_sm100a():
             assert gc.lib.gc_program_source(C.byref(p), dt, buf, n) == n
             src = buf.value
             assert (b"#define GC_T double" if dt == gc.F64 else b"#define GC_T float") in src
-            h = C.c_void_p()
-            assert nv.nvrtcCreateProgram(C.byref(h), src, b"gc_integrand.cu", 0, None, None) == 0
-            rc = nv.nvrtcCompileProgram(h, 3, opts)
-            size = C.c_size_t()
-            nv.nvrtcGetProgramLogSize(h, C.byref(size))
-            log = C.create_string_buffer(size.value)
-            nv.nvrtcGetProgramLog(h, log)
-            nv.nvrtcDestroyProgram(C.byref(h))
-            assert rc == 0, (name, dt, log.value.decode())
+            # The variant for fields whose offsets fit 32 bits and whose cell
+            # pairs are aligned prepends two defines.
+            for variant in (src, b"#define GC_IDX32 1\n#define GC_PAIRS 1\n" + src):
+                h = C.c_void_p()
+                assert nv.nvrtcCreateProgram(C.byref(h), variant, b"gc_integrand.cu", 0, None, None) == 0
+                rc = nv.nvrtcCompileProgram(h, 3, opts)
+                size = C.c_size_t()
+                nv.nvrtcGetProgramLogSize(h, C.byref(size))
+                log = C.create_string_buffer(size.value)
+                nv.nvrtcGetProgramLog(h, log)
+                nv.nvrtcDestroyProgram(C.byref(h))
+                assert rc == 0, (name, dt, log.value.decode())
     bad = gc.gc_program(1, 1, 1, 0)
     bad.instr[0] = gc.gc_instr(2, 0, 0, 0, 0.0)   # reads a register never written
     assert gc.lib.gc_program_source(C.byref(bad), gc.F64, None, 0) == 0

@@ -164,9 +164,9 @@ def test_own_transform_lengths(gc, shape):
     g = gc.Grid(nx, ny, nz, *h)
     x = _dev(f)
     ft = torch.from_numpy(f)
-    kx = torch.fft.rfftfreq(nx, d=h[0]) * 2 * np.pi
-    ky = torch.fft.fftfreq(ny, d=h[1]) * 2 * np.pi
-    kz = torch.fft.fftfreq(nz, d=h[2]) * 2 * np.pi
+    kx = torch.fft.rfftfreq(nx, d=h[0], dtype=torch.float64) * 2 * np.pi   # (torch's default dtype is float32)
+    ky = torch.fft.fftfreq(ny, d=h[1], dtype=torch.float64) * 2 * np.pi
+    kz = torch.fft.fftfreq(nz, d=h[2], dtype=torch.float64) * 2 * np.pi
     k2 = kx[None, None, :] ** 2 + ky[None, :, None] ** 2 + kz[:, None, None] ** 2
     want = torch.fft.irfftn(-k2 * torch.fft.rfftn(ft), s=shape).numpy()
     assert _close(_host(gc.spectral_laplacian(x, g)), want), shape
