@@ -56,7 +56,6 @@ struct TileShape {
   int tw, ty, nty;
 };
 constexpr TileShape kShapes[] = {{32, 16, 4}, {64, 8, 4}, {64, 16, 4}, {64, 32, 8}};
-constexpr int kNumStageShapes = 4;
 constexpr int kFusedShape = 4;   // the fused four-stage kernel (orders 2 and 4)
 constexpr int kNumShapes = 5;
 static_assert(kFusedShape == GC_BATCH_FUSED, "the C ABI's shape number of the fused kernel");
