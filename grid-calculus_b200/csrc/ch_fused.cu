@@ -48,15 +48,16 @@ constexpr long long kFzWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
 
 constexpr size_t fz_al(size_t b) { return (b + 127) / 128 * 128; }
 
-// Tile of 64 x TY_ output cells: TY_ = 28 (two CTAs per SM) for grids with
-// enough tiles, TY_ = 16 (three CTAs per SM, more tiles) for small grids.
-template <int TY_>
+// Tile of TX_ x TY_ output cells: 64 x 28 (two CTAs per SM) for grids with
+// enough tiles, 64 x 16 (three CTAs per SM, more tiles) for small grids and
+// 32 x 16 for grids that 64 x 16 tiles would not spread over every SM.
+template <int TY_, int TX_ = 64>
 struct FzLayout {
   static constexpr int R = 1;
   static constexpr int H = 8 * R;         // four stages x 2R
-  static constexpr int TX = 64, TY = TY_;  // output tile
+  static constexpr int TX = TX_, TY = TY_;  // output tile
   static constexpr int CTAS_PER_SM = TY_ <= 16 ? 3 : 2;
-  static constexpr int SX = TX + 2 * H;   // frame row (80 doubles, 640 B)
+  static constexpr int SX = TX + 2 * H;   // frame row (80 doubles = 640 B at TX = 64)
   static constexpr int SY = TY + 2 * H;   // frame rows
   static constexpr int YR0 = 2 * R;       // first frame row the y buffer holds (halo 6R)
   static constexpr int YROWS = SY - 2 * YR0;
@@ -71,7 +72,9 @@ struct FzLayout {
   static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(double) * SX * SY);
 };
 static_assert(FzLayout<28>::BYTES <= 113 * 1024, "two CTAs per SM");
-static_assert(FzLayout<16>::BYTES <= 74 * 1024, "three CTAs per SM");
+static_assert(FzLayout<16>::BYTES <= 74 * 1024 && FzLayout<16, 32>::BYTES <= 74 * 1024, "three CTAs per SM");
+static_assert((FzLayout<16, 32>::SX * 8) % 16 == 0 && FzLayout<16, 32>::TX % 8 == 0,
+              "TMA box rows and x offsets stay 16-byte multiples");
 static_assert((FzLayout<28>::SX * 8) % 16 == 0 && FzLayout<28>::H % 2 == 0,
               "TMA box rows and x offsets stay 16-byte multiples");
 
@@ -88,9 +91,8 @@ struct FzParams {
 // it, j = t / W < NS, with NS = 512 / W strips of RP = ceil(NR / NS) rows.
 // f(off, rr, cc, k) for each of its cells in order down the column (k the
 // cell's index within the strip, for the caller's register window).
-template <int W, int NR, class F>
+template <int SX, int W, int NR, class F>
 __device__ __forceinline__ void fz_strips(int base, F&& f) {
-  constexpr int SX = FzLayout<28>::SX;  // the frame row is 80 doubles for every tile height
   constexpr int NS = kFzThreads / W;
   constexpr int RP = (NR + NS - 1) / NS;
   const int t = threadIdx.x, j = t / W, cc = t - j * W;
@@ -112,11 +114,11 @@ __device__ __forceinline__ void fz_strips(int base, F&& f) {
 // in registers, so a cell reads three values from shared memory (the new
 // row below, the two x neighbours).  UNIT: unit spacing, mobility and kappa
 // (the multiplies by 1 are skipped, as the stage kernels' exact shortcuts do).
-template <int TYT, int S, bool UNIT>
+template <int TYT, int TXT, int S, bool UNIT>
 __device__ __forceinline__ void fz_stage(const FzParams& a, const double* __restrict__ ps, double* __restrict__ ys,
                                          double* __restrict__ ms, double* __restrict__ k1s,
                                          double* __restrict__ k23s, int x0, int y0) {
-  using L = FzLayout<TYT>;
+  using L = FzLayout<TYT, TXT>;
   using T = double;
   constexpr int R = L::R, H = L::H, TX = L::TX, TY = L::TY, SX = L::SX;
   constexpr int hy = H - 2 * R * S, hm = hy - R, hk = hm - R;
@@ -128,7 +130,7 @@ __device__ __forceinline__ void fz_stage(const FzParams& a, const double* __rest
     constexpr int W = TX + 2 * hm, NR = TY + 2 * hm, B = H - hm;
     const T* yb = S == 0 ? ps : ys - YOFF;  // indexed by frame offset (valid rows only)
     T w0 = 0.0, w1 = 0.0;
-    fz_strips<W, NR>(B * SX + B, [&](int off, int, int, int k) {
+    fz_strips<SX, W, NR>(B * SX + B, [&](int off, int, int, int k) {
       if (k == 0) {
         w0 = yb[off - SX];
         w1 = yb[off];
@@ -154,7 +156,7 @@ __device__ __forceinline__ void fz_stage(const FzParams& a, const double* __rest
     constexpr int W = TX + 2 * hk, NR = TY + 2 * hk, B = H - hk;
     const T* mb = ms - MOFF;
     T w0 = 0.0, w1 = 0.0;
-    fz_strips<W, NR>(B * SX + B, [&](int off, int rr, int cc, int k) {
+    fz_strips<SX, W, NR>(B * SX + B, [&](int off, int rr, int cc, int k) {
       if (k == 0) {
         w0 = mb[off - SX];
         w1 = mb[off];
@@ -194,10 +196,10 @@ __device__ __forceinline__ void fz_stage(const FzParams& a, const double* __rest
   __syncthreads();
 }
 
-template <int TYT, bool UNIT>
-__global__ void __launch_bounds__(kFzThreads, FzLayout<TYT>::CTAS_PER_SM)
+template <int TYT, int TXT, bool UNIT>
+__global__ void __launch_bounds__(kFzThreads, FzLayout<TYT, TXT>::CTAS_PER_SM)
     ch_fused_rk4_kernel(const FzParams a, const __grid_constant__ CUtensorMap m_psi, int* status) {
-  using L = FzLayout<TYT>;
+  using L = FzLayout<TYT, TXT>;
   using T = double;
   constexpr int H = L::H, TX = L::TX, TY = L::TY, SX = L::SX, SY = L::SY;
   extern __shared__ unsigned char smem_raw[];
@@ -260,10 +262,10 @@ __global__ void __launch_bounds__(kFzThreads, FzLayout<TYT>::CTAS_PER_SM)
     }
     __syncthreads();
     if (*s_abort) break;
-    fz_stage<TYT, 0, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
-    fz_stage<TYT, 1, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
-    fz_stage<TYT, 2, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
-    fz_stage<TYT, 3, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<TYT, TXT, 0, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<TYT, TXT, 1, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<TYT, TXT, 2, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
+    fz_stage<TYT, TXT, 3, UNIT>(a, ps, ys, ms, k1s, k23s, x0, y0);
   }
 }
 
@@ -271,14 +273,14 @@ __global__ void __launch_bounds__(kFzThreads, FzLayout<TYT>::CTAS_PER_SM)
 
 namespace {
 
-template <int TYT>
+template <int TYT, int TXT>
 gc_status fz_launch(gc_context* ctx, const gc_grid* g, FzParams a, bool unit) {
-  using L = FzLayout<TYT>;
+  using L = FzLayout<TYT, TXT>;
   CUtensorMap m{};
   if (!make_tensor_map_2d(&m, a.psi, g->nx, g->ny, 8, L::SX, L::SY)) return GC_ERR_UNSUPPORTED;
   a.tiles_x = div_up(g->nx, L::TX);
   a.tiles_y = div_up(g->ny, L::TY);
-  auto kern = unit ? ch_fused_rk4_kernel<TYT, true> : ch_fused_rk4_kernel<TYT, false>;
+  auto kern = unit ? ch_fused_rk4_kernel<TYT, TXT, true> : ch_fused_rk4_kernel<TYT, TXT, false>;
   int per_sm = 1;
   GC_TRY(kernel_setup(kern, kFzThreads, L::BYTES, &per_sm));
   const long long ntiles = static_cast<long long>(a.tiles_x) * a.tiles_y;
@@ -293,14 +295,15 @@ gc_status fz_launch(gc_context* ctx, const gc_grid* g, FzParams a, bool unit) {
 gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const double* src, double* dst,
                         double dt, bool* done) {
   *done = false;
-  if (g->nz != 1 || cp->order != 2 || g->nx < FzLayout<16>::SX || g->ny < FzLayout<16>::SY) return GC_OK;
+  if (g->nz != 1 || cp->order != 2 || g->nx < FzLayout<16, 32>::SX || g->ny < FzLayout<16, 32>::SY) return GC_OK;
   // Measured on B200 per RK4 step (fused with 64 x 28 tiles / fused with
   // 64 x 16 tiles / four stage kernels): 256^2 9.2 / 7.2 / 24.5 us, 512^2
   // 13.3 / 10.0 / 24.4, 1024^2 22.8 / 28.2 / 45.7, 4096^2 311 / 362 / 427,
   // 8192^2 1196 / 1415 / 1553.  The taller tiles halve the halo's share of
   // the work; the shorter ones make more tiles and fit three CTAs per SM,
   // which pays while 64 x 28 tiles would fill fewer than two rounds of the
-  // persistent CTAs.
+  // persistent CTAs.  32 x 16 tiles, on grids that 64 x 16 tiles would not
+  // spread over every SM: 128^2 6.8 -> 5.5 us, 256^2 7.1 -> 5.4 us.
   FzParams a{};
   StageParams<double>& p = a.p;
   p.nx = g->nx; p.ny = g->ny; p.nz = 1;
@@ -320,8 +323,12 @@ gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* c
   a.c3 = dt / 3.0;
   const bool unit = p.unit_h && p.unit_m && p.unit_k;
   const long long tiles28 = static_cast<long long>(div_up(g->nx, 64)) * div_up(g->ny, 28);
+  const long long tiles16 = static_cast<long long>(div_up(g->nx, 64)) * div_up(g->ny, 16);
   const bool tall = g->ny >= FzLayout<28>::SY && tiles28 >= 2LL * FzLayout<28>::CTAS_PER_SM * ctx->num_sms;
-  const gc_status s = tall ? fz_launch<28>(ctx, g, a, unit) : fz_launch<16>(ctx, g, a, unit);
+  const bool narrow = g->nx < FzLayout<16>::SX || tiles16 < ctx->num_sms;
+  const gc_status s = tall     ? fz_launch<28, 64>(ctx, g, a, unit)
+                      : narrow ? fz_launch<16, 32>(ctx, g, a, unit)
+                               : fz_launch<16, 64>(ctx, g, a, unit);
   if (s == GC_ERR_UNSUPPORTED) return GC_OK;  // layout unfit for TMA: the stage kernels run
   if (s != GC_OK) return s;
   *done = true;
