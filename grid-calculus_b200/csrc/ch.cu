@@ -828,12 +828,11 @@ StageParams<T> base_params(const gc_grid* g, const gc_ch_params* cp) {
 template <class T>
 gc_status enqueue_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const T* src,
                        T* dst, T* k1, T* k2, T* k3, double dt, gc_integrator integ) {
-  if constexpr (sizeof(T) == 8) {
-    if (integ == GC_RK4 && ctx->fused_step) {
-      bool done = false;
-      GC_TRY(ch_fused_step(ctx, g, cp, src, dst, dt, &done));
-      if (done) return GC_OK;
-    }
+  if (integ == GC_RK4 && ctx->fused_step) {
+    bool done = false;
+    if constexpr (sizeof(T) == 8) GC_TRY(ch_fused_step(ctx, g, cp, src, dst, dt, &done));
+    else GC_TRY(ch_fused_step_f32(ctx, g, cp, src, dst, dt, &done));
+    if (done) return GC_OK;
   }
   StageParams<T> p = base_params<T>(g, cp);
   p.psi = src;

@@ -259,10 +259,53 @@ __device__ __forceinline__ void bf_stage(const StageParams<T>& p, const Member<T
   __syncthreads();
 }
 
+// Work sources of the fused walk.  item(k, m, x0, y0) gives item k's member
+// (extents, offset, coefficients) and tile origin; params(m) its stage
+// parameters.  The ensemble reads both from device tables (unit spacing);
+// a single grid is one member with the grid's own spacing, tiled by index.
+template <class T>
+struct BfItems {
+  const Member<T>* members;
+  const int4* items;
+  int n;
+  __device__ int count() const { return n; }
+  __device__ void item(int k, Member<T>& m, int& x0, int& y0) const {
+    const int4 w = items[k];
+    m = members[w.x];
+    x0 = w.y;
+    y0 = w.z;
+  }
+  __device__ StageParams<T> params(const Member<T>& m) const {
+    StageParams<T> p{};
+    p.nx = m.nx;
+    p.ny = m.ny;
+    p.nz = 1;
+    p.ihx2 = p.ihy2 = p.ihz2 = T(1);
+    p.unit_h = true;
+    p.mob = m.mob;
+    p.kappa = m.kappa;
+    p.unit_m = m.unit_m;
+    p.unit_k = m.unit_k;
+    return p;
+  }
+};
+
 template <class T, int ORDER>
-__global__ void __launch_bounds__(kBfThreads) ch_batch_fused_kernel(const Member<T>* __restrict__ members,
-                                                                    const int4* __restrict__ items, int n_items,
-                                                                    const T* __restrict__ psi, T* __restrict__ dst) {
+struct BfGrid {
+  Member<T> m;      // the grid as a member at offset 0
+  StageParams<T> p; // with its spacing
+  int tiles_x, n;
+  __device__ int count() const { return n; }
+  __device__ void item(int k, Member<T>& mm, int& x0, int& y0) const {
+    mm = m;
+    x0 = (k % tiles_x) * BfLayout<T, ORDER>::TX;
+    y0 = (k / tiles_x) * BfLayout<T, ORDER>::TY;
+  }
+  __device__ StageParams<T> params(const Member<T>&) const { return p; }
+};
+
+template <class T, int ORDER, class Src>
+__device__ __forceinline__ void bf_walk(const Src& src, const T* __restrict__ psi, T* __restrict__ dst) {
   using L = BfLayout<T, ORDER>;
   constexpr int H = L::H, SX = L::SX, FRAME = L::FRAME;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -271,15 +314,17 @@ __global__ void __launch_bounds__(kBfThreads) ch_batch_fused_kernel(const Member
   T* ms = sm + L::OFF_MU;
   T* k1s = sm + L::OFF_K1;
   T* k23s = sm + L::OFF_K23;
+  const int n_items = src.count();
 
   auto issue = [&](int k, int b) {
-    const int4 w = items[k];
-    const Member<T> m = members[w.x];
-    const T* src = psi + m.off;
+    Member<T> m;
+    int x0, y0;
+    src.item(k, m, x0, y0);
+    const T* f0 = psi + m.off;
     T* f = sm + b * FRAME;
     for (int e = threadIdx.x; e < FRAME; e += kBfThreads) {
       const int r = e / SX, c = e - r * SX;
-      cp_async_elem(f + e, src + static_cast<size_t>(wrap(w.z - H + r, m.ny)) * m.nx + wrap(w.y - H + c, m.nx),
+      cp_async_elem(f + e, f0 + static_cast<size_t>(wrap(y0 - H + r, m.ny)) * m.nx + wrap(x0 - H + c, m.nx),
                     sizeof(T));
     }
   };
@@ -293,26 +338,34 @@ __global__ void __launch_bounds__(kBfThreads) ch_batch_fused_kernel(const Member
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();  // every thread's copies of this frame have landed
-    const int4 w = items[k];
-    const Member<T> m = members[w.x];
-    StageParams<T> p{};
-    p.nx = m.nx;
-    p.ny = m.ny;
-    p.nz = 1;
-    p.ihx2 = p.ihy2 = p.ihz2 = T(1);
-    p.unit_h = true;
-    p.mob = m.mob;
-    p.kappa = m.kappa;
-    p.unit_m = m.unit_m;
-    p.unit_k = m.unit_k;
+    Member<T> m;
+    int x0, y0;
+    src.item(k, m, x0, y0);
+    const StageParams<T> p = src.params(m);
     const T* ps = sm + b * FRAME;
     T* out = dst + m.off;
-    bf_stage<T, ORDER, 0>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
-    bf_stage<T, ORDER, 1>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
-    bf_stage<T, ORDER, 2>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
-    bf_stage<T, ORDER, 3>(p, m, out, ps, ys, ms, k1s, k23s, w.y, w.z);
+    bf_stage<T, ORDER, 0>(p, m, out, ps, ys, ms, k1s, k23s, x0, y0);
+    bf_stage<T, ORDER, 1>(p, m, out, ps, ys, ms, k1s, k23s, x0, y0);
+    bf_stage<T, ORDER, 2>(p, m, out, ps, ys, ms, k1s, k23s, x0, y0);
+    bf_stage<T, ORDER, 3>(p, m, out, ps, ys, ms, k1s, k23s, x0, y0);
   }
   cp_async_wait<0>();
+}
+
+template <class T, int ORDER>
+__global__ void __launch_bounds__(kBfThreads) ch_batch_fused_kernel(const Member<T>* __restrict__ members,
+                                                                    const int4* __restrict__ items, int n_items,
+                                                                    const T* __restrict__ psi, T* __restrict__ dst) {
+  bf_walk<T, ORDER>(BfItems<T>{members, items, n_items}, psi, dst);
+}
+
+// The same fused step on one 2-D grid (float storage, orders 2 and 4): the
+// single-grid RK4 path's step when the context's fused step is on.
+template <int ORDER>
+__global__ void __launch_bounds__(kBfThreads) ch_fused_f32_kernel(const BfGrid<float, ORDER> src,
+                                                                  const float* __restrict__ psi,
+                                                                  float* __restrict__ dst) {
+  bf_walk<float, ORDER>(src, psi, dst);
 }
 
 // ---- per-member FP64 diagnostics -----------------------------------------
@@ -495,6 +548,46 @@ gc_status launch_batch_fused(gc_ch_batch* b, const T* src, T* dst) {
   return GC_OK;
 }
 
+template <int ORDER>
+gc_status fused_f32_launch(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const float* src, float* dst,
+                           double dt) {
+  using L = BfLayout<float, ORDER>;
+  BfGrid<float, ORDER> a{};
+  Member<float>& m = a.m;
+  m.nx = g->nx;
+  m.ny = g->ny;
+  m.off = 0;
+  m.dt = static_cast<float>(dt);
+  m.half = static_cast<float>(0.5 * dt);
+  m.sixth = static_cast<float>(dt / 6.0);
+  m.third = static_cast<float>(dt / 3.0);
+  m.kappa = static_cast<float>(cp->kappa);
+  m.mob = static_cast<float>(cp->mobility);
+  m.unit_m = m.mob == 1.f;
+  m.unit_k = m.kappa == 1.f;
+  StageParams<float>& p = a.p;  // as the stage kernels form them (ch.cu base_params)
+  p.nx = g->nx;
+  p.ny = g->ny;
+  p.nz = 1;
+  p.ihx2 = static_cast<float>(1.0 / (g->hx * g->hx));
+  p.ihy2 = static_cast<float>(1.0 / (g->hy * g->hy));
+  p.ihz2 = static_cast<float>(1.0 / (g->hz * g->hz));
+  p.mob = m.mob;
+  p.kappa = m.kappa;
+  p.unit_h = p.ihx2 == 1.f && p.ihy2 == 1.f && p.ihz2 == 1.f;
+  p.unit_m = m.unit_m;
+  p.unit_k = m.unit_k;
+  a.tiles_x = div_up(g->nx, L::TX);
+  a.n = a.tiles_x * div_up(g->ny, L::TY);
+  auto kern = ch_fused_f32_kernel<ORDER>;
+  int per_sm = 1;
+  GC_TRY(kernel_setup(kern, kBfThreads, L::BYTES, &per_sm));
+  const int grid = std::max(1, std::min(a.n, per_sm * ctx->num_sms));
+  kern<<<grid, kBfThreads, L::BYTES, ctx->stream>>>(a, src, dst);
+  GC_CHECK_LAUNCH("ch_fused_f32_kernel");
+  return GC_OK;
+}
+
 template <class T>
 gc_status batch_step(gc_ch_batch* b, const T* src, T* dst) {
   if (b->shape == kFusedShape)
@@ -638,6 +731,19 @@ std::string signature(const gc_ch_batch* b) {
 }
 
 }  // namespace
+}  // namespace gcb
+
+namespace gcb {
+
+gc_status ch_fused_step_f32(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const float* src, float* dst,
+                            double dt, bool* done) {
+  *done = false;
+  if (g->nz != 1 || (cp->order != 2 && cp->order != 4)) return GC_OK;
+  GC_TRY(cp->order == 2 ? fused_f32_launch<2>(ctx, g, cp, src, dst, dt) : fused_f32_launch<4>(ctx, g, cp, src, dst, dt));
+  *done = true;
+  return GC_OK;
+}
+
 }  // namespace gcb
 
 extern "C" {

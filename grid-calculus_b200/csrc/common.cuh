@@ -112,6 +112,10 @@ gc_status ch_cluster_integrate(gc_context* ctx, const gc_grid* g, gc_dtype dt, c
 // or its layout does not suit it, use the stage kernels).
 gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const double* src, double* dst,
                         double dt, bool* done);
+// The same for a 2-D float grid at order 2 or 4 (ch_batch.cu: the ensemble's
+// fused tile walk over one grid).
+gc_status ch_fused_step_f32(gc_context* ctx, const gc_grid* g, const gc_ch_params* cp, const float* src, float* dst,
+                            double dt, bool* done);
 
 // Opts kernel `kern` into `smem` bytes of dynamic shared memory on the
 // current device and, with ctas_per_sm, returns how many CTAs of `threads`

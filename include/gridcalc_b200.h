@@ -96,10 +96,11 @@ GC_API gc_status gc_context_destroy(gc_context* ctx);
  *     size (128^2: 9.2 against 13.1 us per RK4 step).  Same values, bit for
  *     bit in double.
  *   GC_OPT_FUSED_STEP (default 1): gc_ch_integrate runs each RK4 step of a
- *     2-D double grid at order 2 as one fused kernel (all four stages on a
- *     tile with an 8-cell halo in shared memory; psi read and psi' written
- *     once per step); 0 uses the four stage kernels.  Same values, bit for
- *     bit. */
+ *     2-D double grid at order 2, and of a 2-D float grid at order 2 or 4,
+ *     as one fused kernel (all four stages on a tile with a halo of 8R cells
+ *     in shared memory; psi read and psi' written once per step); 0 uses
+ *     the four stage kernels.  Same values, bit for bit, in double; in
+ *     float the two may differ in rounding. */
 typedef enum gc_option { GC_OPT_CLUSTER_STEPPING = 0, GC_OPT_FUSED_STEP = 1 } gc_option;
 GC_API gc_status gc_context_set_option(gc_context* ctx, int32_t option, int32_t value);
 GC_API gc_status gc_synchronize(gc_context* ctx);
@@ -301,8 +302,9 @@ GC_API gc_status gc_ch_rhs(gc_context* ctx, const gc_grid* g, gc_dtype dt,
  * (solve/RK4.hpp:99-154, solve/ExplicitEuler.hpp:79-112) with the
  * Cahn-Hilliard RHS, psi advanced in place.  RK4 runs four fused stage
  * kernels per step (each reads and writes every field once); the steps are
- * replayed from a captured CUDA graph (a 2-D double grid at order 2 runs one
- * fused kernel per step instead, GC_OPT_FUSED_STEP).  With
+ * replayed from a captured CUDA graph (a 2-D double grid at order 2, or a
+ * 2-D float grid at order 2 or 4, runs one fused kernel per step instead,
+ * GC_OPT_FUSED_STEP).  With
  * GC_OPT_CLUSTER_STEPPING on, a 2-D grid whose state fits in one
  * thread-block cluster's shared memory (gc_ch_cluster_ctas > 0) runs all
  * n_steps in one cluster-resident launch. */
