@@ -4,7 +4,8 @@ Headline workload: the plain method -- explicit RK4 Cahn-Hilliard, FP64,
 order-2 Laplacian applied twice, M = kappa = 1, dx = 1, dt = 0.01, initial
 c = U[-0.05, 0.05] from a seed -- on a 2-D periodic 8192 x 8192 grid (each
 field 512 MiB, far beyond the 126 MB L2, so every step streams from HBM).
-One "step" is one RK4 step (four fused stage kernels).  Metric: Mcell-steps/s.
+One "step" is one RK4 step (one launch of the fused step kernel, all four
+stages on a tile in shared memory).  Metric: Mcell-steps/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -717,10 +718,10 @@ def run_case(name: str) -> None:
         c = torch.from_numpy(L.initial_condition(9000, 512)).cuda()[None].contiguous()
         for _ in range(3):
             net.forward(c)
-    elif name == "lap2_384":        # 3-D laplacian order 2, 384^3 FP64 (plane ring)
-        n = 384
+    elif name in ("lap2_384", "lap2_f32_512"):  # 3-D laplacian order 2 (plane ring): 384^3 FP64 / 512^3 FP32
+        n = 384 if name == "lap2_384" else 512
         g = gc.Grid(n, n, n, 1 / n, 1 / n, 1 / n)
-        f = torch.rand(n, n, n, device="cuda", dtype=torch.float64)
+        f = torch.rand(n, n, n, device="cuda", dtype=torch.float64 if name == "lap2_384" else torch.float32)
         out = torch.empty_like(f)
         for _ in range(3):
             gc.laplacian(f, g, 2, out)
@@ -748,8 +749,8 @@ def run_case(name: str) -> None:
         for i, c in enumerate(ics):
             b.set_member(i, c)
         b.run(16)
-    elif name == "ch_f32_4096":     # plain FP32 RK4 CH, 4096^2 (two-column tiles)
-        n = 4096
+    elif name in ("ch_f32_4096", "ch_f32_8192"):  # plain FP32 RK4 CH, order 2 (fused step kernel), 4096^2 / 8192^2
+        n = 4096 if name == "ch_f32_4096" else 8192
         g = gc.Grid(n, n, 1)
         x = (0.05 * (2 * torch.rand(1, n, n, device="cuda", dtype=torch.float64) - 1)).float()
         gc.ch_integrate(x, g, gc.CahnHilliardRhs(1.0, 1.0, 2), DT, 32, gc.RK4)
@@ -924,7 +925,7 @@ def main():
     ap.add_argument("--grid", type=int, default=NX, help="side of the square grid (default 8192)")
     ap.add_argument("--case", default=None,
                     help="run one small profiling workload and exit: conv_b16_512, learned_b1_512, lap2_384, fvm_256, "
-                         "batch64_f32, batch256_f32, ch_f32_4096, fused_4096, eval_fe_320")
+                         "batch64_f32, batch256_f32, ch_f32_4096, ch_f32_8192, fused_4096, eval_fe_320, lap2_f32_512")
     ap.add_argument("--min-seconds", type=float, default=1.5,
                     help="repeat the K-step timed block until this much device time has passed")
     ap.add_argument("--forms", default="all",
