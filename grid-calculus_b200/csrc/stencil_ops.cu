@@ -315,11 +315,27 @@ __device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, int byt
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// Tile rows: the 32 x 8 threads cover 8 * CPT rows, each thread CPT cells of
+// its column per plane, so the per-plane work (the wait, the barrier, the
+// ring-slot arithmetic and the copy bookkeeping) is shared by CPT cells.  One
+// cell per thread and plane left the float kernel bound by that work (105
+// instructions per cell at 83 % issue).  Measured on B200 at 512^3, ms per
+// launch for CPT = 1 / 2 / 4 (float) and 1 / 2 (double): float laplacian
+// order 2 0.466 / 0.368 / 0.309, order 4 0.583 / 0.478 / 0.443, biharmonic
+// 0.726 / 0.669 / 0.642; double laplacian order 2 0.500 / 0.455, order 4
+// 0.755 / 0.766, biharmonic 1.041 / 1.074 (at radius 2 the taller double
+// ring costs more occupancy than the shared work saves).
+template <class T, int R>
+__host__ __device__ constexpr int zring_cpt() {
+  return sizeof(T) == 4 ? 4 : (R == 1 ? 2 : 1);
+}
+
 template <class T, int OP, int ORDER>
 __global__ void __launch_bounds__(NT) zring_kernel(const OpParams<T> p) {
   constexpr int R = OpShape<OP, ORDER>::R;
   constexpr int NF = OpShape<OP, ORDER>::NF;
-  constexpr int PW = BX + 2 * R, PH = BY + 2 * R, PS = PW * PH;
+  constexpr int CPT = zring_cpt<T, R>(), TY = BY * CPT;
+  constexpr int PW = BX + 2 * R, PH = TY + 2 * R, PS = PW * PH;
   constexpr int NB = 2 * R + 1 + kRing;
   constexpr int EPT = (PS + NT - 1) / NT;  // staged elements per thread per plane and field
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -327,7 +343,7 @@ __global__ void __launch_bounds__(NT) zring_kernel(const OpParams<T> p) {
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
-  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * TY;
   const int z0 = blockIdx.z * p.zc;
   const int z1 = min(z0 + p.zc, nz);
   const size_t plane = static_cast<size_t>(nx) * ny;
@@ -342,11 +358,16 @@ __global__ void __launch_bounds__(NT) zring_kernel(const OpParams<T> p) {
     const int r = idx / PW, cc = idx - r * PW;
     goff[e] = idx < PS ? static_cast<size_t>(wrap(y0 - R + r, ny)) * nx + wrap(x0 - R + cc, nx) : 0;
   }
-  auto slot_of = [&](int z) { return (z - z0 + R) % NB; };
-  auto issue = [&](int z) {  // plane z (wrapped) into its slot, as one commit group
+  // Slot of plane z + d from the slot s0 of plane z (|d| < NB).
+  auto slot_at = [](int s0, int d) {
+    int s = s0 + d;
+    s += s < 0 ? NB : 0;
+    s -= s >= NB ? NB : 0;
+    return s;
+  };
+  auto issue = [&](int z, int sl) {  // plane z (wrapped) into slot sl, as one commit group
     if (z <= z1 - 1 + R) {
       const size_t zo = static_cast<size_t>(wrap(z, nz)) * plane;
-      const int sl = slot_of(z);
 #pragma unroll
       for (int f = 0; f < NF; ++f)
 #pragma unroll
@@ -356,20 +377,31 @@ __global__ void __launch_bounds__(NT) zring_kernel(const OpParams<T> p) {
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
 
-  for (int z = z0 - R; z < z0 + R + kRing; ++z) issue(z);
-  const int gx = x0 + tx, gy = y0 + ty;
-  const bool active = gx < nx && gy < ny;
+  // Plane z0 - R + j goes to slot j, so plane z sits in slot (z - z0 + R) mod NB.
+  for (int j = 0; j < 2 * R + kRing; ++j) issue(z0 - R + j, j);
+  const int gx = x0 + tx;
+  int s0 = R;  // slot of plane z
   for (int z = z0; z < z1; ++z) {
     // plane z + R landed: the kRing - 1 later groups may still be in flight
     asm volatile("cp.async.wait_group %0;" ::"n"(kRing - 1) : "memory");
     __syncthreads();
-    if (active) {
-      auto at = [&](int f, int dx, int dy, int dz) -> T {
-        return ring[(f * NB + slot_of(z + dz)) * PS + (ty + R + dy) * PW + (tx + R + dx)];
-      };
-      cell_op<T, OP, ORDER, true>(p, static_cast<size_t>(z) * plane + static_cast<size_t>(gy) * nx + gx, at);
+    int sl[2 * R + 1];
+#pragma unroll
+    for (int d = -R; d <= R; ++d) sl[d + R] = slot_at(s0, d);
+#pragma unroll
+    for (int q = 0; q < CPT; ++q) {
+      const int row = ty + q * BY, gy = y0 + row;
+      if (gx < nx && gy < ny) {
+        auto at = [&](int f, int dx, int dy, int dz) -> T {
+          return ring[(f * NB + sl[dz + R]) * PS + (row + R + dy) * PW + (tx + R + dx)];
+        };
+        cell_op<T, OP, ORDER, true>(p, static_cast<size_t>(z) * plane + static_cast<size_t>(gy) * nx + gx, at);
+      }
     }
-    issue(z + R + kRing);
+    // The slot of plane z + R + kRing held plane z - R - 1, read by no one
+    // once every thread has passed this plane's barrier.
+    issue(z + R + kRing, slot_at(s0, R + kRing));
+    s0 = slot_at(s0, 1);
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
@@ -378,9 +410,10 @@ template <class T, int OP, int ORDER>
 gc_status launch_zring(gc_context* ctx, const OpParams<T>& p0) {
   constexpr int R = OpShape<OP, ORDER>::R;
   constexpr int NF = OpShape<OP, ORDER>::NF;
-  constexpr size_t smem = sizeof(T) * NF * (2 * R + 1 + kRing) * (BX + 2 * R) * (BY + 2 * R);
+  constexpr int TY = BY * zring_cpt<T, R>();
+  constexpr size_t smem = sizeof(T) * NF * (2 * R + 1 + kRing) * (BX + 2 * R) * (TY + 2 * R);
   OpParams<T> p = p0;
-  const int tiles_x = div_up(p.nx, BX), tiles_y = div_up(p.ny, BY);
+  const int tiles_x = div_up(p.nx, BX), tiles_y = div_up(p.ny, TY);
   const long long tiles = static_cast<long long>(tiles_x) * tiles_y;
   // Enough CTAs to fill the GPU several times, chunks of at least 32 planes
   // so the 2R + kRing prologue planes stay a small overhead.
