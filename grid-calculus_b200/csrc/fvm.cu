@@ -360,8 +360,11 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_kernel(const FvmParams
 template <int MODE>
 __global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_x2_kernel(const FvmParams<float> p, int zc) {
   constexpr int RW = 2 * FZ_X + 4;
-  __shared__ __align__(8) float sy[FZ_Y + 2][RW];
-  __shared__ __align__(8) float sd[FZ_Y + 2][RW];
+  // Two plane buffers: plane z's rows go to buffer z & 1, so the one barrier
+  // per plane suffices (a buffer is rewritten two planes later, after every
+  // thread has passed the barrier of the plane in between).
+  __shared__ __align__(8) float sy2[2][FZ_Y + 2][RW];
+  __shared__ __align__(8) float sd2[2][FZ_Y + 2][RW];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const int x0 = blockIdx.x * (2 * FZ_X), y0 = blockIdx.y * FZ_Y;
@@ -429,6 +432,8 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_x2_kernel(const FvmPar
     qk[2] = n_k;
     qy[2] = y2(n_p, n_k);
     qd[2] = n_d;
+    float(&sy)[FZ_Y + 2][RW] = sy2[(z - z0) & 1];
+    float(&sd)[FZ_Y + 2][RW] = sd2[(z - z0) & 1];
     const float hxy = n_hxy, hxd = n_hxd;
     const float2 hyy = n_hyy, hyd = n_hyd, k1c = n_k1, k2c = n_k2;
     if (z + 1 < z1) {
@@ -489,7 +494,6 @@ __global__ void __launch_bounds__(FZ_X * FZ_Y) fvm_zmarch_x2_kernel(const FvmPar
       const size_t gi = static_cast<size_t>(z) * plane + static_cast<size_t>(y0 + ty) * nx + (x0 + 2 * tx);
       *reinterpret_cast<float2*>(p.out + gi) = make_float2(out[0], out[1]);
     }
-    __syncthreads();
   }
 }
 
