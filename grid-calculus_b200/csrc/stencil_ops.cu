@@ -461,15 +461,20 @@ gc_status launch_one(gc_context* ctx, const OpParams<T>& p0) {
 template <class T, int OP>
 gc_status dispatch_order(gc_context* ctx, int order, const OpParams<T>& p) {
   const bool z3 = p.nz > 1;
-  // 3-D grids.  Gradient, divergence and the order-6 laplacian march with a
-  // register queue (one field's value per plane and thread, halo strips by
-  // a few threads); the order-2/4 laplacian and the biharmonic stage whole
-  // planes through the asynchronous ring (measured per operator and order
-  // on 256^3 and 512^3).  The z-march needs the z extent to exceed the
-  // radius; smaller extents take the ring (planes wrap).
+  // 3-D grids.  The divergence, and in double the gradient above order 2
+  // and the order-6 laplacian, march with a register queue (one field's
+  // value per plane and thread, halo strips by a few threads); everything
+  // else stages whole planes through the asynchronous ring with several
+  // cells per thread.  Measured on B200 at 512^3, ms per launch (z-march /
+  // ring): float gradient order 2 0.521 / 0.411, order 4 0.614 / 0.494,
+  // laplacian order 6 0.589 / 0.543; double gradient order 2 0.821 / 0.729,
+  // order 4 0.936 / 1.052, laplacian order 6 0.788 / 0.964.  The z-march
+  // needs the z extent to exceed the radius; smaller extents take the ring
+  // (planes wrap).
   if (z3) {
     if constexpr (OP == OP_GRAD || OP == OP_DIV || OP == OP_LAP) {
-      if ((OP != OP_LAP || order == 6) && p.nz > 2 * OpShape<OP, 6>::R) {
+      const bool queue = OP == OP_DIV || (sizeof(T) == 8 && (OP == OP_GRAD ? order > 2 : order == 6));
+      if (queue && p.nz > 2 * OpShape<OP, 6>::R) {
         switch (order) {
           case 2: return launch_zmarch<T, OP, 2>(ctx, p);
           case 4: return launch_zmarch<T, OP, 4>(ctx, p);
