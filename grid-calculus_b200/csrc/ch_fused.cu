@@ -49,8 +49,9 @@ constexpr long long kFzWaitCycles = 4000000000LL;  // about 2 s at 2 GHz
 constexpr size_t fz_al(size_t b) { return (b + 127) / 128 * 128; }
 
 // Tile of TX_ x TY_ output cells: 64 x 28 (two CTAs per SM) for grids with
-// enough tiles, 64 x 16 (three CTAs per SM, more tiles) for small grids and
-// 32 x 16 for grids that 64 x 16 tiles would not spread over every SM.
+// enough tiles, 64 x 16 (three CTAs per SM, more tiles) for small grids,
+// 32 x 16 for grids that 64 x 16 tiles would not spread over every SM and
+// 32 x 8 where 32 x 16 tiles would fill under half of them.
 template <int TY_, int TX_ = 64>
 struct FzLayout {
   static constexpr int R = 1;
@@ -72,7 +73,9 @@ struct FzLayout {
   static constexpr uint32_t TX_BYTES = static_cast<uint32_t>(sizeof(double) * SX * SY);
 };
 static_assert(FzLayout<28>::BYTES <= 113 * 1024, "two CTAs per SM");
-static_assert(FzLayout<16>::BYTES <= 74 * 1024 && FzLayout<16, 32>::BYTES <= 74 * 1024, "three CTAs per SM");
+static_assert(FzLayout<16>::BYTES <= 74 * 1024 && FzLayout<16, 32>::BYTES <= 74 * 1024 &&
+                  FzLayout<8, 32>::BYTES <= 74 * 1024,
+              "three CTAs per SM");
 static_assert((FzLayout<16, 32>::SX * 8) % 16 == 0 && FzLayout<16, 32>::TX % 8 == 0,
               "TMA box rows and x offsets stay 16-byte multiples");
 static_assert((FzLayout<28>::SX * 8) % 16 == 0 && FzLayout<28>::H % 2 == 0,
@@ -303,7 +306,9 @@ gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* c
   // the work; the shorter ones make more tiles and fit three CTAs per SM,
   // which pays while 64 x 28 tiles would fill fewer than two rounds of the
   // persistent CTAs.  32 x 16 tiles, on grids that 64 x 16 tiles would not
-  // spread over every SM: 128^2 6.8 -> 5.5 us, 256^2 7.1 -> 5.4 us.
+  // spread over every SM: 128^2 6.8 -> 5.5 us, 256^2 7.1 -> 5.4 us; 32 x 8
+  // tiles where 32 x 16 ones would fill under half the SMs: 128^2 5.5 ->
+  // 4.5 us.
   FzParams a{};
   StageParams<double>& p = a.p;
   p.nx = g->nx; p.ny = g->ny; p.nz = 1;
@@ -325,8 +330,11 @@ gc_status ch_fused_step(gc_context* ctx, const gc_grid* g, const gc_ch_params* c
   const long long tiles28 = static_cast<long long>(div_up(g->nx, 64)) * div_up(g->ny, 28);
   const long long tiles16 = static_cast<long long>(div_up(g->nx, 64)) * div_up(g->ny, 16);
   const bool tall = g->ny >= FzLayout<28>::SY && tiles28 >= 2LL * FzLayout<28>::CTAS_PER_SM * ctx->num_sms;
+  const long long tiles16n = static_cast<long long>(div_up(g->nx, 32)) * div_up(g->ny, 16);
   const bool narrow = g->nx < FzLayout<16>::SX || tiles16 < ctx->num_sms;
+  const bool flat = narrow && 2 * tiles16n < ctx->num_sms;  // 32 x 16 tiles would fill under half the SMs
   const gc_status s = tall     ? fz_launch<28, 64>(ctx, g, a, unit)
+                      : flat   ? fz_launch<8, 32>(ctx, g, a, unit)
                       : narrow ? fz_launch<16, 32>(ctx, g, a, unit)
                                : fz_launch<16, 64>(ctx, g, a, unit);
   if (s == GC_ERR_UNSUPPORTED) return GC_OK;  // layout unfit for TMA: the stage kernels run

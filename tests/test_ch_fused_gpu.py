@@ -1,8 +1,9 @@
 """The fused RK4 step kernel (all four stages of a step on a tile with an
 8-cell halo in shared memory; one launch per step) against the oracle, bit
 for bit: grids with TMA-loaded interior tiles and wrapped edge tiles, partial
-last tiles, each of its three tile shapes (32 x 16 on grids that 64 x 16
-tiles would not spread over every SM, 64 x 16, 64 x 28 on large grids), the
+last tiles, each of its four tile shapes (32 x 8 and 32 x 16 on grids that
+64 x 16 tiles would not spread over every SM, 64 x 16, 64 x 28 on large
+grids), the
 smallest grid it takes, non-unit spacing / mobility / kappa, step counts
 across graph replays; and against the four stage kernels on a larger grid."""
 import numpy as np
@@ -34,8 +35,8 @@ def ctx(gc):
 
 
 @pytest.mark.parametrize("shape", [(1, 44, 80), (1, 100, 160), (1, 131, 250), (1, 300, 400), (1, 87, 82),
-                                   (1, 64, 1030), (1, 33, 48), (1, 40, 50), (1, 128, 128), (1, 512, 512),
-                                   (1, 520, 600)])
+                                   (1, 64, 1030), (1, 33, 48), (1, 40, 50), (1, 128, 128), (1, 256, 256),
+                                   (1, 512, 512), (1, 520, 600)])
 @pytest.mark.parametrize("steps", [1, 17, 40])
 def test_fused_bit_exact(gc, oracle, ctx, shape, steps):
     rng = np.random.default_rng(shape[1] * 7 + shape[2] + steps)
