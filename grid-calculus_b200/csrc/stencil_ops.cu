@@ -461,14 +461,15 @@ __device__ __forceinline__ void cp_async_n(void* smem, const void* gmem, int byt
 // ring-slot arithmetic and the copy bookkeeping) is shared by CPT cells.  One
 // cell per thread and plane left the float kernel bound by that work (105
 // instructions per cell at 83 % issue).  Measured on B200 at 512^3, ms per
-// launch for CPT = 1 / 2 / 4 (float) and 1 / 2 (double): float laplacian
+// launch for CPT = 1 / 2 / 4 (float; 8 at radius 1: laplacian order 2 0.291,
+// gradient order 2 0.415 against 0.411 at 4) and 1 / 2 (double): float laplacian
 // order 2 0.466 / 0.368 / 0.309, order 4 0.583 / 0.478 / 0.443, biharmonic
 // 0.726 / 0.669 / 0.642; double laplacian order 2 0.500 / 0.455, order 4
 // 0.755 / 0.766, biharmonic 1.041 / 1.074 (at radius 2 the taller double
 // ring costs more occupancy than the shared work saves).
 template <class T, int R>
 __host__ __device__ constexpr int zring_cpt() {
-  return sizeof(T) == 4 ? 4 : (R == 1 ? 2 : 1);
+  return sizeof(T) == 4 ? (R == 1 ? 8 : 4) : (R == 1 ? 2 : 1);
 }
 
 template <class T, int OP, int ORDER>
