@@ -49,6 +49,18 @@ def test_python_mirror_imports():
         raise AssertionError("Grid(0, 1, 1) accepted")
 
 
+def test_python_mirror_constants_match_the_header():
+    """The Python mirror's enum-like constants are the header's values."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "grid-calculus_b200"))
+    import gridcalc_b200 as gc
+    text = open(HEADER).read()
+    assert int(re.search(r"#define GC_BATCH_FUSED (\d+)", text).group(1)) == gc.ChBatch.FUSED
+    opts = dict(re.findall(r"(GC_OPT_\w+) = (\d+)", text))
+    assert int(opts["GC_OPT_CLUSTER_STEPPING"]) == gc.OPT_CLUSTER_STEPPING
+    assert int(opts["GC_OPT_FUSED_STEP"]) == gc.OPT_FUSED_STEP
+
+
 def test_c_program_uses_the_abi_without_gpu(tmp_path):
     """tests/c/abi_c_test.c: the header compiles as strict C99 and a C
     program linked against the library runs the device-free entry points."""
